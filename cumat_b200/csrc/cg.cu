@@ -1,0 +1,1364 @@
+// Conjugate-gradient solver behind the C ABI.
+//
+// Replaces cuMat's ConjugateGradient / IterativeSolverBase / DiagonalPreconditioner
+// / IdentityPreconditioner (cuMat/src/ConjugateGradient.h:66-265,
+// IterativeSolverBase.h:10-135) for sparse matrices. The reference runs each
+// iteration as ~11 kernel launches (SpMV, 4 cwise kernels, 3 two-pass CUB
+// reductions) plus a blocking device-to-host copy of |r|^2
+// (ConjugateGradient.h:180-203). Here:
+//
+//  * PERSISTENT path: one launch for the whole solve. Each CTA pulls a
+//    (system, batch) instance from an atomic work counter (largest systems
+//    first) and runs the complete PCG loop for it with CTA-level reductions
+//    only (__syncthreads, no grid synchronisation, no host round trip).
+//  * GRID path (large systems): three fused kernels per iteration over 256-row
+//    tiles - SpMV + p.q, x/r update + |r|^2 + r.z, p update - with the per-system
+//    reductions finished by the last tile of each system (ticket counter, fixed
+//    combine order, deterministic). Scalars stay on the device; the loop is a
+//    CUDA graph with a conditional WHILE node whose condition a one-thread
+//    kernel sets from the device-side count of running systems.
+//  * REFINED solve (mixed precision): FP64 outer residual / update / norms
+//    around the FP32 (F32 or BF16 values) inner PCG, fused into the persistent
+//    kernel per system, or driven from the host over the grid path.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "cg_dev.cuh"
+#include "common.cuh"
+#include "objects.h"
+
+namespace cmcg {
+cmcg_status spmv_dispatch(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t xb, void* y, int32_t mode);
+cmcg_status dot_dispatch(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb,
+                         void* out, int32_t ob);
+cmcg_status sddmm_dispatch(cmcg_matrix M, int32_t dt, double alpha, const void* u, int32_t ub, const void* v,
+                           int32_t vb, void* out, int32_t ob);
+}  // namespace cmcg
+
+using namespace cmcg;
+
+namespace {
+
+constexpr int kTile = 256;          // rows per tile of the grid path (= threads per CTA)
+constexpr int kPersistThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Kernel arguments
+// ---------------------------------------------------------------------------
+
+template <typename MT>
+struct MatArgs {
+    const int32_t* rp;
+    const int32_t* ci;
+    const int32_t* ell;
+    int32_t width, rows_pad;
+    const MT* vals;
+    int64_t vstride;
+    int32_t mb;
+};
+
+template <typename MT, int FMT>
+__device__ __forceinline__ InstMatrix<MT, FMT> inst_matrix(const MatArgs<MT>& m, int b) {
+    InstMatrix<MT, FMT> A;
+    const MT* v = m.vals + (m.mb == 1 ? 0 : static_cast<int64_t>(b) * m.vstride);
+    A.csr = CsrView<MT>{m.rp, m.ci, v};
+    A.ell = EllView<MT>{m.ell, v, m.width, m.rows_pad};
+    return A;
+}
+
+// Per-instance state (instance = batch * n_sys + system).
+struct InstState {
+    double* bb;      // |b|^2
+    double* rr;      // |r|^2 (latest)
+    double* rz;      // r.z
+    double* alpha;
+    double* beta;
+    int32_t* it;     // iterations (reference semantics)
+    int32_t* status;
+    int32_t* outer;  // refinement steps
+    double* err;     // sqrt(rr / bb) written by the finaliser
+    unsigned* tk1;
+    unsigned* tk2;
+};
+
+template <typename VT, typename MT>
+struct SolveArgs {
+    MatArgs<MT> m;
+    int32_t rows, n_sys, ob;
+    const int32_t* row_off;
+    const int32_t* order;          // persistent: systems, largest first
+    int32_t* next;                 // persistent: work counter
+    // grid path tiles
+    int32_t n_tiles;
+    const int32_t* tile_row0;
+    const int32_t* tile_sys;
+    const int32_t* sys_tile_begin;
+    VT* part1;
+    VT* part2;
+    int32_t* active;
+    int32_t* loops;
+    int32_t loop_cap;
+    cudaGraphConditionalHandle cond;
+    // vectors, [batch][rows]
+    const VT* dinv;
+    int32_t dinv_b;
+    const VT* b;
+    int32_t b_b;
+    const VT* guess;
+    int32_t g_b;
+    VT* x;
+    VT* r;
+    VT* p;
+    VT* q;
+    double tol;
+    int64_t max_iter;              // < 0: 2 * rows of the system
+    InstState st;
+};
+
+__device__ __forceinline__ int64_t sys_max_iter(int64_t mi, int n) { return mi < 0 ? 2 * static_cast<int64_t>(n) : mi; }
+
+// ---------------------------------------------------------------------------
+// One system, one CTA (shared by the persistent plain and refined kernels)
+// ---------------------------------------------------------------------------
+
+// PCG of one system with the whole CTA. Vectors are batch slices indexed by
+// global row. Returns the status; writes iterations / |r|^2 / |b|^2.
+template <typename VT, typename MT, int FMT>
+__device__ int32_t cta_pcg(const InstMatrix<MT, FMT>& A, int r0, int n, const VT* __restrict__ bv,
+                           const VT* __restrict__ g, VT* __restrict__ x, VT* __restrict__ r, VT* __restrict__ p,
+                           VT* __restrict__ q, const VT* __restrict__ dinv, VT tol, int64_t maxit, WarpStage<VT>* stage,
+                           VT* red, int32_t& it_out, VT& rr_out, VT& bb_out, bool abs_zero_test = true) {
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int r1 = r0 + n;
+    VT acc[2] = {VT(0), VT(0)};
+    if (g) {
+        cta_rows_product<VT>(A, r0, n, GlobalX<VT>{g}, stage, [&](int row, VT v) {
+            const VT bi = bv[row];
+            const VT ri = bi - v;
+            r[row] = ri;
+            x[row] = g[row];
+            acc[0] += bi * bi;
+            acc[1] += ri * ri;
+        });
+    } else {
+        for (int i = r0 + tid; i < r1; i += T) {
+            const VT bi = bv[i];
+            r[i] = bi;
+            x[i] = VT(0);
+            acc[0] += bi * bi;
+        }
+        acc[1] = acc[0];
+    }
+    block_sum<VT, 2>(acc, red);
+    const VT bb = acc[0];
+    VT rr = acc[1];
+    const VT thr = tol * tol * bb;
+    int32_t status = ST_RUNNING;
+    int32_t it = 0;
+    if ((abs_zero_test && bb < tol * tol) || bb == VT(0)) {
+        for (int i = r0 + tid; i < r1; i += T) x[i] = VT(0);
+        status = CMCG_SOLVE_ZERO_RHS;
+    } else if (!finite_(rr) || !finite_(bb)) {
+        status = CMCG_SOLVE_NON_FINITE;
+    } else if (rr < thr) {
+        status = CMCG_SOLVE_CONVERGED;
+    } else {
+        VT rzv[1] = {VT(0)};
+        for (int i = r0 + tid; i < r1; i += T) {
+            const VT ri = r[i];
+            const VT zi = dinv ? dinv[i] * ri : ri;
+            p[i] = zi;
+            rzv[0] += ri * zi;
+        }
+        block_sum<VT, 1>(rzv, red);
+        VT rz = rzv[0];
+        if (!finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
+        else if (!(rz > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
+        while (status == ST_RUNNING) {
+            if (it >= maxit) { status = CMCG_SOLVE_MAX_ITER; break; }
+            VT pq[1] = {VT(0)};
+            cta_rows_product<VT>(A, r0, n, GlobalX<VT>{p}, stage, [&](int row, VT v) {
+                q[row] = v;
+                pq[0] += p[row] * v;
+            });
+            block_sum<VT, 1>(pq, red);
+            const VT alpha = rz / pq[0];
+            if (!finite_(pq[0]) || !finite_(alpha)) { status = CMCG_SOLVE_NON_FINITE; break; }
+            if (!(pq[0] > VT(0))) { status = CMCG_SOLVE_BREAKDOWN; break; }
+            VT s2[2] = {VT(0), VT(0)};
+            for (int i = r0 + tid; i < r1; i += T) {
+                x[i] += alpha * p[i];
+                const VT ri = r[i] - alpha * q[i];
+                r[i] = ri;
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                s2[0] += ri * ri;
+                s2[1] += ri * zi;
+            }
+            block_sum<VT, 2>(s2, red);
+            rr = s2[0];
+            if (!finite_(rr) || !finite_(s2[1])) { status = CMCG_SOLVE_NON_FINITE; break; }
+            if (rr < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+            const VT rzn = s2[1];
+            if (!(rzn > VT(0))) { status = CMCG_SOLVE_BREAKDOWN; break; }
+            const VT beta = rzn / rz;
+            rz = rzn;
+            for (int i = r0 + tid; i < r1; i += T) {
+                const VT ri = r[i];
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                p[i] = zi + beta * p[i];
+            }
+            __syncthreads();
+            ++it;
+        }
+    }
+    __syncthreads();
+    it_out = it;
+    rr_out = rr;
+    bb_out = bb;
+    return status;
+}
+
+__device__ __forceinline__ int fetch_item(int32_t* next, int* slot) {
+    if (threadIdx.x == 0) *slot = atomicAdd(next, 1);
+    __syncthreads();
+    const int item = *slot;
+    __syncthreads();
+    return item;
+}
+
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kPersistThreads) k_persistent_cg(SolveArgs<VT, MT> a) {
+    __shared__ WarpStage<VT> stage[kPersistThreads / 32];
+    __shared__ VT red[2 * (kPersistThreads / 32)];
+    __shared__ int slot;
+    const int n_inst = a.n_sys * a.ob;
+    for (;;) {
+        const int item = fetch_item(a.next, &slot);
+        if (item >= n_inst) return;
+        const int s = a.order[item / a.ob], b = item % a.ob, inst = b * a.n_sys + s;
+        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
+        const auto A = inst_matrix<MT, FMT>(a.m, b);
+        const int64_t vo = static_cast<int64_t>(b) * a.rows;
+        int32_t it;
+        VT rr, bb;
+        const int32_t status = cta_pcg<VT, MT, FMT>(
+            A, r0, n, a.b + (a.b_b == 1 ? 0 : vo), a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr, a.x + vo,
+            a.r + vo, a.p + vo, a.q + vo, a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr, static_cast<VT>(a.tol),
+            sys_max_iter(a.max_iter, n), stage, red, it, rr, bb);
+        if (threadIdx.x == 0) {
+            a.st.it[inst] = it;
+            a.st.status[inst] = status;
+            a.st.rr[inst] = static_cast<double>(rr);
+            a.st.bb[inst] = static_cast<double>(bb);
+            a.st.outer[inst] = 0;
+            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(static_cast<double>(rr) / static_cast<double>(bb));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Refined (mixed precision) persistent kernel
+// ---------------------------------------------------------------------------
+
+template <typename MI, typename MO>
+struct RefineArgs {
+    MatArgs<MI> inner;      // F32 / BF16 values, FP32 arithmetic
+    MatArgs<MO> outer;      // F32 / F64 values, FP64 arithmetic
+    int32_t rows, n_sys, ob;
+    const int32_t* row_off;
+    const int32_t* order;
+    int32_t* next;
+    const float* dinv;
+    int32_t dinv_b;
+    const double* b;
+    int32_t b_b;
+    double* x;
+    float* r32;   // inner rhs = rounded outer residual
+    float* d32;   // inner solution
+    float* r;     // inner CG vectors
+    float* p;
+    float* q;
+    double inner_tol, outer_tol;
+    int64_t max_inner;
+    int32_t max_outer;
+    InstState st;
+};
+
+template <typename MI, typename MO, int FMT>
+__global__ void __launch_bounds__(kPersistThreads) k_persistent_refined(RefineArgs<MI, MO> a) {
+    __shared__ WarpStage<double> stage_raw[kPersistThreads / 32];  // large enough for float too
+    __shared__ double red64[2 * (kPersistThreads / 32)];
+    __shared__ float red32[2 * (kPersistThreads / 32)];
+    __shared__ int slot;
+    WarpStage<float>* stage32 = reinterpret_cast<WarpStage<float>*>(stage_raw);
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int n_inst = a.n_sys * a.ob;
+    for (;;) {
+        const int item = fetch_item(a.next, &slot);
+        if (item >= n_inst) return;
+        const int s = a.order[item / a.ob], bi = item % a.ob, inst = bi * a.n_sys + s;
+        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0, r1 = r0 + n;
+        const auto Ai = inst_matrix<MI, FMT>(a.inner, bi);
+        const auto Ao = inst_matrix<MO, FMT>(a.outer, bi);
+        const int64_t vo = static_cast<int64_t>(bi) * a.rows;
+        const double* bv = a.b + (a.b_b == 1 ? 0 : vo);
+        double* x = a.x + vo;
+        float* r32 = a.r32 + vo;
+        float* d32 = a.d32 + vo;
+        const float* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+        // x = 0, r = b
+        double acc[1] = {0.0};
+        for (int i = r0 + tid; i < r1; i += T) {
+            const double b_i = bv[i];
+            x[i] = 0.0;
+            r32[i] = static_cast<float>(b_i);
+            acc[0] += b_i * b_i;
+        }
+        block_sum<double, 1>(acc, red64);
+        const double bb = acc[0];
+        double rr = bb;
+        int32_t status = ST_RUNNING, outer = 0;
+        int64_t inner_total = 0;
+        const double thr = a.outer_tol * a.outer_tol * bb;
+        if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
+        else if (!finite_(bb)) status = CMCG_SOLVE_NON_FINITE;
+        while (status == ST_RUNNING) {
+            if (rr < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+            if (outer >= a.max_outer) { status = CMCG_SOLVE_MAX_ITER; break; }
+            int32_t it;
+            float rr_in, bb_in;
+            const int32_t st_in = cta_pcg<float, MI, FMT>(Ai, r0, n, r32, nullptr, d32, a.r + vo, a.p + vo, a.q + vo,
+                                                          dinv, static_cast<float>(a.inner_tol),
+                                                          sys_max_iter(a.max_inner, n), stage32, red32, it, rr_in, bb_in,
+                                                          /*abs_zero_test=*/false);
+            inner_total += it;
+            if (st_in == CMCG_SOLVE_NON_FINITE || (st_in == CMCG_SOLVE_BREAKDOWN && it == 0)) { status = st_in; break; }
+            for (int i = r0 + tid; i < r1; i += T) x[i] += static_cast<double>(d32[i]);
+            __syncthreads();
+            // FP64 residual with the outer values, rounded into the next inner rhs
+            double rv[1] = {0.0};
+            cta_rows_product<double>(Ao, r0, n, GlobalX<double>{x}, stage_raw, [&](int row, double v) {
+                const double ri = bv[row] - v;
+                r32[row] = static_cast<float>(ri);
+                rv[0] += ri * ri;
+            });
+            block_sum<double, 1>(rv, red64);
+            rr = rv[0];
+            ++outer;
+            if (!finite_(rr)) { status = CMCG_SOLVE_NON_FINITE; break; }
+        }
+        if (tid == 0) {
+            a.st.it[inst] = static_cast<int32_t>(inner_total < INT32_MAX ? inner_total : INT32_MAX);
+            a.st.status[inst] = status;
+            a.st.rr[inst] = rr;
+            a.st.bb[inst] = bb;
+            a.st.outer[inst] = outer;
+            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(rr / bb);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Grid path kernels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int32_t ld_status(const int32_t* s) { return *reinterpret_cast<const volatile int32_t*>(s); }
+
+// Publishes this tile's NV partial sums and, if it is the last tile of its
+// system instance, returns true with the instance totals (fixed order) in tot.
+template <typename VT, int NV>
+__device__ bool tile_ticket(const VT (&v)[NV], VT* const (&part)[NV], int64_t pbase, int t_begin, int t_count,
+                            int64_t pidx, unsigned* tk, int inst, VT (&tot)[NV], VT* red, bool* last_s) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) part[j][pidx] = v[j];
+        __threadfence();
+        const unsigned t = atomicAdd(tk + inst, 1u);
+        *last_s = (t == static_cast<unsigned>(t_count - 1));
+    }
+    __syncthreads();
+    const bool last = *last_s;
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) tot[j] = VT(0);
+    for (int i = threadIdx.x; i < t_count; i += blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) tot[j] += __ldcg(part[j] + pbase + t_begin + i);
+    }
+    block_sum<VT, NV>(tot, red);
+    if (threadIdx.x == 0) tk[inst] = 0u;
+    return true;
+}
+
+struct TileInfo {
+    int b, t, s, inst, r0, r1, t_begin, t_count;
+};
+
+template <typename VT, typename MT>
+__device__ __forceinline__ TileInfo tile_info(const SolveArgs<VT, MT>& a, int64_t item) {
+    TileInfo ti;
+    ti.b = static_cast<int>(item / a.n_tiles);
+    ti.t = static_cast<int>(item - static_cast<int64_t>(ti.b) * a.n_tiles);
+    ti.s = a.tile_sys[ti.t];
+    ti.inst = ti.b * a.n_sys + ti.s;
+    ti.r0 = a.tile_row0[ti.t];
+    ti.r1 = min(ti.r0 + kTile, a.row_off[ti.s + 1]);
+    ti.t_begin = a.sys_tile_begin[ti.s];
+    ti.t_count = a.sys_tile_begin[ti.s + 1] - ti.t_begin;
+    return ti;
+}
+
+// init A: x = guess or 0, r = b - A x, |b|^2, |r|^2 -> status
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
+    __shared__ WarpStage<VT> stage[kTile / 32];
+    __shared__ VT red[2 * (kTile / 32)];
+    __shared__ bool last_s;
+    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const TileInfo ti = tile_info(a, item);
+        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+        const VT* bv = a.b + (a.b_b == 1 ? 0 : vo);
+        VT* x = a.x + vo;
+        VT* r = a.r + vo;
+        VT acc[2] = {VT(0), VT(0)};
+        if (a.guess) {
+            const VT* g = a.guess + (a.g_b == 1 ? 0 : vo);
+            const auto A = inst_matrix<MT, FMT>(a.m, ti.b);
+            cta_rows_product<VT>(A, ti.r0, ti.r1 - ti.r0, GlobalX<VT>{g}, stage, [&](int row, VT v) {
+                const VT bi = bv[row];
+                const VT ri = bi - v;
+                r[row] = ri;
+                x[row] = g[row];
+                acc[0] += bi * bi;
+                acc[1] += ri * ri;
+            });
+        } else {
+            const int i = ti.r0 + threadIdx.x;
+            if (i < ti.r1) {
+                const VT bi = bv[i];
+                r[i] = bi;
+                x[i] = VT(0);
+                acc[0] = bi * bi;
+                acc[1] = acc[0];
+            }
+        }
+        block_sum<VT, 2>(acc, red);
+        VT tot[2];
+        VT* const parts[2] = {a.part1, a.part2};
+        if (tile_ticket<VT, 2>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
+                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk1, ti.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const VT bb = tot[0], rr = tot[1], tol = static_cast<VT>(a.tol);
+            a.st.bb[ti.inst] = bb;
+            a.st.rr[ti.inst] = rr;
+            a.st.it[ti.inst] = 0;
+            a.st.outer[ti.inst] = 0;
+            int32_t status = ST_RUNNING;
+            if (bb < tol * tol || bb == VT(0)) status = CMCG_SOLVE_ZERO_RHS;
+            else if (!finite_(bb) || !finite_(rr)) status = CMCG_SOLVE_NON_FINITE;
+            else if (rr < tol * tol * bb) status = CMCG_SOLVE_CONVERGED;
+            a.st.status[ti.inst] = status;
+            if (status == ST_RUNNING) atomicAdd(a.active, 1);
+        }
+    }
+}
+
+// init B: zero x of zero-rhs systems; p = M^-1 r and r.z of running systems
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
+    __shared__ VT red[2 * (kTile / 32)];
+    __shared__ bool last_s;
+    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const TileInfo ti = tile_info(a, item);
+        const int32_t st = ld_status(a.st.status + ti.inst);
+        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+        const int i = ti.r0 + threadIdx.x;
+        if (st == CMCG_SOLVE_ZERO_RHS) {
+            if (i < ti.r1) a.x[vo + i] = VT(0);
+            continue;
+        }
+        if (st != ST_RUNNING) continue;
+        const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+        VT acc[1] = {VT(0)};
+        if (i < ti.r1) {
+            const VT ri = a.r[vo + i];
+            const VT zi = dinv ? dinv[i] * ri : ri;
+            a.p[vo + i] = zi;
+            acc[0] = ri * zi;
+        }
+        block_sum<VT, 1>(acc, red);
+        VT tot[1];
+        VT* const parts[1] = {a.part1};
+        if (tile_ticket<VT, 1>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
+                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk2, ti.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const VT rz = tot[0];
+            a.st.rz[ti.inst] = rz;
+            int32_t status = ST_RUNNING;
+            if (!finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
+            else if (!(rz > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
+            if (status != ST_RUNNING) {
+                a.st.status[ti.inst] = status;
+                atomicSub(a.active, 1);
+            }
+        }
+    }
+}
+
+// iteration kernel 1: q = A p, p.q -> alpha
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
+    __shared__ WarpStage<VT> stage[kTile / 32];
+    __shared__ VT red[kTile / 32];
+    __shared__ bool last_s;
+    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const TileInfo ti = tile_info(a, item);
+        if (ld_status(a.st.status + ti.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+        const VT* p = a.p + vo;
+        VT* q = a.q + vo;
+        const auto A = inst_matrix<MT, FMT>(a.m, ti.b);
+        VT acc[1] = {VT(0)};
+        cta_rows_product<VT>(A, ti.r0, ti.r1 - ti.r0, GlobalX<VT>{p}, stage, [&](int row, VT v) {
+            q[row] = v;
+            acc[0] += p[row] * v;
+        });
+        block_sum<VT, 1>(acc, red);
+        VT tot[1];
+        VT* const parts[1] = {a.part1};
+        if (tile_ticket<VT, 1>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
+                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk1, ti.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const VT pq = tot[0];
+            const VT alpha = static_cast<VT>(a.st.rz[ti.inst]) / pq;
+            int32_t status = ST_RUNNING;
+            if (!finite_(pq) || !finite_(alpha)) status = CMCG_SOLVE_NON_FINITE;
+            else if (!(pq > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
+            if (status != ST_RUNNING) {
+                a.st.status[ti.inst] = status;
+                atomicSub(a.active, 1);
+            } else {
+                a.st.alpha[ti.inst] = alpha;
+            }
+        }
+    }
+}
+
+// iteration kernel 2: x += alpha p, r -= alpha q, |r|^2, r.z -> convergence, beta
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
+    __shared__ VT red[2 * (kTile / 32)];
+    __shared__ bool last_s;
+    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const TileInfo ti = tile_info(a, item);
+        if (ld_status(a.st.status + ti.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+        const VT alpha = static_cast<VT>(a.st.alpha[ti.inst]);
+        const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+        const int i = ti.r0 + threadIdx.x;
+        VT acc[2] = {VT(0), VT(0)};
+        if (i < ti.r1) {
+            a.x[vo + i] += alpha * a.p[vo + i];
+            const VT ri = a.r[vo + i] - alpha * a.q[vo + i];
+            a.r[vo + i] = ri;
+            const VT zi = dinv ? dinv[i] * ri : ri;
+            acc[0] = ri * ri;
+            acc[1] = ri * zi;
+        }
+        block_sum<VT, 2>(acc, red);
+        VT tot[2];
+        VT* const parts[2] = {a.part1, a.part2};
+        if (tile_ticket<VT, 2>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
+                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk2, ti.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const VT rr = tot[0], rzn = tot[1];
+            const VT tol = static_cast<VT>(a.tol);
+            const VT bb = static_cast<VT>(a.st.bb[ti.inst]);
+            a.st.rr[ti.inst] = rr;
+            int32_t status = ST_RUNNING;
+            const int n = a.row_off[ti.s + 1] - a.row_off[ti.s];
+            if (!finite_(rr) || !finite_(rzn)) status = CMCG_SOLVE_NON_FINITE;
+            else if (rr < tol * tol * bb) status = CMCG_SOLVE_CONVERGED;
+            else if (!(rzn > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
+            else {
+                const VT rz = static_cast<VT>(a.st.rz[ti.inst]);
+                a.st.beta[ti.inst] = rzn / rz;
+                a.st.rz[ti.inst] = rzn;
+                const int32_t it = a.st.it[ti.inst] + 1;
+                a.st.it[ti.inst] = it;
+                if (it >= sys_max_iter(a.max_iter, n)) status = CMCG_SOLVE_MAX_ITER;
+            }
+            if (status != ST_RUNNING) {
+                a.st.status[ti.inst] = status;
+                atomicSub(a.active, 1);
+            }
+        }
+    }
+}
+
+// iteration kernel 3: p = M^-1 r + beta p
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kTile) k_grid_pupdate(SolveArgs<VT, MT> a) {
+    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const TileInfo ti = tile_info(a, item);
+        if (ld_status(a.st.status + ti.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+        const int i = ti.r0 + threadIdx.x;
+        if (i < ti.r1) {
+            const VT beta = static_cast<VT>(a.st.beta[ti.inst]);
+            const VT ri = a.r[vo + i];
+            const VT zi = a.dinv ? a.dinv[(a.dinv_b == 1 ? 0 : vo) + i] * ri : ri;
+            a.p[vo + i] = zi + beta * a.p[vo + i];
+        }
+    }
+}
+
+// loop condition of the graph's WHILE node (one thread)
+__global__ void k_grid_cond(const int32_t* active, int32_t* loops, int32_t cap, cudaGraphConditionalHandle h) {
+    const int32_t l = ++(*loops);
+    const unsigned go = (*reinterpret_cast<const volatile int32_t*>(active) > 0 && l < cap) ? 1u : 0u;
+    cudaGraphSetConditional(h, go);
+}
+
+__global__ void k_finalize(InstState st, int32_t n_inst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_inst) return;
+    int32_t s = st.status[i];
+    if (s == ST_RUNNING) { s = CMCG_SOLVE_MAX_ITER; st.status[i] = s; }
+    st.err[i] = (s == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(st.rr[i] / st.bb[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi: inverse diagonal per batch of values, 1 where a_ii is 0 or absent
+// (reference DiagonalPreconditioner + cwiseInverseCheck, ConjugateGradient.h:228-230,
+// UnaryOps.h:177; diagonal lookup as coeff(i, i), SparseMatrixBase.h:258-271)
+// ---------------------------------------------------------------------------
+template <typename VT, typename MT, int FMT>
+__global__ void k_inv_diag(MatArgs<MT> m, int32_t rows, VT* __restrict__ out) {
+    const int64_t items = static_cast<int64_t>(rows) * m.mb;
+    for (int64_t it = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(it / rows);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * rows);
+        const MT* v = m.vals + static_cast<int64_t>(b) * m.vstride;
+        VT d = VT(0);
+        if (FMT == CMCG_CSR) {
+            for (int k = m.rp[r]; k < m.rp[r + 1]; ++k)
+                if (m.ci[k] == r) { d = mval<VT>(v[k]); break; }
+        } else {
+            for (int j = 0; j < m.width; ++j) {
+                const int64_t o = r + static_cast<int64_t>(j) * m.rows_pad;
+                if (m.ell[o] == r) { d = mval<VT>(v[o]); break; }
+            }
+        }
+        out[it] = (d != VT(0)) ? VT(1) / d : VT(1);
+    }
+}
+
+template <typename MT>
+MatArgs<MT> mat_args(cmcg_matrix A) {
+    cmcg_pattern p = A->pat;
+    return MatArgs<MT>{p->d_row_ptr, p->d_col, p->d_ell, p->width, p->rows_pad, static_cast<const MT*>(A->d_vals),
+                       A->stride, A->batches};
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Solver object
+// ---------------------------------------------------------------------------
+
+struct cmcg_solver_s {
+    cmcg_matrix A = nullptr;
+    int32_t precond = CMCG_PRECOND_JACOBI;
+    double tol = 0.0;
+    int64_t max_iter = -1;
+    int32_t path = CMCG_PATH_AUTO;
+    // plan
+    int32_t n_sys = 0, max_sys_rows = 0, n_tiles = 0;
+    int32_t* d_order = nullptr;
+    int32_t* d_tile_row0 = nullptr;
+    int32_t* d_tile_sys = nullptr;
+    int32_t* d_sys_tile_begin = nullptr;
+    // Jacobi inverse diagonal per vector type (F32, F64), [matrix batches][rows]
+    void* dinv[2] = {nullptr, nullptr};
+    // workspace
+    void* vec_ws = nullptr;   size_t vec_ws_bytes = 0;
+    void* ref_ws = nullptr;   size_t ref_ws_bytes = 0;
+    void* part_ws = nullptr;  size_t part_ws_bytes = 0;
+    void* st_ws = nullptr;    size_t st_ws_bytes = 0;
+    int32_t* counters = nullptr;  // next, active, loops
+    void* host_io = nullptr;  size_t host_io_bytes = 0;
+    InstState st{};
+    int32_t st_inst = 0;
+    // graph cache of the grid path
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    std::vector<char> gkey;
+    // last solve
+    int32_t last_inst = 0;
+    bool last_refined = false;
+};
+
+namespace {
+
+cmcg_status build_plan(cmcg_solver s) {
+    cmcg_pattern p = s->A->pat;
+    const auto& ro = p->row_off;
+    const int32_t n_sys = static_cast<int32_t>(ro.size() - 1);
+    std::vector<int64_t> nnz(n_sys);
+    int32_t maxr = 0;
+    for (int32_t i = 0; i < n_sys; ++i) {
+        const int64_t a = ro[i], e = ro[i + 1];
+        maxr = std::max<int32_t>(maxr, static_cast<int32_t>(e - a));
+        nnz[i] = (p->format == CMCG_CSR) ? (p->h_row_ptr[e] - p->h_row_ptr[a]) : (e - a) * p->width;
+    }
+    std::vector<int32_t> order(n_sys);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return nnz[x] > nnz[y]; });
+    std::vector<int32_t> t_row0, t_sys, t_begin(n_sys + 1);
+    for (int32_t i = 0; i < n_sys; ++i) {
+        t_begin[i] = static_cast<int32_t>(t_row0.size());
+        for (int64_t r = ro[i]; r < ro[i + 1]; r += kTile) {
+            t_row0.push_back(static_cast<int32_t>(r));
+            t_sys.push_back(i);
+        }
+    }
+    t_begin[n_sys] = static_cast<int32_t>(t_row0.size());
+    s->n_sys = n_sys;
+    s->max_sys_rows = maxr;
+    s->n_tiles = static_cast<int32_t>(t_row0.size());
+    cudaStream_t st = p->ctx->stream;
+    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_order), order.size() * 4));
+    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_tile_row0), t_row0.size() * 4));
+    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_tile_sys), t_sys.size() * 4));
+    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_sys_tile_begin), t_begin.size() * 4));
+    CMCG_CUDA(cudaMemcpyAsync(s->d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
+    CMCG_CUDA(cudaMemcpyAsync(s->d_tile_row0, t_row0.data(), t_row0.size() * 4, cudaMemcpyHostToDevice, st));
+    CMCG_CUDA(cudaMemcpyAsync(s->d_tile_sys, t_sys.data(), t_sys.size() * 4, cudaMemcpyHostToDevice, st));
+    CMCG_CUDA(cudaMemcpyAsync(s->d_sys_tile_begin, t_begin.data(), t_begin.size() * 4, cudaMemcpyHostToDevice, st));
+    CMCG_CUDA(cudaStreamSynchronize(st));
+    return CMCG_OK;
+}
+
+template <typename VT, typename MT>
+cmcg_status compute_dinv_t(cmcg_solver s, VT* out) {
+    cmcg_matrix A = s->A;
+    cmcg_pattern p = A->pat;
+    const MatArgs<MT> m = mat_args<MT>(A);
+    const int64_t n = static_cast<int64_t>(p->rows) * A->batches;
+    const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, p->ctx->sm_count * 8));
+    if (p->format == CMCG_CSR) k_inv_diag<VT, MT, CMCG_CSR><<<blocks, 256, 0, p->ctx->stream>>>(m, p->rows, out);
+    else k_inv_diag<VT, MT, CMCG_ELLPACK><<<blocks, 256, 0, p->ctx->stream>>>(m, p->rows, out);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+// Returns the inverse diagonal for vector type vdt (computed on first use).
+cmcg_status get_dinv(cmcg_solver s, int32_t vdt, const void** out) {
+    *out = nullptr;
+    if (s->precond != CMCG_PRECOND_JACOBI) return CMCG_OK;
+    const int k = (vdt == CMCG_F64) ? 1 : 0;
+    if (!s->dinv[k]) {
+        const size_t es = (vdt == CMCG_F64) ? 8 : 4;
+        CMCG_TRY(dev_alloc(&s->dinv[k], es * s->A->pat->rows * s->A->batches));
+        cmcg_status st;
+        if (vdt == CMCG_F64) {
+            double* o = static_cast<double*>(s->dinv[k]);
+            st = s->A->dtype == CMCG_F32 ? compute_dinv_t<double, float>(s, o)
+               : s->A->dtype == CMCG_F64 ? compute_dinv_t<double, double>(s, o)
+                                         : compute_dinv_t<double, __nv_bfloat16>(s, o);
+        } else {
+            float* o = static_cast<float*>(s->dinv[k]);
+            st = s->A->dtype == CMCG_F32 ? compute_dinv_t<float, float>(s, o)
+               : s->A->dtype == CMCG_F64 ? compute_dinv_t<float, double>(s, o)
+                                         : compute_dinv_t<float, __nv_bfloat16>(s, o);
+        }
+        if (st != CMCG_OK) return st;
+    }
+    *out = s->dinv[k];
+    return CMCG_OK;
+}
+
+cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
+    const size_t per = 6 * sizeof(double) + 3 * sizeof(int32_t) + 2 * sizeof(unsigned);
+    const size_t need = per * static_cast<size_t>(n_inst) + 256;
+    if (s->st_inst >= n_inst && s->st_ws) return CMCG_OK;
+    dev_free(s->st_ws);
+    s->st_ws = nullptr;
+    s->st_ws_bytes = 0;
+    CMCG_TRY(dev_alloc(&s->st_ws, need));
+    s->st_ws_bytes = need;
+    char* b = static_cast<char*>(s->st_ws);
+    const size_t n = static_cast<size_t>(n_inst);
+    s->st.bb = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.rr = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.rz = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.alpha = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.beta = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.err = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.it = reinterpret_cast<int32_t*>(b); b += 4 * n;
+    s->st.status = reinterpret_cast<int32_t*>(b); b += 4 * n;
+    s->st.outer = reinterpret_cast<int32_t*>(b); b += 4 * n;
+    s->st.tk1 = reinterpret_cast<unsigned*>(b); b += 4 * n;
+    s->st.tk2 = reinterpret_cast<unsigned*>(b); b += 4 * n;
+    CMCG_CUDA(cudaMemsetAsync(s->st_ws, 0, need, s->A->pat->ctx->stream));
+    s->st_inst = n_inst;
+    // the cached graph points at the old state
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+    s->gkey.clear();
+    return CMCG_OK;
+}
+
+int32_t choose_path(cmcg_solver s, int32_t n_inst) {
+    if (s->path != CMCG_PATH_AUTO) return s->path;
+    const int sms = s->A->pat->ctx->sm_count;
+    // many independent systems of moderate size: one CTA per system
+    if (s->max_sys_rows <= 65536 && n_inst >= sms) return CMCG_PATH_PERSISTENT;
+    return CMCG_PATH_GRID;
+}
+
+template <typename VT, typename MT>
+SolveArgs<VT, MT> base_args(cmcg_solver s, int32_t ob) {
+    cmcg_pattern p = s->A->pat;
+    SolveArgs<VT, MT> a{};
+    a.m = mat_args<MT>(s->A);
+    a.rows = p->rows;
+    a.n_sys = s->n_sys;
+    a.ob = ob;
+    a.row_off = p->d_row_off;
+    a.order = s->d_order;
+    a.next = s->counters;
+    a.active = s->counters + 1;
+    a.loops = s->counters + 2;
+    a.n_tiles = s->n_tiles;
+    a.tile_row0 = s->d_tile_row0;
+    a.tile_sys = s->d_tile_sys;
+    a.sys_tile_begin = s->d_sys_tile_begin;
+    a.tol = s->tol;
+    a.max_iter = s->max_iter;
+    a.st = s->st;
+    return a;
+}
+
+template <typename VT, typename MT, int FMT>
+cmcg_status run_persistent(cmcg_solver s, SolveArgs<VT, MT>& a) {
+    cmcg_ctx ctx = s->A->pat->ctx;
+    int occ = 0;
+    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persistent_cg<VT, MT, FMT>, kPersistThreads, 0));
+    const int n_inst = a.n_sys * a.ob;
+    const int grid = std::max(1, std::min(n_inst, ctx->sm_count * std::max(occ, 1)));
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+    k_persistent_cg<VT, MT, FMT><<<grid, kPersistThreads, 0, ctx->stream>>>(a);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+template <typename VT, typename MT, int FMT>
+cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
+    cmcg_ctx ctx = s->A->pat->ctx;
+    cudaStream_t st = ctx->stream;
+    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
+    int occ = 0;
+    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_grid_spmv_pq<VT, MT, FMT>, kTile, 0));
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, static_cast<int64_t>(ctx->sm_count) * std::max(occ, 1))));
+    const size_t need = 2 * sizeof(VT) * static_cast<size_t>(items) + 64;
+    if (s->part_ws_bytes < need) {
+        CMCG_TRY(ensure_buffer(&s->part_ws, &s->part_ws_bytes, need));
+        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+        if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+        s->gkey.clear();
+    }
+    a.part1 = static_cast<VT*>(s->part_ws);
+    a.part2 = a.part1 + items;
+    int64_t cap = 0;
+    if (s->max_iter >= 0) cap = s->max_iter;
+    else cap = 2 * static_cast<int64_t>(s->max_sys_rows);
+    a.loop_cap = static_cast<int32_t>(std::min<int64_t>(cap + 2, INT32_MAX - 1));
+
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), st));
+    k_grid_init<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+    k_grid_init2<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+    count_launch(2);
+    CMCG_CHECK_LAUNCH();
+
+    // graph with a WHILE node over the three iteration kernels; rebuilt when any
+    // kernel argument changes
+    std::vector<char> key(sizeof(a) + sizeof(int) * 2);
+    {
+        SolveArgs<VT, MT> k = a;
+        k.cond = 0;
+        std::memcpy(key.data(), &k, sizeof(k));
+        const int ids[2] = {DT<VT>::id, FMT};
+        std::memcpy(key.data() + sizeof(k), ids, sizeof(ids));
+    }
+    if (!s->gexec || key != s->gkey) {
+        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+        if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+        cudaGraph_t g;
+        CMCG_CUDA(cudaGraphCreate(&g, 0));
+        s->graph = g;
+        cudaGraphConditionalHandle h;
+        CMCG_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CMCG_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        a.cond = h;
+        CMCG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+        k_grid_update<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+        k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+        k_grid_cond<<<1, 1, 0, st>>>(a.active, a.loops, a.loop_cap, h);
+        cudaGraph_t captured = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(st, &captured);
+        if (ce != cudaSuccess) return cuda_fail(ce, "capture of the CG iteration", __FILE__, __LINE__);
+        CMCG_CUDA(cudaGraphInstantiate(&s->gexec, g, 0));
+        s->gkey = key;
+    }
+    CMCG_CUDA(cudaGraphLaunch(s->gexec, st));
+    // kernels inside the graph: 4 per executed iteration (counted as launched
+    // by the graph, not by the host)
+    count_launch(1);
+    return CMCG_OK;
+}
+
+cmcg_status ensure_vec_ws(cmcg_solver s, size_t bytes) {
+    if (s->vec_ws_bytes >= bytes && s->vec_ws) return CMCG_OK;
+    CMCG_TRY(ensure_buffer(&s->vec_ws, &s->vec_ws_bytes, bytes));
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+    s->gkey.clear();
+    return CMCG_OK;
+}
+
+template <typename VT, typename MT, int FMT>
+cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT* x, int32_t ob) {
+    cmcg_pattern p = s->A->pat;
+    cmcg_ctx ctx = p->ctx;
+    const int32_t n_inst = ob * s->n_sys;
+    CMCG_TRY(ensure_state(s, n_inst));
+    const void* dinv = nullptr;
+    CMCG_TRY(get_dinv(s, DT<VT>::id, &dinv));
+    const int32_t path = choose_path(s, n_inst);
+    const size_t vbytes = sizeof(VT) * static_cast<size_t>(p->rows) * ob;
+    SolveArgs<VT, MT> a = base_args<VT, MT>(s, ob);
+    a.dinv = static_cast<const VT*>(dinv);
+    a.dinv_b = s->A->batches;
+    if (path == CMCG_PATH_PERSISTENT) {
+        CMCG_TRY(ensure_vec_ws(s, 3 * vbytes + 256));
+        VT* w = static_cast<VT*>(s->vec_ws);
+        a.b = b; a.b_b = b_b; a.guess = guess; a.g_b = ob; a.x = x;
+        a.r = w; a.p = w + p->rows * static_cast<size_t>(ob); a.q = a.p + p->rows * static_cast<size_t>(ob);
+        CMCG_TRY((run_persistent<VT, MT, FMT>(s, a)));
+    } else {
+        // the graph iterates on internal copies of x so that its arguments do not
+        // depend on the caller's buffers
+        CMCG_TRY(ensure_vec_ws(s, 4 * vbytes + 256));
+        VT* w = static_cast<VT*>(s->vec_ws);
+        const size_t nv = p->rows * static_cast<size_t>(ob);
+        a.r = w; a.p = w + nv; a.q = w + 2 * nv; a.x = w + 3 * nv;
+        a.b = b; a.b_b = b_b; a.guess = guess; a.g_b = ob;
+        CMCG_TRY((run_grid<VT, MT, FMT>(s, a)));
+        const int fb = (n_inst + 255) / 256;
+        k_finalize<<<fb, 256, 0, ctx->stream>>>(s->st, n_inst);
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        CMCG_CUDA(cudaMemcpyAsync(x, a.x, vbytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    s->last_inst = n_inst;
+    s->last_refined = false;
+    return CMCG_OK;
+}
+
+template <typename VT>
+cmcg_status solve_vt(cmcg_solver s, const VT* b, int32_t b_b, const VT* g, VT* x, int32_t ob) {
+    const int fmt = s->A->pat->format;
+    switch (s->A->dtype) {
+        case CMCG_F32:
+            return fmt == CMCG_CSR ? solve_t<VT, float, CMCG_CSR>(s, b, b_b, g, x, ob) : solve_t<VT, float, CMCG_ELLPACK>(s, b, b_b, g, x, ob);
+        case CMCG_F64:
+            return fmt == CMCG_CSR ? solve_t<VT, double, CMCG_CSR>(s, b, b_b, g, x, ob) : solve_t<VT, double, CMCG_ELLPACK>(s, b, b_b, g, x, ob);
+        case CMCG_BF16:
+            return fmt == CMCG_CSR ? solve_t<VT, __nv_bfloat16, CMCG_CSR>(s, b, b_b, g, x, ob)
+                                   : solve_t<VT, __nv_bfloat16, CMCG_ELLPACK>(s, b, b_b, g, x, ob);
+    }
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "unsupported matrix dtype");
+}
+
+// ---- refined solve ----------------------------------------------------------------
+
+template <typename MI, typename MO, int FMT>
+cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_b, double* x, int32_t ob,
+                               double outer_tol, int32_t max_outer) {
+    cmcg_pattern p = s->A->pat;
+    cmcg_ctx ctx = p->ctx;
+    const int32_t n_inst = ob * s->n_sys;
+    CMCG_TRY(ensure_state(s, n_inst));
+    const void* dinv = nullptr;
+    CMCG_TRY(get_dinv(s, CMCG_F32, &dinv));
+    const size_t nv = static_cast<size_t>(p->rows) * ob;
+    CMCG_TRY(ensure_buffer(&s->ref_ws, &s->ref_ws_bytes, 5 * nv * sizeof(float) + 256));
+    float* w = static_cast<float*>(s->ref_ws);
+    RefineArgs<MI, MO> a{};
+    a.inner = mat_args<MI>(s->A);
+    a.outer = mat_args<MO>(Ao);
+    a.rows = p->rows;
+    a.n_sys = s->n_sys;
+    a.ob = ob;
+    a.row_off = p->d_row_off;
+    a.order = s->d_order;
+    a.next = s->counters;
+    a.dinv = static_cast<const float*>(dinv);
+    a.dinv_b = s->A->batches;
+    a.b = b;
+    a.b_b = b_b;
+    a.x = x;
+    a.r32 = w; a.d32 = w + nv; a.r = w + 2 * nv; a.p = w + 3 * nv; a.q = w + 4 * nv;
+    a.inner_tol = s->tol;
+    a.outer_tol = outer_tol;
+    a.max_inner = s->max_iter;
+    a.max_outer = max_outer;
+    a.st = s->st;
+    int occ = 0;
+    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persistent_refined<MI, MO, FMT>, kPersistThreads, 0));
+    const int grid = std::max(1, std::min(n_inst, ctx->sm_count * std::max(occ, 1)));
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+    k_persistent_refined<MI, MO, FMT><<<grid, kPersistThreads, 0, ctx->stream>>>(a);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    s->last_inst = n_inst;
+    s->last_refined = true;
+    return CMCG_OK;
+}
+
+// FP64 residual r = b - A x (values of Ao) into r32 (rounded) and per-system
+// |r|^2 / |b|^2, for the host-driven refinement of the grid path.
+__global__ void k_axpy_f32_to_f64(double* __restrict__ x, const float* __restrict__ d, int64_t n) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        x[i] += static_cast<double>(d[i]);
+}
+__global__ void k_sub_round(const double* __restrict__ b, int32_t b_b, const double* __restrict__ ax, float* __restrict__ r32,
+                            double* __restrict__ r64, int32_t rows, int64_t n) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double bi = b[b_b == 1 ? (i % rows) : i];
+        const double ri = bi - ax[i];
+        r64[i] = ri;
+        r32[i] = static_cast<float>(ri);
+    }
+}
+
+cmcg_status refined_grid(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_b, double* x, int32_t ob,
+                         double outer_tol, int32_t max_outer) {
+    // Host-driven outer loop for large systems: one sync per refinement step.
+    // Supports a single system per batch (the grid path's use case).
+    cmcg_pattern p = s->A->pat;
+    cmcg_ctx ctx = p->ctx;
+    cudaStream_t st = ctx->stream;
+    const size_t nv = static_cast<size_t>(p->rows) * ob;
+    const int32_t n_inst = ob * s->n_sys;
+    // buffers: r64, ax (FP64) + r32, d32 (FP32) + norms
+    void* buf = nullptr;
+    CMCG_TRY(dev_alloc(&buf, nv * (8 + 8 + 4 + 4) + 2 * 8 * static_cast<size_t>(ob) + 512));
+    double* r64 = static_cast<double*>(buf);
+    double* ax = r64 + nv;
+    float* r32 = reinterpret_cast<float*>(ax + nv);
+    float* d32 = r32 + nv;
+    double* nrm = reinterpret_cast<double*>(d32 + nv + 64);
+    auto cleanup = [&](cmcg_status code) { cudaStreamSynchronize(st); dev_free(buf); return code; };
+    cmcg_status rc;
+    const int blocks = ctx->sm_count * 8;
+    std::vector<double> hb(ob), hr(ob);
+    std::vector<int32_t> outer(n_inst, 0), it_tot(n_inst, 0), status(n_inst, ST_RUNNING);
+    if (cudaMemsetAsync(x, 0, nv * 8, st) != cudaSuccess) return cleanup(fail(CMCG_ERR_CUDA, "memset x"));
+    // |b|^2 per batch (b broadcast when b_b == 1)
+    if ((rc = dot_dispatch(ctx, CMCG_F64, p->rows, b, b_b, b, b_b, nrm, b_b)) != CMCG_OK) return cleanup(rc);
+    if (cudaMemcpyAsync(hb.data(), nrm, 8 * b_b, cudaMemcpyDeviceToHost, st) != cudaSuccess) return cleanup(fail(CMCG_ERR_CUDA, "D2H"));
+    if (cudaStreamSynchronize(st) != cudaSuccess) return cleanup(fail(CMCG_ERR_CUDA, "sync"));
+    for (int32_t i = b_b; i < ob; ++i) hb[i] = hb[0];
+    {
+        // x == 0: r = b
+        const int32_t bb = b_b;
+        for (int32_t i = 0; i < ob; ++i) {
+            const double* src = b + (bb == 1 ? 0 : static_cast<size_t>(i) * p->rows);
+            if (cudaMemcpyAsync(r64 + static_cast<size_t>(i) * p->rows, src, 8 * p->rows, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                return cleanup(fail(CMCG_ERR_CUDA, "copy b"));
+        }
+        if ((rc = convert(ctx, CMCG_F64, r64, CMCG_F32, r32, static_cast<int64_t>(nv))) != CMCG_OK) return cleanup(rc);
+    }
+    for (int32_t i = 0; i < ob; ++i) hr[i] = hb[i];
+    for (int32_t step = 0;; ++step) {
+        bool all_done = true;
+        for (int32_t i = 0; i < ob; ++i) {
+            if (status[i] != ST_RUNNING) continue;
+            if (hb[i] == 0.0) status[i] = CMCG_SOLVE_ZERO_RHS;
+            else if (!std::isfinite(hr[i])) status[i] = CMCG_SOLVE_NON_FINITE;
+            else if (hr[i] < outer_tol * outer_tol * hb[i]) status[i] = CMCG_SOLVE_CONVERGED;
+            else if (step >= max_outer) status[i] = CMCG_SOLVE_MAX_ITER;
+            else all_done = false;
+        }
+        if (all_done) break;
+        // inner solve A d = r32 (FP32) on the grid path
+        const int32_t saved = s->path;
+        s->path = CMCG_PATH_GRID;
+        rc = solve_vt<float>(s, r32, ob, nullptr, d32, ob);
+        s->path = saved;
+        if (rc != CMCG_OK) return cleanup(rc);
+        std::vector<int32_t> it(n_inst);
+        if (cudaMemcpyAsync(it.data(), s->st.it, 4 * n_inst, cudaMemcpyDeviceToHost, st) != cudaSuccess) return cleanup(fail(CMCG_ERR_CUDA, "D2H"));
+        k_axpy_f32_to_f64<<<blocks, 256, 0, st>>>(x, d32, static_cast<int64_t>(nv));
+        count_launch();
+        if ((rc = spmv_dispatch(Ao, CMCG_F64, x, ob, ax, CMCG_ASSIGN)) != CMCG_OK) return cleanup(rc);
+        k_sub_round<<<blocks, 256, 0, st>>>(b, b_b, ax, r32, r64, p->rows, static_cast<int64_t>(nv));
+        count_launch();
+        if ((rc = dot_dispatch(ctx, CMCG_F64, p->rows, r64, ob, r64, ob, nrm, ob)) != CMCG_OK) return cleanup(rc);
+        if (cudaMemcpyAsync(hr.data(), nrm, 8 * ob, cudaMemcpyDeviceToHost, st) != cudaSuccess) return cleanup(fail(CMCG_ERR_CUDA, "D2H"));
+        if (cudaStreamSynchronize(st) != cudaSuccess) return cleanup(fail(CMCG_ERR_CUDA, "refinement step"));
+        for (int32_t i = 0; i < ob; ++i)
+            if (status[i] == ST_RUNNING) { outer[i]++; it_tot[i] += it[i]; }
+    }
+    // publish stats in the instance state
+    std::vector<double> err(n_inst), rrv(n_inst), bbv(n_inst);
+    for (int32_t i = 0; i < n_inst; ++i) {
+        err[i] = status[i] == CMCG_SOLVE_ZERO_RHS ? 0.0 : std::sqrt(hr[i] / hb[i]);
+        rrv[i] = hr[i];
+        bbv[i] = hb[i];
+    }
+    if (cudaMemcpyAsync(s->st.err, err.data(), 8 * n_inst, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->st.rr, rrv.data(), 8 * n_inst, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->st.bb, bbv.data(), 8 * n_inst, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->st.it, it_tot.data(), 4 * n_inst, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->st.outer, outer.data(), 4 * n_inst, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->st.status, status.data(), 4 * n_inst, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return cleanup(fail(CMCG_ERR_CUDA, "stats upload"));
+    s->last_inst = n_inst;
+    s->last_refined = true;
+    return cleanup(CMCG_OK);
+}
+
+template <typename MI, int FMT>
+cmcg_status refined_mi(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_b, double* x, int32_t ob, double ot,
+                       int32_t mo) {
+    if (Ao->dtype == CMCG_F32) return refined_persistent<MI, float, FMT>(s, Ao, b, b_b, x, ob, ot, mo);
+    if (Ao->dtype == CMCG_F64) return refined_persistent<MI, double, FMT>(s, Ao, b, b_b, x, ob, ot, mo);
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "refined solve: the outer matrix must be F32 or F64");
+}
+
+}  // namespace
+
+extern "C" {
+
+cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
+    CMCG_REQUIRE(A && out, "cmcg_cg_create: NULL argument");
+    *out = nullptr;
+    CMCG_REQUIRE(A->pat->rows == A->pat->cols, "cmcg_cg_create: matrix must be square");
+    CMCG_REQUIRE(precond == CMCG_PRECOND_IDENTITY || precond == CMCG_PRECOND_JACOBI, "cmcg_cg_create: bad preconditioner");
+    CMCG_CUDA(cudaSetDevice(A->pat->ctx->device));
+    auto* s = new cmcg_solver_s();
+    s->A = A;
+    s->precond = precond;
+    // default tolerance: epsilon of the scalar type (IterativeSolverBase.h:131)
+    s->tol = (A->dtype == CMCG_F64) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+    cmcg_status st = build_plan(s);
+    if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);
+    if (st == CMCG_OK && cudaMemsetAsync(s->counters, 0, 64, A->pat->ctx->stream) != cudaSuccess) st = fail(CMCG_ERR_CUDA, "memset");
+    if (st != CMCG_OK) { cmcg_cg_destroy(s); return st; }
+    // Jacobi is extracted at construction like the reference's DiagonalPreconditioner(A)
+    if (precond == CMCG_PRECOND_JACOBI) {
+        const void* d;
+        st = get_dinv(s, A->dtype == CMCG_F64 ? CMCG_F64 : CMCG_F32, &d);
+        if (st != CMCG_OK) { cmcg_cg_destroy(s); return st; }
+    }
+    *out = s;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_destroy(cmcg_solver s) {
+    if (!s) return CMCG_OK;
+    cudaSetDevice(s->A->pat->ctx->device);
+    cudaStreamSynchronize(s->A->pat->ctx->stream);
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_tile_sys),
+                    static_cast<void*>(s->d_sys_tile_begin), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
+                    s->st_ws, static_cast<void*>(s->counters)})
+        dev_free(p);
+    if (s->host_io) cudaFreeHost(s->host_io);
+    delete s;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_set_tolerance(cmcg_solver s, double tol) {
+    CMCG_REQUIRE(s, "cmcg_cg_set_tolerance: NULL solver");
+    CMCG_REQUIRE(tol >= 0.0 && std::isfinite(tol), "cmcg_cg_set_tolerance: tolerance must be finite and >= 0");
+    s->tol = tol;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_set_max_iterations(cmcg_solver s, int64_t max_iter) {
+    CMCG_REQUIRE(s, "cmcg_cg_set_max_iterations: NULL solver");
+    CMCG_REQUIRE(max_iter < INT32_MAX, "cmcg_cg_set_max_iterations: too large");
+    s->max_iter = max_iter < 0 ? -1 : max_iter;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_get_settings(cmcg_solver s, double* tol, int64_t* max_iter) {
+    CMCG_REQUIRE(s, "cmcg_cg_get_settings: NULL solver");
+    if (tol) *tol = s->tol;
+    if (max_iter) *max_iter = s->max_iter < 0 ? 2 * static_cast<int64_t>(s->max_sys_rows) : s->max_iter;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_set_path(cmcg_solver s, int32_t path) {
+    CMCG_REQUIRE(s, "cmcg_cg_set_path: NULL solver");
+    CMCG_REQUIRE(path == CMCG_PATH_AUTO || path == CMCG_PATH_PERSISTENT || path == CMCG_PATH_GRID, "cmcg_cg_set_path: bad path");
+    s->path = path;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_solve(cmcg_solver s, int32_t vdt, const void* b, int32_t b_batches, const void* guess, void* x) {
+    CMCG_REQUIRE(s && b && x, "cmcg_cg_solve: NULL argument");
+    CMCG_REQUIRE(b_batches >= 1, "cmcg_cg_solve: b_batches must be >= 1");
+    CMCG_REQUIRE(s->A->batches == 1 || b_batches == 1 || b_batches == s->A->batches,
+                 "cmcg_cg_solve: batch counts of matrix and rhs must match or be 1");
+    const int32_t ob = std::max(s->A->batches, b_batches);
+    CMCG_REQUIRE(static_cast<int64_t>(ob) * s->n_sys <= INT32_MAX / 2, "cmcg_cg_solve: too many systems");
+    CMCG_CUDA(cudaSetDevice(s->A->pat->ctx->device));
+    if (vdt == CMCG_F32)
+        return solve_vt<float>(s, static_cast<const float*>(b), b_batches, static_cast<const float*>(guess), static_cast<float*>(x), ob);
+    if (vdt == CMCG_F64)
+        return solve_vt<double>(s, static_cast<const double*>(b), b_batches, static_cast<const double*>(guess), static_cast<double*>(x), ob);
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "cmcg_cg_solve: vector dtype must be F32 or F64");
+}
+
+cmcg_status cmcg_cg_solve_host(cmcg_solver s, int32_t vdt, const void* b_host, int32_t b_batches, const void* guess_host,
+                               void* x_host) {
+    CMCG_REQUIRE(s && b_host && x_host, "cmcg_cg_solve_host: NULL argument");
+    CMCG_REQUIRE(vdt == CMCG_F32 || vdt == CMCG_F64, "cmcg_cg_solve_host: vector dtype must be F32 or F64");
+    CMCG_REQUIRE(b_batches >= 1, "cmcg_cg_solve_host: b_batches must be >= 1");
+    cmcg_ctx ctx = s->A->pat->ctx;
+    CMCG_CUDA(cudaSetDevice(ctx->device));
+    const int32_t ob = std::max(s->A->batches, b_batches);
+    const size_t es = dtype_size(vdt);
+    const size_t nb = es * s->A->pat->rows * static_cast<size_t>(b_batches);
+    const size_t nx = es * s->A->pat->rows * static_cast<size_t>(ob);
+    // device staging: b | guess | x
+    void* dbuf = nullptr;
+    CMCG_TRY(dev_alloc(&dbuf, nb + 2 * nx + 512));
+    char* db = static_cast<char*>(dbuf);
+    char* dg = db + ((nb + 255) / 256) * 256;
+    char* dx = dg + ((nx + 255) / 256) * 256;
+    cudaStream_t st = ctx->stream;
+    cmcg_status rc = CMCG_OK;
+    if (cudaMemcpyAsync(db, b_host, nb, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = fail(CMCG_ERR_CUDA, "upload b");
+    if (rc == CMCG_OK && guess_host && cudaMemcpyAsync(dg, guess_host, nx, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        rc = fail(CMCG_ERR_CUDA, "upload guess");
+    if (rc == CMCG_OK) rc = cmcg_cg_solve(s, vdt, db, b_batches, guess_host ? dg : nullptr, dx);
+    if (rc == CMCG_OK && cudaMemcpyAsync(x_host, dx, nx, cudaMemcpyDeviceToHost, st) != cudaSuccess) rc = fail(CMCG_ERR_CUDA, "download x");
+    if (cudaStreamSynchronize(st) != cudaSuccess && rc == CMCG_OK) rc = fail(CMCG_ERR_CUDA, "solve failed");
+    dev_free(dbuf);
+    return rc;
+}
+
+static cmcg_status fetch_stats(cmcg_solver s, std::vector<int32_t>* it, std::vector<double>* err, std::vector<int32_t>* st,
+                               std::vector<int32_t>* outer) {
+    CMCG_REQUIRE(s->last_inst > 0, "no solve has been run");
+    cudaStream_t stream = s->A->pat->ctx->stream;
+    CMCG_CUDA(cudaStreamSynchronize(stream));
+    const size_t n = s->last_inst;
+    if (it) { it->resize(n); CMCG_CUDA(cudaMemcpy(it->data(), s->st.it, 4 * n, cudaMemcpyDeviceToHost)); }
+    if (err) { err->resize(n); CMCG_CUDA(cudaMemcpy(err->data(), s->st.err, 8 * n, cudaMemcpyDeviceToHost)); }
+    if (st) { st->resize(n); CMCG_CUDA(cudaMemcpy(st->data(), s->st.status, 4 * n, cudaMemcpyDeviceToHost)); }
+    if (outer) { outer->resize(n); CMCG_CUDA(cudaMemcpy(outer->data(), s->st.outer, 4 * n, cudaMemcpyDeviceToHost)); }
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_iterations(cmcg_solver s, int64_t* iterations) {
+    CMCG_REQUIRE(s && iterations, "cmcg_cg_iterations: NULL argument");
+    std::vector<int32_t> it;
+    CMCG_TRY(fetch_stats(s, &it, nullptr, nullptr, nullptr));
+    *iterations = it.empty() ? 0 : *std::max_element(it.begin(), it.end());
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_error(cmcg_solver s, double* error) {
+    CMCG_REQUIRE(s && error, "cmcg_cg_error: NULL argument");
+    std::vector<double> e;
+    CMCG_TRY(fetch_stats(s, nullptr, &e, nullptr, nullptr));
+    double m = 0.0;
+    for (double v : e) m = (std::isnan(v) || std::isnan(m)) ? NAN : std::max(m, v);
+    *error = m;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_system_stats(cmcg_solver s, int32_t* iters, double* err, int32_t* status, int32_t* outer) {
+    CMCG_REQUIRE(s, "cmcg_cg_system_stats: NULL solver");
+    std::vector<int32_t> it, st, ou;
+    std::vector<double> e;
+    CMCG_TRY(fetch_stats(s, iters ? &it : nullptr, err ? &e : nullptr, status ? &st : nullptr, outer ? &ou : nullptr));
+    if (iters) std::copy(it.begin(), it.end(), iters);
+    if (err) std::copy(e.begin(), e.end(), err);
+    if (status) std::copy(st.begin(), st.end(), status);
+    if (outer) std::copy(ou.begin(), ou.end(), outer);
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_batches, double* x,
+                                  double outer_tol, int32_t max_outer) {
+    CMCG_REQUIRE(s && b && x, "cmcg_cg_solve_refined: NULL argument");
+    if (!Ao) Ao = s->A;
+    CMCG_REQUIRE(Ao->pat == s->A->pat, "cmcg_cg_solve_refined: outer matrix must share the solver's pattern");
+    CMCG_REQUIRE(Ao->batches == s->A->batches, "cmcg_cg_solve_refined: outer matrix batch count differs");
+    CMCG_REQUIRE(Ao->dtype == CMCG_F32 || Ao->dtype == CMCG_F64, "cmcg_cg_solve_refined: outer values must be F32 or F64");
+    CMCG_REQUIRE(s->A->dtype == CMCG_F32 || s->A->dtype == CMCG_BF16, "cmcg_cg_solve_refined: inner values must be F32 or BF16");
+    CMCG_REQUIRE(outer_tol > 0.0 && max_outer >= 1, "cmcg_cg_solve_refined: need outer_tol > 0 and max_outer >= 1");
+    CMCG_REQUIRE(b_batches >= 1 && (s->A->batches == 1 || b_batches == 1 || b_batches == s->A->batches),
+                 "cmcg_cg_solve_refined: batch counts must match or be 1");
+    CMCG_CUDA(cudaSetDevice(s->A->pat->ctx->device));
+    const int32_t ob = std::max(s->A->batches, b_batches);
+    const int32_t path = choose_path(s, ob * s->n_sys);
+    if (path == CMCG_PATH_GRID) {
+        CMCG_REQUIRE(s->n_sys == 1, "cmcg_cg_solve_refined: the grid path refines one system per batch");
+        return refined_grid(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
+    }
+    const int fmt = s->A->pat->format;
+    if (s->A->dtype == CMCG_F32)
+        return fmt == CMCG_CSR ? refined_mi<float, CMCG_CSR>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer)
+                               : refined_mi<float, CMCG_ELLPACK>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
+    return fmt == CMCG_CSR ? refined_mi<__nv_bfloat16, CMCG_CSR>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer)
+                           : refined_mi<__nv_bfloat16, CMCG_ELLPACK>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
+}
+
+cmcg_status cmcg_cg_adjoint(cmcg_solver s, cmcg_matrix Ao, const double* x, const double* gx, int32_t batches, double* gb,
+                            double* gA, double outer_tol, int32_t max_outer) {
+    CMCG_REQUIRE(s && x && gx && gb, "cmcg_cg_adjoint: NULL argument");
+    // A symmetric: A^T lambda = gx is A lambda = gx, solved by the same fused CG
+    CMCG_TRY(cmcg_cg_solve_refined(s, Ao, gx, batches, gb, outer_tol, max_outer));
+    if (gA) {
+        // dL/dA_ij = -lambda_i x_j on the pattern (one sampled outer product)
+        const int32_t ob = std::max(s->A->batches, batches);
+        CMCG_TRY(sddmm_dispatch(s->A, CMCG_F64, -1.0, gb, ob, x, ob, gA, ob));
+    }
+    return CMCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,322 @@
+// Stand-alone sparse products and batched reductions behind the C ABI.
+//
+//  cmcg_spmv          replaces ProductAssignment<... SparseMatrix<CSR|ELLPACK> ...>
+//                     (cuMat/src/SparseProductEvaluation.h:95-139, :232-276) and their
+//                     thread-per-row kernels (:43-88, :194-226)
+//  cmcg_dot,
+//  cmcg_squared_norm  replace dot / squaredNorm (cuMat/src/ReductionOpsPlugin.inl:279-315),
+//                     which run CUB DeviceReduce / segmented reductions with a
+//                     temporary allocation per call (ReductionOps.h:563-598)
+//  cmcg_sddmm         replaces the sparse outer product on a pattern
+//                     (SparseProductEvaluation.h:16-37 + SparseEvaluation.h:15-34)
+//
+// Design: CSR rows are processed in 32-row blocks per warp with 16-byte loads
+// of the block's contiguous entries (warp_csr_rows); ELLPACK is thread per row
+// over the column-major slabs. Reductions are warp shuffles, one partial per
+// CTA and a single deterministic combine by the last CTA of each batch (ticket
+// counter, no spinning).
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "objects.h"
+#include "spmv_dev.cuh"
+
+namespace cmcg {
+namespace {
+
+constexpr int kSpmvThreads = 256;
+
+template <int MODE, typename VT>
+__device__ __forceinline__ void assign_out(VT* y, VT v) {
+    if (MODE == CMCG_ASSIGN) *y = v;
+    else if (MODE == CMCG_ADD) *y += v;
+    else *y -= v;
+}
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                           const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                           const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                           VT* __restrict__ y, int32_t rows, int32_t ob) {
+    __shared__ WarpStage<VT> stage[kSpmvThreads / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nblk = (rows + 31) >> 5;
+    const int64_t items = static_cast<int64_t>(nblk) * ob;
+    const int64_t wstride = static_cast<int64_t>(gridDim.x) * (kSpmvThreads / 32);
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * (kSpmvThreads / 32) + warp; it < items; it += wstride) {
+        const int b = static_cast<int>(it / nblk);
+        const int r0 = static_cast<int>(it - static_cast<int64_t>(b) * nblk) * 32;
+        const int nr = min(32, rows - r0);
+        CsrView<MT> A{rp, ci, vals + (mb == 1 ? 0 : b * vstride)};
+        GlobalX<VT> xf{x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols)};
+        const VT v = warp_csr_rows<VT>(A, r0, nr, xf, stage[warp]);
+        if (lane < nr) assign_out<MODE>(y + static_cast<int64_t>(b) * rows + r0 + lane, v);
+    }
+}
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell(const int32_t* __restrict__ idx, int32_t width, int32_t rows_pad,
+                                                           const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                           const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                           VT* __restrict__ y, int32_t rows, int32_t ob) {
+    const int64_t items = static_cast<int64_t>(rows) * ob;
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * kSpmvThreads) {
+        const int b = static_cast<int>(it / rows);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * rows);
+        EllView<MT> A{idx, vals + (mb == 1 ? 0 : b * vstride), width, rows_pad};
+        GlobalX<VT> xf{x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols)};
+        assign_out<MODE>(y + it, ell_row<VT>(A, r, xf));
+    }
+}
+
+template <typename MT, typename VT>
+cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode) {
+    cmcg_pattern p = A->pat;
+    cmcg_ctx ctx = p->ctx;
+    const int32_t ob = std::max(A->batches, xb);
+    const MT* vals = static_cast<const MT*>(A->d_vals);
+    const VT* xv = static_cast<const VT*>(x);
+    VT* yv = static_cast<VT*>(y);
+    const int max_blocks = ctx->sm_count * 8;
+    if (p->format == CMCG_CSR) {
+        const int64_t warps = static_cast<int64_t>((p->rows + 31) / 32) * ob;
+        const int blocks = static_cast<int>(std::min<int64_t>((warps + 7) / 8, max_blocks));
+#define CMCG_LAUNCH_CSR(M)                                                                                       \
+    k_spmv_csr<MT, VT, M><<<blocks, kSpmvThreads, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride,     \
+                                                                    A->batches, xv, p->cols, xb, yv, p->rows, ob)
+        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR(CMCG_ASSIGN);
+        else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR(CMCG_ADD);
+        else CMCG_LAUNCH_CSR(CMCG_SUB);
+#undef CMCG_LAUNCH_CSR
+    } else {
+        const int64_t threads = static_cast<int64_t>(p->rows) * ob;
+        const int blocks = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
+#define CMCG_LAUNCH_ELL(M)                                                                                      \
+    k_spmv_ell<MT, VT, M><<<blocks, kSpmvThreads, 0, ctx->stream>>>(p->d_ell, p->width, p->rows_pad, vals,       \
+                                                                    A->stride, A->batches, xv, p->cols, xb, yv,  \
+                                                                    p->rows, ob)
+        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_ELL(CMCG_ASSIGN);
+        else if (mode == CMCG_ADD) CMCG_LAUNCH_ELL(CMCG_ADD);
+        else CMCG_LAUNCH_ELL(CMCG_SUB);
+#undef CMCG_LAUNCH_ELL
+    }
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+// ---- batched dot / squared norm -------------------------------------------------
+
+constexpr int kRedThreads = 256;
+
+// grid (gx, ob): CTA (bx, b) sums a grid-stride slice of batch b; the last CTA
+// of batch b (ticket) adds the gx partials in index order and resets the ticket.
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_dot(int64_t n, const VT* __restrict__ x, int32_t xb,
+                                                     const VT* __restrict__ y, int32_t yb, VT* __restrict__ out,
+                                                     VT* __restrict__ partial, unsigned* __restrict__ ticket) {
+    __shared__ VT red[kRedThreads / 32];
+    __shared__ bool last;
+    const int b = blockIdx.y;
+    const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * n);
+    const VT* yv = y + (yb == 1 ? 0 : static_cast<int64_t>(b) * n);
+    VT acc[1] = {VT(0)};
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kRedThreads + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * kRedThreads)
+        acc[0] += __ldg(xv + i) * __ldg(yv + i);
+    block_sum<VT, 1>(acc, red);
+    if (threadIdx.x == 0) {
+        partial[static_cast<int64_t>(b) * gridDim.x + blockIdx.x] = acc[0];
+        __threadfence();
+        const unsigned t = atomicAdd(ticket + b, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    VT s[1] = {VT(0)};
+    const volatile VT* pv = partial + static_cast<int64_t>(b) * gridDim.x;
+    for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += kRedThreads) s[0] += pv[i];
+    block_sum<VT, 1>(s, red);
+    if (threadIdx.x == 0) {
+        out[b] = s[0];
+        ticket[b] = 0;
+    }
+}
+
+template <typename VT>
+cmcg_status launch_dot(cmcg_ctx ctx, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb, void* out,
+                       int32_t ob) {
+    const int64_t want = std::max<int64_t>(1, (n + kRedThreads * 4 - 1) / (kRedThreads * 4));
+    const int gx = static_cast<int>(std::min<int64_t>(want, std::max(1, (ctx->sm_count * 4) / std::max(1, ob) + 1)));
+    CMCG_TRY(ensure_buffer(&ctx->red_partial, &ctx->red_partial_bytes, static_cast<size_t>(gx) * ob * sizeof(VT)));
+    if (ctx->red_ticket_count < static_cast<size_t>(ob)) {
+        dev_free(ctx->red_ticket);
+        ctx->red_ticket = nullptr;
+        ctx->red_ticket_count = 0;
+        CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&ctx->red_ticket), ob * sizeof(unsigned)));
+        CMCG_CUDA(cudaMemsetAsync(ctx->red_ticket, 0, ob * sizeof(unsigned), ctx->stream));
+        ctx->red_ticket_count = ob;
+    }
+    dim3 grid(gx, ob);
+    k_dot<VT><<<grid, kRedThreads, 0, ctx->stream>>>(n, static_cast<const VT*>(x), xb, static_cast<const VT*>(y), yb,
+                                                     static_cast<VT*>(out), static_cast<VT*>(ctx->red_partial),
+                                                     ctx->red_ticket);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+// ---- sampled outer product on the pattern -----------------------------------------
+
+template <typename VT>
+__global__ void k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, int32_t rows, int32_t cols,
+                            int64_t vstride, VT alpha, const VT* __restrict__ u, int32_t ub, const VT* __restrict__ v,
+                            int32_t vb, VT* __restrict__ out, int32_t ob) {
+    // warp per 32-row block: lane-parallel over the block's contiguous entries,
+    // row of an entry found by a short search over the block's row bounds
+    __shared__ int32_t bounds[8][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nblk = (rows + 31) >> 5;
+    const int64_t items = static_cast<int64_t>(nblk) * ob;
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * 8 + warp; it < items; it += static_cast<int64_t>(gridDim.x) * 8) {
+        const int b = static_cast<int>(it / nblk);
+        const int r0 = static_cast<int>(it - static_cast<int64_t>(b) * nblk) * 32;
+        const int nr = min(32, rows - r0);
+        if (lane <= nr) bounds[warp][lane] = __ldg(rp + r0 + lane);
+        __syncwarp();
+        const int lo = bounds[warp][0], hi = bounds[warp][nr];
+        const VT* ub_ = u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows);
+        const VT* vb_ = v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        VT* ob_ = out + static_cast<int64_t>(b) * vstride;
+        for (int k = lo + lane; k < hi; k += 32) {
+            int a = 0, e = nr;  // find row j with bounds[j] <= k < bounds[j+1]
+            while (e - a > 1) {
+                const int m = (a + e) >> 1;
+                if (bounds[warp][m] <= k) a = m; else e = m;
+            }
+            ob_[k] = alpha * ub_[r0 + a] * vb_[__ldg(ci + k)];
+        }
+        __syncwarp();
+    }
+}
+
+template <typename VT>
+__global__ void k_sddmm_ell(const int32_t* __restrict__ idx, int32_t width, int32_t rows_pad, int32_t rows, int32_t cols,
+                            int64_t vstride, VT alpha, const VT* __restrict__ u, int32_t ub, const VT* __restrict__ v,
+                            int32_t vb, VT* __restrict__ out, int32_t ob) {
+    const int64_t per = static_cast<int64_t>(rows) * width;
+    const int64_t items = per * ob;
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(it / per);
+        const int64_t rem = it - b * per;
+        const int j = static_cast<int>(rem / rows);
+        const int r = static_cast<int>(rem - static_cast<int64_t>(j) * rows);
+        const int c = __ldg(idx + r + static_cast<int64_t>(j) * rows_pad);
+        const VT* ub_ = u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows);
+        const VT* vb_ = v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        // output in the caller's dense [batch][slot][row] layout
+        out[it] = (c >= 0) ? alpha * ub_[r] * vb_[c] : VT(0);
+    }
+}
+
+template <typename VT>
+cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub, const void* v, int32_t vb, void* out,
+                         int32_t ob) {
+    cmcg_pattern p = M->pat;
+    cmcg_ctx ctx = p->ctx;
+    if (p->format == CMCG_CSR) {
+        const int64_t warps = static_cast<int64_t>((p->rows + 31) / 32) * ob;
+        const int blocks = static_cast<int>(std::min<int64_t>((warps + 7) / 8, ctx->sm_count * 8));
+        k_sddmm_csr<VT><<<blocks, 256, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, p->rows, p->cols, p->nnz,
+                                                         static_cast<VT>(alpha), static_cast<const VT*>(u), ub,
+                                                         static_cast<const VT*>(v), vb, static_cast<VT*>(out), ob);
+    } else {
+        const int64_t n = p->nnz * ob;
+        const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, ctx->sm_count * 8));
+        k_sddmm_ell<VT><<<blocks, 256, 0, ctx->stream>>>(p->d_ell, p->width, p->rows_pad, p->rows, p->cols, p->nnz,
+                                                         static_cast<VT>(alpha), static_cast<const VT*>(u), ub,
+                                                         static_cast<const VT*>(v), vb, static_cast<VT*>(out), ob);
+    }
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+}  // namespace
+
+// Internal entry used by the solver (device pointers, no validation).
+cmcg_status spmv_dispatch(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t xb, void* y, int32_t mode) {
+    if (vec_dtype == CMCG_F32) {
+        switch (A->dtype) {
+            case CMCG_F32: return launch_spmv<float, float>(A, x, xb, y, mode);
+            case CMCG_BF16: return launch_spmv<__nv_bfloat16, float>(A, x, xb, y, mode);
+            case CMCG_F64: return launch_spmv<double, float>(A, x, xb, y, mode);
+        }
+    } else if (vec_dtype == CMCG_F64) {
+        switch (A->dtype) {
+            case CMCG_F32: return launch_spmv<float, double>(A, x, xb, y, mode);
+            case CMCG_BF16: return launch_spmv<__nv_bfloat16, double>(A, x, xb, y, mode);
+            case CMCG_F64: return launch_spmv<double, double>(A, x, xb, y, mode);
+        }
+    }
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "cmcg_spmv: vector dtype must be F32 or F64");
+}
+
+cmcg_status dot_dispatch(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb,
+                         void* out, int32_t ob) {
+    if (dtype == CMCG_F32) return launch_dot<float>(ctx, n, x, xb, y, yb, out, ob);
+    if (dtype == CMCG_F64) return launch_dot<double>(ctx, n, x, xb, y, yb, out, ob);
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "dot: dtype must be F32 or F64");
+}
+
+cmcg_status sddmm_dispatch(cmcg_matrix M, int32_t dt, double alpha, const void* u, int32_t ub, const void* v,
+                           int32_t vb, void* out, int32_t ob) {
+    if (dt == CMCG_F32) return launch_sddmm<float>(M, alpha, u, ub, v, vb, out, ob);
+    if (dt == CMCG_F64) return launch_sddmm<double>(M, alpha, u, ub, v, vb, out, ob);
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "sddmm: dtype must be F32 or F64");
+}
+
+}  // namespace cmcg
+
+using namespace cmcg;
+
+extern "C" {
+
+cmcg_status cmcg_spmv(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t x_batches, void* y, int32_t mode) {
+    CMCG_REQUIRE(A && x && y, "cmcg_spmv: NULL argument");
+    CMCG_REQUIRE(x_batches >= 1, "cmcg_spmv: x_batches must be >= 1");
+    CMCG_REQUIRE(A->batches == 1 || x_batches == 1 || A->batches == x_batches,
+                 "cmcg_spmv: batch counts of matrix and vector must match or be 1");
+    CMCG_REQUIRE(mode == CMCG_ASSIGN || mode == CMCG_ADD || mode == CMCG_SUB, "cmcg_spmv: bad assignment mode");
+    CMCG_CUDA(cudaSetDevice(A->pat->ctx->device));
+    return spmv_dispatch(A, vec_dtype, x, x_batches, y, mode);
+}
+
+cmcg_status cmcg_dot(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb,
+                     void* out) {
+    CMCG_REQUIRE(ctx && x && y && out, "cmcg_dot: NULL argument");
+    CMCG_REQUIRE(n >= 0 && xb >= 1 && yb >= 1, "cmcg_dot: bad size");
+    CMCG_REQUIRE(xb == 1 || yb == 1 || xb == yb, "cmcg_dot: batch counts must match or be 1");
+    CMCG_REQUIRE(std::max(xb, yb) <= 65535, "cmcg_dot: at most 65535 batches");
+    CMCG_CUDA(cudaSetDevice(ctx->device));
+    return dot_dispatch(ctx, dtype, n, x, xb, y, yb, out, std::max(xb, yb));
+}
+
+cmcg_status cmcg_squared_norm(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t batches, void* out) {
+    return cmcg_dot(ctx, dtype, n, x, batches, x, batches, out);
+}
+
+cmcg_status cmcg_sddmm(cmcg_matrix M, int32_t vec_dtype, double alpha, const void* u, int32_t ub, const void* v,
+                       int32_t vb, void* out, int32_t ob) {
+    CMCG_REQUIRE(M && u && v && out, "cmcg_sddmm: NULL argument");
+    CMCG_REQUIRE(ub >= 1 && vb >= 1 && ob >= 1, "cmcg_sddmm: batch counts must be >= 1");
+    CMCG_REQUIRE((ub == 1 || ub == ob) && (vb == 1 || vb == ob), "cmcg_sddmm: batch counts must match or be 1");
+    CMCG_CUDA(cudaSetDevice(M->pat->ctx->device));
+    return sddmm_dispatch(M, vec_dtype, alpha, u, ub, v, vb, out, ob);
+}
+
+}  // extern "C"

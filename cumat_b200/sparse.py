@@ -1,0 +1,291 @@
+"""Python mirror of cuMat's sparse / iterative-solver interface over the C ABI.
+
+Names and argument meanings follow the reference so that code and tests read
+like the reference's own (paths relative to the reference repository):
+
+* ``SparsityPattern``  - cuMat/src/SparseMatrixBase.h:29-206 (CSR: ``JA`` row
+  pointers, ``IA`` column indices; ELLPACK: ``indices`` column-major, -1 padding;
+  ``assertValid()``)
+* ``SparseMatrix``     - cuMat/src/SparseMatrix.h:48-414 (values ``[batch][nnz]``)
+* ``A * x``            - operator*, cuMat/src/ProductOp.h:519-524
+* ``dot`` / ``squaredNorm`` / ``norm`` - cuMat/src/ReductionOpsPlugin.inl:279-334
+* ``ConjugateGradient`` with ``DiagonalPreconditioner`` (default) or
+  ``IdentityPreconditioner`` - cuMat/src/ConjugateGradient.h:66-265,
+  cuMat/src/IterativeSolverBase.h:10-135
+
+Device vectors are torch tensors (torch provides device memory and the stream;
+all arithmetic runs in this package's CUDA library). Vectors are shaped
+``(n,)`` or ``(batches, n)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+CSR = N.CSR
+ELLPACK = N.ELLPACK
+
+_TORCH_DT = {torch.float32: N.F32, torch.float64: N.F64, torch.bfloat16: N.BF16}
+_NP_DT = {np.dtype(np.float32): N.F32, np.dtype(np.float64): N.F64}
+
+
+def _vp(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr()) if isinstance(t, torch.Tensor) else C.c_void_p(t)
+
+
+class Context:
+    """Device + stream, like cuMat::Context (cuMat/src/Context.h:132-214).
+
+    ``Context.current()`` binds the library to torch's current CUDA stream, so
+    torch-produced inputs and library kernels are ordered on one stream.
+    """
+
+    _per_device: dict = {}
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        self.device = device
+        h = C.c_void_p()
+        N.call("cmcg_ctx_create", device, C.c_void_p(stream) if stream else None, C.byref(h))
+        self.handle = h
+
+    @classmethod
+    def current(cls, device: Optional[int] = None) -> "Context":
+        if device is None:
+            device = torch.cuda.current_device()
+        stream = torch.cuda.current_stream(device).cuda_stream
+        key = (device, stream)
+        ctx = cls._per_device.get(key)
+        if ctx is None:
+            ctx = cls(device, stream)
+            cls._per_device[key] = ctx
+        return ctx
+
+    def synchronize(self) -> None:
+        N.call("cmcg_ctx_synchronize", self.handle)
+
+    @property
+    def torch_device(self) -> torch.device:
+        return torch.device("cuda", self.device)
+
+
+class SparsityPattern:
+    """Mirror of ``cuMat::SparsityPattern<CSR|ELLPACK>``; fill the fields, then
+    ``assertValid()`` validates and uploads (the reference's assertValid only
+    checks sizes; here malformed patterns raise ``CuMatError``)."""
+
+    def __init__(self, fmt: int = CSR):
+        self.format = fmt
+        self.rows = 0
+        self.cols = 0
+        self.nnz = 0            # CSR
+        self.IA = None          # CSR column indices (nnz)
+        self.JA = None          # CSR row pointers (rows + 1)
+        self.nnzPerRow = 0      # ELLPACK
+        self.indices = None     # ELLPACK (rows, nnzPerRow), -1 = padding
+        self.handle = None
+        self._ctx = None
+        self.row_off = None
+
+    # convenience constructors
+    @classmethod
+    def csr(cls, rows, cols, row_ptr, col_idx, ctx: Optional[Context] = None) -> "SparsityPattern":
+        p = cls(CSR)
+        p.rows, p.cols = int(rows), int(cols)
+        p.JA = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        p.IA = np.ascontiguousarray(col_idx, dtype=np.int32)
+        p.nnz = int(p.IA.size)
+        p.assertValid(ctx)
+        return p
+
+    @classmethod
+    def ell(cls, rows, cols, indices, ctx: Optional[Context] = None) -> "SparsityPattern":
+        """indices: (rows, nnzPerRow) array (any memory order)."""
+        p = cls(ELLPACK)
+        ind = np.asarray(indices, dtype=np.int32)
+        p.rows, p.cols = int(rows), int(cols)
+        p.nnzPerRow = int(ind.shape[1])
+        p.indices = ind
+        p.assertValid(ctx)
+        return p
+
+    def assertValid(self, ctx: Optional[Context] = None) -> None:
+        ctx = ctx or Context.current()
+        self._ctx = ctx
+        h = C.c_void_p()
+        if self.format == CSR:
+            ja = np.ascontiguousarray(self.JA, dtype=np.int32)
+            ia = np.ascontiguousarray(self.IA, dtype=np.int32)
+            if ja.size != self.rows + 1 or ia.size != self.nnz:
+                raise ValueError("SparsityPattern<CSR>: JA must have rows+1 and IA nnz entries")
+            N.call("cmcg_pattern_create_csr", ctx.handle, self.rows, self.cols, self.nnz,
+                   ja.ctypes.data_as(C.c_void_p), ia.ctypes.data_as(C.c_void_p) if ia.size else None, 0, C.byref(h))
+        else:
+            ind = np.asarray(self.indices, dtype=np.int32)
+            if ind.shape != (self.rows, self.nnzPerRow):
+                raise ValueError("SparsityPattern<ELLPACK>: indices must be rows x nnzPerRow")
+            colmajor = np.ascontiguousarray(ind.T)  # [slot][row]
+            N.call("cmcg_pattern_create_ell", ctx.handle, self.rows, self.cols, self.nnzPerRow,
+                   colmajor.ctypes.data_as(C.c_void_p), 0, C.byref(h))
+        self._release()
+        self.handle = h
+
+    def set_systems(self, row_off) -> None:
+        """Declares independent diagonal blocks (packed batch of systems)."""
+        ro = np.ascontiguousarray(row_off, dtype=np.int64)
+        N.call("cmcg_pattern_set_systems", self.handle, ro.size - 1, ro.ctypes.data_as(C.c_void_p))
+        self.row_off = ro
+
+    def getNNZ(self) -> int:
+        return self.nnz if self.format == CSR else self.rows * self.nnzPerRow
+
+    def download(self):
+        """Device copy of the index arrays: (JA, IA) for CSR, (rows, width) indices for ELLPACK."""
+        if self.format == CSR:
+            ja = np.empty(self.rows + 1, np.int32)
+            ia = np.empty(max(self.nnz, 1), np.int32)
+            N.call("cmcg_pattern_download", self.handle, ja.ctypes.data_as(C.c_void_p), ia.ctypes.data_as(C.c_void_p))
+            return ja, ia[: self.nnz]
+        out = np.empty((self.nnzPerRow, self.rows), np.int32)
+        N.call("cmcg_pattern_download", self.handle, out.ctypes.data_as(C.c_void_p), None)
+        return out.T.copy()
+
+    def _release(self):
+        if self.handle is not None:
+            N.lib.cmcg_pattern_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
+
+
+class SparseMatrix:
+    """Mirror of ``cuMat::SparseMatrix<Scalar, Batches, Flags>``: ``batches``
+    value sets on one shared pattern."""
+
+    def __init__(self, pattern: SparsityPattern, dtype=torch.float32, batches: int = 1):
+        if pattern.handle is None:
+            pattern.assertValid()
+        self.pattern = pattern
+        self.dtype = dtype
+        self.batches = int(batches)
+        h = C.c_void_p()
+        N.call("cmcg_matrix_create", pattern.handle, _TORCH_DT[dtype], self.batches, C.byref(h))
+        self.handle = h
+
+    @property
+    def rows(self) -> int:
+        return self.pattern.rows
+
+    @property
+    def cols(self) -> int:
+        return self.pattern.cols
+
+    def getSparsityPattern(self) -> SparsityPattern:
+        return self.pattern
+
+    def setData(self, values) -> "SparseMatrix":
+        """values: batch-major ``[batches][nnz]`` (CSR) or ``[batches][rows][width]``
+        / ``[rows][width]`` (ELLPACK, converted to the column-major layout).
+        numpy (host) or torch (host or device), F32 / F64 / BF16."""
+        if self.pattern.format == ELLPACK:
+            v = values if isinstance(values, torch.Tensor) else torch.as_tensor(np.asarray(values))
+            if v.dim() == 2:
+                v = v.unsqueeze(0)
+            v = v.transpose(1, 2).contiguous()  # [b][slot][row]
+            values = v
+        if isinstance(values, torch.Tensor):
+            t = values.contiguous()
+            if t.dtype not in _TORCH_DT:
+                t = t.to(torch.float64)
+            if t.numel() != self.batches * self.pattern.getNNZ():
+                raise ValueError("setData: expected batches * nnz values")
+            N.call("cmcg_matrix_set_values", self.handle, _TORCH_DT[t.dtype], _vp(t), 1 if t.is_cuda else 0)
+            if t.is_cuda:
+                self.pattern._ctx.synchronize()
+            return self
+        a = np.ascontiguousarray(values)
+        if a.dtype not in _NP_DT:
+            a = a.astype(np.float64)
+        if a.size != self.batches * self.pattern.getNNZ():
+            raise ValueError("setData: expected batches * nnz values")
+        N.call("cmcg_matrix_set_values", self.handle, _NP_DT[a.dtype], a.ctypes.data_as(C.c_void_p), 0)
+        return self
+
+    def getData(self) -> np.ndarray:
+        """Values as stored (F32 / F64; BF16 returned as float32), batch-major."""
+        n = self.batches * self.pattern.getNNZ()
+        if self.dtype == torch.bfloat16:
+            raw = np.empty(n, np.uint16)
+            N.call("cmcg_matrix_get_values", self.handle, raw.ctypes.data_as(C.c_void_p))
+            out = (raw.astype(np.uint32) << 16).view(np.float32)
+        else:
+            out = np.empty(n, np.float32 if self.dtype == torch.float32 else np.float64)
+            N.call("cmcg_matrix_get_values", self.handle, out.ctypes.data_as(C.c_void_p))
+        if self.pattern.format == ELLPACK:
+            return out.reshape(self.batches, self.pattern.nnzPerRow, self.rows).transpose(0, 2, 1)
+        return out.reshape(self.batches, self.pattern.nnz)
+
+    def product(self, x: torch.Tensor, out: Optional[torch.Tensor] = None, mode: int = N.ASSIGN) -> torch.Tensor:
+        """out (mode)= A * x; x is (cols,) or (xb, cols) float32/float64 on the device."""
+        xb = 1 if x.dim() == 1 else x.shape[0]
+        ob = max(self.batches, xb)
+        if out is None:
+            shape = (self.rows,) if (x.dim() == 1 and self.batches == 1) else (ob, self.rows)
+            out = torch.empty(shape, dtype=x.dtype, device=x.device)
+        x = x.contiguous()
+        N.call("cmcg_spmv", self.handle, _TORCH_DT[x.dtype], _vp(x), xb, _vp(out), mode)
+        return out
+
+    def __mul__(self, x: torch.Tensor) -> torch.Tensor:
+        return self.product(x)
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) is not None:
+                N.lib.cmcg_matrix_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def dot(x: torch.Tensor, y: torch.Tensor) -> torch.Tensor:
+    """Batched dot product: (n,) -> scalar tensor, (b, n) -> (b,)."""
+    ctx = Context.current()
+    xb = 1 if x.dim() == 1 else x.shape[0]
+    yb = 1 if y.dim() == 1 else y.shape[0]
+    n = x.shape[-1]
+    ob = max(xb, yb)
+    out = torch.empty(ob, dtype=x.dtype, device=x.device)
+    N.call("cmcg_dot", ctx.handle, _TORCH_DT[x.dtype], n, _vp(x.contiguous()), xb, _vp(y.contiguous()), yb, _vp(out))
+    return out[0] if (x.dim() == 1 and y.dim() == 1) else out
+
+
+def squaredNorm(x: torch.Tensor) -> torch.Tensor:
+    ctx = Context.current()
+    b = 1 if x.dim() == 1 else x.shape[0]
+    out = torch.empty(b, dtype=x.dtype, device=x.device)
+    N.call("cmcg_squared_norm", ctx.handle, _TORCH_DT[x.dtype], x.shape[-1], _vp(x.contiguous()), b, _vp(out))
+    return out[0] if x.dim() == 1 else out
+
+
+def norm(x: torch.Tensor) -> torch.Tensor:
+    return torch.sqrt(squaredNorm(x))
+
+
+def sddmm(A: SparseMatrix, u: torch.Tensor, v: torch.Tensor, alpha: float = 1.0) -> torch.Tensor:
+    """alpha * u v^T sampled on A's pattern, in A's value layout ([batch][nnz])."""
+    ub = 1 if u.dim() == 1 else u.shape[0]
+    vb = 1 if v.dim() == 1 else v.shape[0]
+    ob = max(ub, vb)
+    out = torch.empty((ob, A.pattern.getNNZ()), dtype=u.dtype, device=u.device)
+    N.call("cmcg_sddmm", A.handle, _TORCH_DT[u.dtype], float(alpha), _vp(u.contiguous()), ub, _vp(v.contiguous()), vb,
+           _vp(out), ob)
+    return out
