@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of the batched sparse CG path on B200.
+
+Workload (one "step"): the batching configuration's 4096 independent 2D
+variable-coefficient diffusion systems (5-point finite volume, kappa = exp(g),
+g ~ N(0, 0.5^2), sides ~ U{16..128}, seed 2, FP32 CSR packed into one buffer)
+solved to a relative residual of 1e-10 by the mixed-precision solver: FP32
+Jacobi-CG inner solves to 1e-4 with FP64 residual / update / norms, one
+persistent launch for the whole batch. Metric: solves/s. The same line also
+carries plain FP64 batched CG on the same batch (the comparison named by the
+metric), SpMV GB/s on the 1024^2 Poisson matrix (CSR and ELLPACK), the HBM
+roofline of the dominant kernel, the CPU baseline (the reference's bundled
+Eigen FP64 Jacobi-CG, all host threads, a bounded sample) and the end-to-end
+number through the public API with host buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+N > 1: launch with torch.distributed.run; every rank solves its own batch
+(seed 2 + rank), no collective on the data path (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED = 4096, 16, 128, 0.5, 2
+INNER_TOL, OUTER_TOL, MAX_OUTER = 1e-4, 1e-10, 30
+METRIC = "CG solves/s at 1e-10 rel. residual (mixed FP32/FP64-refined, batched)"
+UNIT = "solves/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [l.split(",") for l in Path(self.f.name).read_text().splitlines() if l.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [c.strip() for c in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_setup(gpus: int):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes (per unit, stated in DESIGN.md)
+# ---------------------------------------------------------------------------
+
+def refined_bytes(bt, inner_iters, outer_steps, inner_value_bytes=4):
+    """Per system s: each inner Jacobi-CG iteration streams the matrix
+    (nnz * (value + 4-byte column) + (n + 1) * 4) plus 13 FP32 n-vectors (the
+    three-pass schedule); each refinement step streams the FP32 matrix once more
+    in FP64 arithmetic plus 3 FP64 n-vectors (read x, b; write the residual)."""
+    n = np.diff(bt.row_off).astype(np.float64)
+    nnz = (bt.row_ptr[bt.row_off[1:]] - bt.row_ptr[bt.row_off[:-1]]).astype(np.float64)
+    b_iter = nnz * (inner_value_bytes + 4) + (n + 1) * 4 + 13 * n * 4
+    b_outer = nnz * (4 + 4) + (n + 1) * 4 + 3 * n * 8
+    return float(np.sum(inner_iters * b_iter + outer_steps * b_outer))
+
+
+def plain_bytes(bt, iters, vbytes=8, vecbytes=8):
+    n = np.diff(bt.row_off).astype(np.float64)
+    nnz = (bt.row_ptr[bt.row_off[1:]] - bt.row_ptr[bt.row_off[:-1]]).astype(np.float64)
+    return float(np.sum(iters * (nnz * (vbytes + 4) + (n + 1) * 4 + 13 * n * vecbytes)))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def time_device(fn, steps, warmup, stream, world):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = start.elapsed_time(end) / steps
+    return max_over_ranks(world, ms)
+
+
+def spmv_gbs(cm, torch, dev, stream):
+    """SpMV y = A x on the 1024^2 Poisson matrix (configuration 2), CSR and
+    ELLPACK, over enough matrix copies to exceed L2 (no reuse between calls)."""
+    from cumat_b200 import problems as P
+    pr = P.poisson2d(1024, 1)
+    n, nnz = pr.n, pr.nnz
+    idx, ev = P.csr_to_ell(n, pr.row_ptr, pr.col, pr.val)
+    csr_bytes = nnz * 8 + (n + 1) * 4 + 2 * n * 4
+    ell_bytes = n * 5 * 8 + 2 * n * 4
+    copies = int(np.ceil(3 * L2_BYTES / csr_bytes)) + 1
+    mats_c, mats_e, xs, ys = [], [], [], []
+    for c in range(copies):
+        p = cm.SparsityPattern.csr(n, n, pr.row_ptr, pr.col)
+        mats_c.append(cm.SparseMatrix(p).setData(pr.val))
+        pe = cm.SparsityPattern.ell(n, n, idx)
+        mats_e.append(cm.SparseMatrix(pe).setData(ev))
+        xs.append(torch.from_numpy(pr.b).to(dev))
+        ys.append(torch.empty(n, device=dev))
+    out = {}
+    for name, mats, byt in [("csr", mats_c, csr_bytes), ("ell", mats_e, ell_bytes)]:
+        for i in range(copies):  # warm-up
+            mats[i].product(xs[i], out=ys[i])
+        torch.cuda.synchronize()
+        reps = 100
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for r in range(reps):
+            i = r % copies
+            mats[i].product(xs[i], out=ys[i])
+        e.record(stream)
+        torch.cuda.synchronize()
+        us = s.elapsed_time(e) * 1000.0 / reps
+        out[name] = {"us": round(us, 3), "gbs": round(byt / us / 1e3, 1), "alg_bytes": byt, "copies": copies}
+    return out
+
+
+def cpu_baseline(bt, budget_s=15.0):
+    """Eigen FP64 Jacobi-CG to 1e-10 (the reference's bundled CPU path) on the
+    first m systems of the batch (sides are drawn i.i.d., so a prefix is a
+    random sample), OpenMP-parallel over systems on all host threads; m is
+    sized from a short probe run to take about budget_s seconds."""
+    from oracle import oracle as O
+    if O.ref_lib() is None:
+        return None
+    b64 = bt.b.astype(np.float64)
+    x64 = np.zeros_like(b64)
+    ep = O.EigenPacked(bt.row_off, bt.row_ptr, bt.col, bt.val)
+    threads = O.ref_threads()
+    m0 = min(bt.n_sys, max(2 * threads, 32))
+    t0, _, _ = ep.solve(0, m0, b64, x64, OUTER_TOL, -1, 1, threads)
+    m = int(min(bt.n_sys, max(m0, m0 / max(t0, 1e-9) * budget_s)))
+    t, it, err = ep.solve(0, m, b64, x64, OUTER_TOL, -1, 1, threads)
+    return {"value": round(m / t, 3), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"first {m} of {bt.n_sys} systems, Eigen 3.3.90 ConjugateGradient<SparseMatrix<double,"
+                      f"RowMajor>, Lower|Upper, DiagonalPreconditioner> to 1e-10, OpenMP over systems, {t:.1f} s"}
+
+
+def run_ours(args):
+    import torch
+
+    import cumat_b200 as cm
+    from cumat_b200 import problems as P
+
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    hbm_peak, peak_src = peaks()
+    bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED + rank)
+    p = cm.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A32 = cm.SparseMatrix(p, dtype=torch.float32).setData(bt.val)
+    cg = cm.ConjugateGradient(A32).setTolerance(INNER_TOL)
+    b64 = torch.from_numpy(bt.b.astype(np.float64)).to(dev)
+    x64 = torch.empty_like(b64)
+
+    def step():
+        cg.solve_refined(b64, outer=A32, outer_tol=OUTER_TOL, max_outer=MAX_OUTER, out=x64)
+
+    launches0 = cm.launch_count()
+    with Clocks(local) as clk:
+        ms = time_device(step, args.steps, args.warmup, stream, world)
+    launches = (cm.launch_count() - launches0) // (args.steps + args.warmup) * args.steps
+    st = cg.system_stats()
+    assert np.all(st["status"] == 0), "some systems did not converge"
+    assert float(st["error"].max()) < OUTER_TOL
+    total_solves = N_SYS * world
+    value = total_solves / (ms / 1e3)
+    # roofline of the dominant (only) kernel: the persistent refined launch
+    alg = refined_bytes(bt, st["iterations"].astype(np.float64), st["outer"].astype(np.float64))
+    achieved = alg / (ms / 1e3) / 1e9
+
+    # plain FP64 batched CG on the same batch (FP64 values and vectors)
+    A64 = cm.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
+    cg64 = cm.ConjugateGradient(A64).setTolerance(OUTER_TOL)
+    xp = torch.empty_like(b64)
+    ms64 = time_device(lambda: cg64.solve(b64, out=xp), max(1, args.steps // 2), 1, stream, world)
+    st64 = cg64.system_stats()
+    fp64 = {"value": round(N_SYS * world / (ms64 / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms64, 3),
+            "converged": int((st64["status"] == 0).sum()), "max_error": float(st64["error"].max()),
+            "iterations_max": int(st64["iterations"].max()),
+            "gbs_alg": round(plain_bytes(bt, st64["iterations"].astype(np.float64)) / (ms64 / 1e3) / 1e9, 1)}
+
+    # end to end through the public API with pinned host buffers
+    hb = torch.from_numpy(bt.b.astype(np.float64)).pin_memory()
+    hx = torch.empty(bt.n, dtype=torch.float64).pin_memory()
+    db = torch.empty_like(b64)
+
+    def e2e_step():
+        db.copy_(hb, non_blocking=True)
+        cg.solve_refined(db, outer=A32, outer_tol=OUTER_TOL, max_outer=MAX_OUTER, out=x64)
+        hx.copy_(x64, non_blocking=True)
+
+    ms_e2e = time_device(e2e_step, args.steps, 1, stream, world)
+
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_spmv:
+        extra["spmv_poisson1024"] = spmv_gbs(cm, torch, dev, stream)
+        for k in ("csr", "ell"):
+            extra["spmv_poisson1024"][k]["frac"] = round(extra["spmv_poisson1024"][k]["gbs"] / hbm_peak, 3)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(bt, args.cpu_budget)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded finite-volume systems)",
+            "config": {"workload": "4096 uneven 2D FV diffusion systems (sides 16..128, kappa=exp(N(0,0.25))), "
+                                   "Jacobi-CG FP32 inner to 1e-4 + FP64 refinement to 1e-10",
+                       "systems_per_gpu": N_SYS, "rows_per_gpu": int(bt.n), "nnz_per_gpu": int(bt.nnz),
+                       "parallelism": f"batch sharding x{world}, no collective",
+                       "l2": "inputs larger than L2 (FP32 CSR batch %.2f GB)" % ((bt.nnz * 8 + bt.n * 4) / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved / hbm_peak, 3), "traffic": None,
+                         "kernel": "k_persistent_refined", "peak_source": peak_src,
+                         "alg_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(N_SYS * world / (ms_e2e / 1e3), 1), "unit": UNIT,
+                    "h2d_bytes_per_step": int(bt.n * 8), "d2h_bytes_per_step": int(bt.n * 8)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "fp64_plain": fp64,
+            "mixed_vs_fp64": round(value / fp64["value"], 3),
+            "solve_stats": {"inner_iterations_max": int(st["iterations"].max()),
+                            "inner_iterations_mean": round(float(st["iterations"].mean()), 1),
+                            "outer_steps_max": int(st["outer"].max()), "max_error": float(st["error"].max())},
+            **extra,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's bundled Eigen CPU path on the host cores
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cumat_b200 import problems as P
+    from oracle import oracle as O
+    if O.ref_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libeigen_ref.so (bundled Eigen) not built"}))
+        return
+    bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED)
+    ep = O.EigenPacked(bt.row_off, bt.row_ptr, bt.col, bt.val)
+    b64 = bt.b.astype(np.float64)
+    x64 = np.zeros_like(b64)
+    threads = O.ref_threads()
+    # each step: a contiguous slice of systems (steps rotate through the batch),
+    # sized to keep the whole run within a few minutes
+    per_step = max(threads * 2, 64)
+    times, solved = [], 0
+    for i in range(args.warmup + args.steps):
+        s0 = (i * per_step) % (N_SYS - per_step)
+        dt, it, err = ep.solve(s0, s0 + per_step, b64, x64, OUTER_TOL, -1, 1, threads)
+        if i >= args.warmup:
+            times.append(dt)
+            solved += per_step
+    secs = sum(times)
+    value = solved / secs
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded finite-volume systems)",
+            "impl": "reference",
+            "config": {"workload": "4096 uneven 2D FV diffusion systems (sides 16..128, kappa=exp(N(0,0.25))), "
+                                   "Eigen FP64 Jacobi-CG to 1e-10", "systems_per_step": per_step},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{per_step} consecutive systems per step of {N_SYS}"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-spmv", action="store_true", help="skip the SpMV GB/s sub-benchmark")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -16,7 +16,8 @@ CSR, ELLPACK = 0, 1
 PRECOND_IDENTITY, PRECOND_JACOBI = 0, 1
 ASSIGN, ADD, SUB = 0, 1, 2
 SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_ZERO_RHS, SOLVE_BREAKDOWN, SOLVE_NON_FINITE = 0, 1, 2, 3, 4
-PATH_AUTO, PATH_PERSISTENT, PATH_GRID = 0, 1, 2
+PATH_AUTO, PATH_PERSISTENT, PATH_GRID, PATH_PERSISTENT_GLOBAL = 0, 1, 2, 3
+REFINE_RELIABLE, REFINE_RESTART = 0, 1
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "OUT_OF_MEMORY", 4: "NOT_SUPPORTED", 5: "INTERNAL"}
 
 _vp = C.c_void_p
@@ -36,6 +37,7 @@ SIGNATURES = {
     "cmcg_ctx_destroy": (_i32, [_vp]),
     "cmcg_ctx_synchronize": (_i32, [_vp]),
     "cmcg_ctx_stream": (_i32, [_vp, C.POINTER(_vp)]),
+    "cmcg_ctx_device_errors": (_i32, [_vp, _pi32]),
     "cmcg_pattern_create_csr": (_i32, [_vp, _i32, _i32, _i64, _vp, _vp, _i32, C.POINTER(_vp)]),
     "cmcg_pattern_create_ell": (_i32, [_vp, _i32, _i32, _i32, _vp, _i32, C.POINTER(_vp)]),
     "cmcg_pattern_set_systems": (_i32, [_vp, _i64, _vp]),
@@ -57,6 +59,7 @@ SIGNATURES = {
     "cmcg_cg_set_max_iterations": (_i32, [_vp, _i64]),
     "cmcg_cg_get_settings": (_i32, [_vp, _pf64, _pi64]),
     "cmcg_cg_set_path": (_i32, [_vp, _i32]),
+    "cmcg_cg_set_refinement": (_i32, [_vp, _i32, _f64]),
     "cmcg_cg_solve": (_i32, [_vp, _i32, _vp, _i32, _vp, _vp]),
     "cmcg_cg_solve_host": (_i32, [_vp, _i32, _vp, _i32, _vp, _vp]),
     "cmcg_cg_iterations": (_i32, [_vp, _pi64]),

@@ -27,7 +27,10 @@
 #include <numeric>
 #include <vector>
 
+#include <type_traits>
+
 #include "cg_dev.cuh"
+#include "cg_smem.cuh"
 #include "common.cuh"
 #include "objects.h"
 
@@ -59,6 +62,13 @@ struct MatArgs {
     const MT* vals;
     int64_t vstride;
     int32_t mb;
+    // sliced ELLPACK copy (CSR patterns)
+    const int32_t* sell_col;
+    const MT* sell_vals;
+    int64_t sell_vstride;
+    const int64_t* slice_off;
+    const int32_t* slice_w;
+    const int32_t* sys_slice0;
 };
 
 template <typename MT, int FMT>
@@ -67,6 +77,11 @@ __device__ __forceinline__ InstMatrix<MT, FMT> inst_matrix(const MatArgs<MT>& m,
     const MT* v = m.vals + (m.mb == 1 ? 0 : static_cast<int64_t>(b) * m.vstride);
     A.csr = CsrView<MT>{m.rp, m.ci, v};
     A.ell = EllView<MT>{m.ell, v, m.width, m.rows_pad};
+    if (FMT == CMCG_CSR)
+        A.rm = RowMat<MT>{m.sell_col, m.sell_vals + (m.mb == 1 ? 0 : static_cast<int64_t>(b) * m.sell_vstride),
+                          m.slice_off, m.slice_w, m.sys_slice0, 0, 0};
+    else
+        A.rm = RowMat<MT>{m.ell, v, nullptr, nullptr, nullptr, m.rows_pad, m.width};
     return A;
 }
 
@@ -116,6 +131,7 @@ struct SolveArgs {
     VT* q;
     double tol;
     int64_t max_iter;              // < 0: 2 * rows of the system
+    int32_t abs_zero_test;         // reference early-out |b|^2 < tol^2 (0 for refinement inner solves)
     InstState st;
 };
 
@@ -128,15 +144,15 @@ __device__ __forceinline__ int64_t sys_max_iter(int64_t mi, int n) { return mi <
 // PCG of one system with the whole CTA. Vectors are batch slices indexed by
 // global row. Returns the status; writes iterations / |r|^2 / |b|^2.
 template <typename VT, typename MT, int FMT>
-__device__ int32_t cta_pcg(const InstMatrix<MT, FMT>& A, int r0, int n, const VT* __restrict__ bv,
+__device__ int32_t cta_pcg(const InstMatrix<MT, FMT>& A, int sys, int r0, int n, const VT* __restrict__ bv,
                            const VT* __restrict__ g, VT* __restrict__ x, VT* __restrict__ r, VT* __restrict__ p,
-                           VT* __restrict__ q, const VT* __restrict__ dinv, VT tol, int64_t maxit, WarpStage<VT>* stage,
+                           VT* __restrict__ q, const VT* __restrict__ dinv, VT tol, int64_t maxit,
                            VT* red, int32_t& it_out, VT& rr_out, VT& bb_out, bool abs_zero_test = true) {
     const int tid = threadIdx.x, T = blockDim.x;
     const int r1 = r0 + n;
     VT acc[2] = {VT(0), VT(0)};
     if (g) {
-        cta_rows_product<VT>(A, r0, n, GlobalX<VT>{g}, stage, [&](int row, VT v) {
+        cta_rows<VT>(A, sys, r0, 0, n, GlobalX<VT>{g}, [&](int row, VT v) {
             const VT bi = bv[row];
             const VT ri = bi - v;
             r[row] = ri;
@@ -181,7 +197,7 @@ __device__ int32_t cta_pcg(const InstMatrix<MT, FMT>& A, int r0, int n, const VT
         while (status == ST_RUNNING) {
             if (it >= maxit) { status = CMCG_SOLVE_MAX_ITER; break; }
             VT pq[1] = {VT(0)};
-            cta_rows_product<VT>(A, r0, n, GlobalX<VT>{p}, stage, [&](int row, VT v) {
+            cta_rows<VT>(A, sys, r0, 0, n, GlobalX<VT>{p}, [&](int row, VT v) {
                 q[row] = v;
                 pq[0] += p[row] * v;
             });
@@ -232,7 +248,6 @@ __device__ __forceinline__ int fetch_item(int32_t* next, int* slot) {
 
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kPersistThreads) k_persistent_cg(SolveArgs<VT, MT> a) {
-    __shared__ WarpStage<VT> stage[kPersistThreads / 32];
     __shared__ VT red[2 * (kPersistThreads / 32)];
     __shared__ int slot;
     const int n_inst = a.n_sys * a.ob;
@@ -246,9 +261,9 @@ __global__ void __launch_bounds__(kPersistThreads) k_persistent_cg(SolveArgs<VT,
         int32_t it;
         VT rr, bb;
         const int32_t status = cta_pcg<VT, MT, FMT>(
-            A, r0, n, a.b + (a.b_b == 1 ? 0 : vo), a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr, a.x + vo,
+            A, s, r0, n, a.b + (a.b_b == 1 ? 0 : vo), a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr, a.x + vo,
             a.r + vo, a.p + vo, a.q + vo, a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr, static_cast<VT>(a.tol),
-            sys_max_iter(a.max_iter, n), stage, red, it, rr, bb);
+            sys_max_iter(a.max_iter, n), red, it, rr, bb, a.abs_zero_test != 0);
         if (threadIdx.x == 0) {
             a.st.it[inst] = it;
             a.st.status[inst] = status;
@@ -290,11 +305,9 @@ struct RefineArgs {
 
 template <typename MI, typename MO, int FMT>
 __global__ void __launch_bounds__(kPersistThreads) k_persistent_refined(RefineArgs<MI, MO> a) {
-    __shared__ WarpStage<double> stage_raw[kPersistThreads / 32];  // large enough for float too
     __shared__ double red64[2 * (kPersistThreads / 32)];
     __shared__ float red32[2 * (kPersistThreads / 32)];
     __shared__ int slot;
-    WarpStage<float>* stage32 = reinterpret_cast<WarpStage<float>*>(stage_raw);
     const int tid = threadIdx.x, T = blockDim.x;
     const int n_inst = a.n_sys * a.ob;
     for (;;) {
@@ -331,9 +344,9 @@ __global__ void __launch_bounds__(kPersistThreads) k_persistent_refined(RefineAr
             if (outer >= a.max_outer) { status = CMCG_SOLVE_MAX_ITER; break; }
             int32_t it;
             float rr_in, bb_in;
-            const int32_t st_in = cta_pcg<float, MI, FMT>(Ai, r0, n, r32, nullptr, d32, a.r + vo, a.p + vo, a.q + vo,
+            const int32_t st_in = cta_pcg<float, MI, FMT>(Ai, s, r0, n, r32, nullptr, d32, a.r + vo, a.p + vo, a.q + vo,
                                                           dinv, static_cast<float>(a.inner_tol),
-                                                          sys_max_iter(a.max_inner, n), stage32, red32, it, rr_in, bb_in,
+                                                          sys_max_iter(a.max_inner, n), red32, it, rr_in, bb_in,
                                                           /*abs_zero_test=*/false);
             inner_total += it;
             if (st_in == CMCG_SOLVE_NON_FINITE || (st_in == CMCG_SOLVE_BREAKDOWN && it == 0)) { status = st_in; break; }
@@ -341,7 +354,7 @@ __global__ void __launch_bounds__(kPersistThreads) k_persistent_refined(RefineAr
             __syncthreads();
             // FP64 residual with the outer values, rounded into the next inner rhs
             double rv[1] = {0.0};
-            cta_rows_product<double>(Ao, r0, n, GlobalX<double>{x}, stage_raw, [&](int row, double v) {
+            cta_rows<double>(Ao, s, r0, 0, n, GlobalX<double>{x}, [&](int row, double v) {
                 const double ri = bv[row] - v;
                 r32[row] = static_cast<float>(ri);
                 rv[0] += ri * ri;
@@ -358,6 +371,317 @@ __global__ void __launch_bounds__(kPersistThreads) k_persistent_refined(RefineAr
             a.st.bb[inst] = bb;
             a.st.outer[inst] = outer;
             a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(rr / bb);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory-resident kernels (systems of at most kSmemMaxRows rows)
+// ---------------------------------------------------------------------------
+
+// FP32 PCG with the reference's algorithm and stopping rule.
+template <typename MT, int FMT>
+__global__ void __launch_bounds__(kSmemThreads, 1) k_cg_smem(SolveArgs<float, MT> a, int nmax) {
+    extern __shared__ __align__(16) float sm[];
+    __shared__ float red[2 * (kSmemThreads / 32)];
+    __shared__ int slot;
+    const SmemLayout L = smem_layout(sm, nmax);
+    const int tid = threadIdx.x;
+    const int n_inst = a.n_sys * a.ob;
+    const float tol = static_cast<float>(a.tol);
+    for (;;) {
+        const int item = fetch_item(a.next, &slot);
+        if (item >= n_inst) return;
+        const int s = a.order[item / a.ob], b = item % a.ob, inst = b * a.n_sys + s;
+        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
+        const auto A = inst_matrix<MT, FMT>(a.m, b);
+        const int64_t vo = static_cast<int64_t>(b) * a.rows;
+        const float* bv = a.b + (a.b_b == 1 ? 0 : vo) + r0;
+        float* xg = a.x + vo + r0;
+        const float* dg = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) + r0 : nullptr;
+        float q[kSmemNK];
+        float acc[2] = {0.0f, 0.0f};
+        // inverse diagonal through the read-only cache (1 for the identity preconditioner)
+        auto dv = [&](int i) { return dg ? __ldg(dg + i) : 1.0f; };
+        if (a.guess) {
+            const float* g = a.guess + (a.g_b == 1 ? 0 : vo);
+            smem_product<MT, FMT>(A, s, r0, n, GlobalX<float>{g}, q);
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const float bi = bv[i];
+                    const float ri = bi - q[k];
+                    L.x[i] = g[r0 + i];
+                    L.r[i] = ri;
+                    acc[0] += bi * bi;
+                    acc[1] += ri * ri;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const float bi = bv[i];
+                    L.r[i] = bi;
+                    L.x[i] = 0.0f;
+                    acc[0] += bi * bi;
+                }
+            }
+            acc[1] = acc[0];
+        }
+        block_sum<float, 2>(acc, red);
+        const float bb = acc[0];
+        float rr = acc[1];
+        const float thr = tol * tol * bb;
+        int32_t status = ST_RUNNING, it = 0;
+        if ((a.abs_zero_test && bb < tol * tol) || bb == 0.0f) {
+            status = CMCG_SOLVE_ZERO_RHS;
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) L.x[i] = 0.0f;
+            }
+        } else if (!finite_(rr) || !finite_(bb)) {
+            status = CMCG_SOLVE_NON_FINITE;
+        } else if (rr < thr) {
+            status = CMCG_SOLVE_CONVERGED;
+        } else {
+            float rz1[1] = {0.0f};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const float ri = L.r[i];
+                    const float zi = dv(i) * ri;
+                    L.p[i] = zi;
+                    rz1[0] += ri * zi;
+                }
+            }
+            block_sum<float, 1>(rz1, red);
+            float rz = rz1[0];
+            if (!finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
+            else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+            const int64_t maxit = sys_max_iter(a.max_iter, n);
+            while (status == ST_RUNNING) {
+                if (it >= maxit) { status = CMCG_SOLVE_MAX_ITER; break; }
+                smem_product<MT, FMT>(A, s, r0, n, SmemX{L.p, r0}, q);
+                float pq[1] = {0.0f};
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) pq[0] += L.p[i] * q[k];
+                }
+                block_sum<float, 1>(pq, red);
+                const float alpha = rz / pq[0];
+                if (!finite_(pq[0]) || !finite_(alpha)) { status = CMCG_SOLVE_NON_FINITE; break; }
+                if (!(pq[0] > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
+                float s2[2] = {0.0f, 0.0f};
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        L.x[i] += alpha * L.p[i];
+                        const float ri = L.r[i] - alpha * q[k];
+                        L.r[i] = ri;
+                        s2[0] += ri * ri;
+                        s2[1] += ri * (dv(i) * ri);
+                    }
+                }
+                block_sum<float, 2>(s2, red);
+                rr = s2[0];
+                if (!finite_(rr) || !finite_(s2[1])) { status = CMCG_SOLVE_NON_FINITE; break; }
+                if (rr < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+                if (!(s2[1] > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
+                const float beta = s2[1] / rz;
+                rz = s2[1];
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) L.p[i] = dv(i) * L.r[i] + beta * L.p[i];
+                }
+                __syncthreads();
+                ++it;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kSmemNK; ++k) {
+            const int i = tid + k * kSmemThreads;
+            if (i < n) xg[i] = L.x[i];
+        }
+        if (tid == 0) {
+            a.st.it[inst] = it;
+            a.st.status[inst] = status;
+            a.st.rr[inst] = rr;
+            a.st.bb[inst] = bb;
+            a.st.outer[inst] = 0;
+            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(static_cast<double>(rr) / static_cast<double>(bb));
+        }
+        __syncthreads();
+    }
+}
+
+// Mixed precision with reliable updates: FP32 PCG (values MI) whose solution
+// increments are folded into the FP64 solution, and whose recursive residual is
+// replaced by the true FP64 residual b - A x (values MO) whenever it has dropped
+// by `delta` since the last replacement or looks converged (residual
+// replacement, van der Vorst & Ye 2000; reliable updates as in Clark et al.
+// 2010). The Krylov direction p is kept across replacements, so the iteration
+// count stays close to plain CG's. Convergence is decided on the FP64 residual:
+// |b - A x| < outer_tol |b|.
+template <typename MI, typename MO, int FMT>
+__global__ void __launch_bounds__(kSmemThreads, 1) k_reliable_smem(RefineArgs<MI, MO> a, int nmax, float delta) {
+    extern __shared__ __align__(16) float sm[];
+    __shared__ float red[2 * (kSmemThreads / 32)];
+    __shared__ double red64[2 * (kSmemThreads / 32)];
+    __shared__ int slot;
+    const SmemLayout L = smem_layout(sm, nmax);
+    const int tid = threadIdx.x;
+    const int n_inst = a.n_sys * a.ob;
+    for (;;) {
+        const int item = fetch_item(a.next, &slot);
+        if (item >= n_inst) return;
+        const int s = a.order[item / a.ob], bi = item % a.ob, inst = bi * a.n_sys + s;
+        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
+        const auto Ai = inst_matrix<MI, FMT>(a.inner, bi);
+        const auto Ao = inst_matrix<MO, FMT>(a.outer, bi);
+        const int64_t vo = static_cast<int64_t>(bi) * a.rows;
+        const double* bv = a.b + (a.b_b == 1 ? 0 : vo);
+        double* x = a.x + vo;
+        const float* dg = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+        float q[kSmemNK];
+        auto dv = [&](int i) { return dg ? __ldg(dg + r0 + i) : 1.0f; };
+        double acc[1] = {0.0};
+        float rz1[1] = {0.0f};
+#pragma unroll
+        for (int k = 0; k < kSmemNK; ++k) {
+            const int i = tid + k * kSmemThreads;
+            if (i < n) {
+                const double b_i = bv[r0 + i];
+                x[r0 + i] = 0.0;
+                const float ri = static_cast<float>(b_i);
+                const float di = dv(i);
+                L.r[i] = ri;
+                L.x[i] = 0.0f;
+                L.p[i] = di * ri;
+                acc[0] += b_i * b_i;
+                rz1[0] += ri * (di * ri);
+            }
+        }
+        block_sum<double, 1>(acc, red64);
+        block_sum<float, 1>(rz1, red);
+        const double bb = acc[0];
+        const double thr = a.outer_tol * a.outer_tol * bb;
+        double rr64 = bb;
+        double rmax2 = bb;                      // |r|^2 at the last replacement
+        const float thr32 = static_cast<float>(thr);
+        float rz = rz1[0];
+        int32_t status = ST_RUNNING, it = 0, updates = 0;
+        if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
+        else if (!finite_(bb)) status = CMCG_SOLVE_NON_FINITE;
+        else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
+        else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+        const int64_t maxit = sys_max_iter(a.max_inner, n);
+        const float d2 = delta * delta;
+        while (status == ST_RUNNING) {
+            if (it >= maxit || updates >= a.max_outer) { status = CMCG_SOLVE_MAX_ITER; break; }
+            smem_product<MI, FMT>(Ai, s, r0, n, SmemX{L.p, r0}, q);
+            float pq[1] = {0.0f};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) pq[0] += L.p[i] * q[k];
+            }
+            block_sum<float, 1>(pq, red);
+            const float alpha = rz / pq[0];
+            if (!finite_(pq[0]) || !finite_(alpha)) { status = CMCG_SOLVE_NON_FINITE; break; }
+            if (!(pq[0] > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
+            float s2[2] = {0.0f, 0.0f};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    L.x[i] += alpha * L.p[i];
+                    const float ri = L.r[i] - alpha * q[k];
+                    L.r[i] = ri;
+                    s2[0] += ri * ri;
+                    s2[1] += ri * (dv(i) * ri);
+                }
+            }
+            block_sum<float, 2>(s2, red);
+            ++it;
+            if (!finite_(s2[0]) || !finite_(s2[1])) { status = CMCG_SOLVE_NON_FINITE; break; }
+            float rzn = s2[1];
+            if (s2[0] < d2 * static_cast<float>(rmax2) || s2[0] < thr32) {
+                // reliable update: fold the FP32 increments into x, replace r
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        x[r0 + i] += static_cast<double>(L.x[i]);
+                        L.x[i] = 0.0f;
+                    }
+                }
+                __syncthreads();
+                double t2[2] = {0.0, 0.0};
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        const double r64 = bv[r0 + i] - row_product<double>(Ao.rm, s, r0, i, GlobalX<double>{x});
+                        const float ri = static_cast<float>(r64);
+                        L.r[i] = ri;
+                        t2[0] += r64 * r64;
+                        t2[1] += static_cast<double>(ri) * static_cast<double>(dv(i) * ri);
+                    }
+                }
+                block_sum<double, 2>(t2, red64);
+                ++updates;
+                rr64 = t2[0];
+                rmax2 = rr64;
+                rzn = static_cast<float>(t2[1]);
+                if (!finite_(rr64)) { status = CMCG_SOLVE_NON_FINITE; break; }
+                if (rr64 < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+            }
+            if (!(rzn > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
+            const float beta = rzn / rz;
+            rz = rzn;
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) L.p[i] = dv(i) * L.r[i] + beta * L.p[i];
+            }
+            __syncthreads();
+        }
+        // fold any pending increments (iteration limit / breakdown exits)
+        bool pending = false;
+#pragma unroll
+        for (int k = 0; k < kSmemNK; ++k) {
+            const int i = tid + k * kSmemThreads;
+            if (i < n && L.x[i] != 0.0f) { x[r0 + i] += static_cast<double>(L.x[i]); pending = true; }
+        }
+        if (__syncthreads_or(pending)) {
+            double t1[1] = {0.0};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const double r64 = bv[r0 + i] - row_product<double>(Ao.rm, s, r0, i, GlobalX<double>{x});
+                    t1[0] += r64 * r64;
+                }
+            }
+            block_sum<double, 1>(t1, red64);
+            rr64 = t1[0];
+        }
+        if (tid == 0) {
+            a.st.it[inst] = it;
+            a.st.status[inst] = status;
+            a.st.rr[inst] = rr64;
+            a.st.bb[inst] = bb;
+            a.st.outer[inst] = updates;
+            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(rr64 / bb);
         }
         __syncthreads();
     }
@@ -398,7 +722,7 @@ __device__ bool tile_ticket(const VT (&v)[NV], VT* const (&part)[NV], int64_t pb
 }
 
 struct TileInfo {
-    int b, t, s, inst, r0, r1, t_begin, t_count;
+    int b, t, s, inst, r0, r1, sr0, t_begin, t_count;   // sr0: first row of the system
 };
 
 template <typename VT, typename MT>
@@ -410,6 +734,7 @@ __device__ __forceinline__ TileInfo tile_info(const SolveArgs<VT, MT>& a, int64_
     ti.inst = ti.b * a.n_sys + ti.s;
     ti.r0 = a.tile_row0[ti.t];
     ti.r1 = min(ti.r0 + kTile, a.row_off[ti.s + 1]);
+    ti.sr0 = a.row_off[ti.s];
     ti.t_begin = a.sys_tile_begin[ti.s];
     ti.t_count = a.sys_tile_begin[ti.s + 1] - ti.t_begin;
     return ti;
@@ -418,7 +743,6 @@ __device__ __forceinline__ TileInfo tile_info(const SolveArgs<VT, MT>& a, int64_
 // init A: x = guess or 0, r = b - A x, |b|^2, |r|^2 -> status
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
-    __shared__ WarpStage<VT> stage[kTile / 32];
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
     const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
@@ -432,7 +756,7 @@ __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
         if (a.guess) {
             const VT* g = a.guess + (a.g_b == 1 ? 0 : vo);
             const auto A = inst_matrix<MT, FMT>(a.m, ti.b);
-            cta_rows_product<VT>(A, ti.r0, ti.r1 - ti.r0, GlobalX<VT>{g}, stage, [&](int row, VT v) {
+            cta_rows<VT>(A, ti.s, ti.sr0, ti.r0 - ti.sr0, ti.r1 - ti.r0, GlobalX<VT>{g}, [&](int row, VT v) {
                 const VT bi = bv[row];
                 const VT ri = bi - v;
                 r[row] = ri;
@@ -462,7 +786,7 @@ __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
             a.st.it[ti.inst] = 0;
             a.st.outer[ti.inst] = 0;
             int32_t status = ST_RUNNING;
-            if (bb < tol * tol || bb == VT(0)) status = CMCG_SOLVE_ZERO_RHS;
+            if ((a.abs_zero_test && bb < tol * tol) || bb == VT(0)) status = CMCG_SOLVE_ZERO_RHS;
             else if (!finite_(bb) || !finite_(rr)) status = CMCG_SOLVE_NON_FINITE;
             else if (rr < tol * tol * bb) status = CMCG_SOLVE_CONVERGED;
             a.st.status[ti.inst] = status;
@@ -517,7 +841,6 @@ __global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
 // iteration kernel 1: q = A p, p.q -> alpha
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
-    __shared__ WarpStage<VT> stage[kTile / 32];
     __shared__ VT red[kTile / 32];
     __shared__ bool last_s;
     const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
@@ -529,7 +852,7 @@ __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
         VT* q = a.q + vo;
         const auto A = inst_matrix<MT, FMT>(a.m, ti.b);
         VT acc[1] = {VT(0)};
-        cta_rows_product<VT>(A, ti.r0, ti.r1 - ti.r0, GlobalX<VT>{p}, stage, [&](int row, VT v) {
+        cta_rows<VT>(A, ti.s, ti.sr0, ti.r0 - ti.sr0, ti.r1 - ti.r0, GlobalX<VT>{p}, [&](int row, VT v) {
             q[row] = v;
             acc[0] += p[row] * v;
         });
@@ -667,11 +990,15 @@ __global__ void k_inv_diag(MatArgs<MT> m, int32_t rows, VT* __restrict__ out) {
     }
 }
 
+// Kernel view of a matrix; for CSR the sliced ELLPACK copy must be current
+// (ensure_sell_values) before the arguments are taken.
 template <typename MT>
 MatArgs<MT> mat_args(cmcg_matrix A) {
     cmcg_pattern p = A->pat;
+    const SellPlan& S = p->sell;
     return MatArgs<MT>{p->d_row_ptr, p->d_col, p->d_ell, p->width, p->rows_pad, static_cast<const MT*>(A->d_vals),
-                       A->stride, A->batches};
+                       A->stride, A->batches, S.d_col, static_cast<const MT*>(A->d_sell_vals), A->sell_stride,
+                       S.d_slice_off, S.d_slice_w, S.d_sys_slice0};
 }
 
 }  // namespace
@@ -686,6 +1013,11 @@ struct cmcg_solver_s {
     double tol = 0.0;
     int64_t max_iter = -1;
     int32_t path = CMCG_PATH_AUTO;
+    int32_t refine_method = CMCG_REFINE_RELIABLE;
+    double refine_delta = 0.1;
+    bool use_smem = true;     // shared-memory-resident kernels where the systems fit
+    bool inner_solve = false; // set while the solver runs the inner solves of a refinement
+    int64_t systems_version = -1;  // pattern systems the plan was built for
     // plan
     int32_t n_sys = 0, max_sys_rows = 0, n_tiles = 0;
     int32_t* d_order = nullptr;
@@ -740,7 +1072,12 @@ cmcg_status build_plan(cmcg_solver s) {
     s->n_sys = n_sys;
     s->max_sys_rows = maxr;
     s->n_tiles = static_cast<int32_t>(t_row0.size());
+    s->systems_version = p->systems_version;
     cudaStream_t st = p->ctx->stream;
+    for (int32_t** d : {&s->d_order, &s->d_tile_row0, &s->d_tile_sys, &s->d_sys_tile_begin}) {
+        dev_free(*d);
+        *d = nullptr;
+    }
     CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_order), order.size() * 4));
     CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_tile_row0), t_row0.size() * 4));
     CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_tile_sys), t_sys.size() * 4));
@@ -750,6 +1087,15 @@ cmcg_status build_plan(cmcg_solver s) {
     CMCG_CUDA(cudaMemcpyAsync(s->d_tile_sys, t_sys.data(), t_sys.size() * 4, cudaMemcpyHostToDevice, st));
     CMCG_CUDA(cudaMemcpyAsync(s->d_sys_tile_begin, t_begin.data(), t_begin.size() * 4, cudaMemcpyHostToDevice, st));
     CMCG_CUDA(cudaStreamSynchronize(st));
+    return CMCG_OK;
+}
+
+// Rebuilds the work plan when the pattern's systems changed since it was made.
+cmcg_status refresh_plan(cmcg_solver s) {
+    if (s->systems_version == s->A->pat->systems_version) return CMCG_OK;
+    CMCG_CUDA(cudaStreamSynchronize(s->A->pat->ctx->stream));
+    CMCG_TRY(build_plan(s));
+    s->st_inst = 0;   // per-instance state is re-sized on the next solve
     return CMCG_OK;
 }
 
@@ -851,13 +1197,37 @@ SolveArgs<VT, MT> base_args(cmcg_solver s, int32_t ob) {
     a.sys_tile_begin = s->d_sys_tile_begin;
     a.tol = s->tol;
     a.max_iter = s->max_iter;
+    a.abs_zero_test = s->inner_solve ? 0 : 1;
     a.st = s->st;
     return a;
 }
 
+// Sets the dynamic shared memory limit of a kernel once per process.
+template <typename K>
+cmcg_status allow_smem(K kern, size_t bytes) {
+    CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    return CMCG_OK;
+}
+
+inline int smem_rows(int32_t max_rows) { return (max_rows + 3) / 4 * 4; }
+
 template <typename VT, typename MT, int FMT>
 cmcg_status run_persistent(cmcg_solver s, SolveArgs<VT, MT>& a) {
     cmcg_ctx ctx = s->A->pat->ctx;
+    if constexpr (std::is_same<VT, float>::value) {
+        if (s->max_sys_rows <= kSmemMaxRows && s->use_smem) {
+            const int nmax = smem_rows(s->max_sys_rows);
+            const size_t sm = smem_bytes(nmax);
+            CMCG_TRY(allow_smem(k_cg_smem<MT, FMT>, sm));
+            const int n_inst = a.n_sys * a.ob;
+            const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
+            CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+            k_cg_smem<MT, FMT><<<grid, kSmemThreads, sm, ctx->stream>>>(a, nmax);
+            count_launch();
+            CMCG_CHECK_LAUNCH();
+            return CMCG_OK;
+        }
+    }
     int occ = 0;
     CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persistent_cg<VT, MT, FMT>, kPersistThreads, 0));
     const int n_inst = a.n_sys * a.ob;
@@ -924,13 +1294,15 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
         CMCG_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         a.cond = h;
-        CMCG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
-        k_grid_update<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
-        k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
-        k_grid_cond<<<1, 1, 0, st>>>(a.active, a.loops, a.loop_cap, h);
+        if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
+        cudaStream_t cs = ctx->capture_stream;
+        CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        k_grid_update<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        k_grid_cond<<<1, 1, 0, cs>>>(a.active, a.loops, a.loop_cap, h);
         cudaGraph_t captured = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(st, &captured);
+        cudaError_t ce = cudaStreamEndCapture(cs, &captured);
         if (ce != cudaSuccess) return cuda_fail(ce, "capture of the CG iteration", __FILE__, __LINE__);
         CMCG_CUDA(cudaGraphInstantiate(&s->gexec, g, 0));
         s->gkey = key;
@@ -961,6 +1333,7 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
     CMCG_TRY(get_dinv(s, DT<VT>::id, &dinv));
     const int32_t path = choose_path(s, n_inst);
     const size_t vbytes = sizeof(VT) * static_cast<size_t>(p->rows) * ob;
+    CMCG_TRY(ensure_sell_values(s->A));
     SolveArgs<VT, MT> a = base_args<VT, MT>(s, ob);
     a.dinv = static_cast<const VT*>(dinv);
     a.dinv_b = s->A->batches;
@@ -1018,6 +1391,8 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     CMCG_TRY(get_dinv(s, CMCG_F32, &dinv));
     const size_t nv = static_cast<size_t>(p->rows) * ob;
     CMCG_TRY(ensure_buffer(&s->ref_ws, &s->ref_ws_bytes, 5 * nv * sizeof(float) + 256));
+    CMCG_TRY(ensure_sell_values(s->A));
+    if (Ao != s->A) CMCG_TRY(ensure_sell_values(Ao));
     float* w = static_cast<float*>(s->ref_ws);
     RefineArgs<MI, MO> a{};
     a.inner = mat_args<MI>(s->A);
@@ -1039,10 +1414,22 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     a.max_inner = s->max_iter;
     a.max_outer = max_outer;
     a.st = s->st;
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+    if (s->refine_method == CMCG_REFINE_RELIABLE && s->max_sys_rows <= kSmemMaxRows && s->use_smem) {
+        const int nmax = smem_rows(s->max_sys_rows);
+        const size_t sm = smem_bytes(nmax);
+        CMCG_TRY(allow_smem(k_reliable_smem<MI, MO, FMT>, sm));
+        const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
+        k_reliable_smem<MI, MO, FMT><<<grid, kSmemThreads, sm, ctx->stream>>>(a, nmax, static_cast<float>(s->refine_delta));
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        s->last_inst = n_inst;
+        s->last_refined = true;
+        return CMCG_OK;
+    }
     int occ = 0;
     CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persistent_refined<MI, MO, FMT>, kPersistThreads, 0));
     const int grid = std::max(1, std::min(n_inst, ctx->sm_count * std::max(occ, 1)));
-    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
     k_persistent_refined<MI, MO, FMT><<<grid, kPersistThreads, 0, ctx->stream>>>(a);
     count_launch();
     CMCG_CHECK_LAUNCH();
@@ -1120,7 +1507,9 @@ cmcg_status refined_grid(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t
         // inner solve A d = r32 (FP32) on the grid path
         const int32_t saved = s->path;
         s->path = CMCG_PATH_GRID;
+        s->inner_solve = true;   // the inner rhs shrinks with the residual: no absolute early-out
         rc = solve_vt<float>(s, r32, ob, nullptr, d32, ob);
+        s->inner_solve = false;
         s->path = saved;
         if (rc != CMCG_OK) return cleanup(rc);
         std::vector<int32_t> it(n_inst);
@@ -1175,6 +1564,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     CMCG_CUDA(cudaSetDevice(A->pat->ctx->device));
     auto* s = new cmcg_solver_s();
     s->A = A;
+    A->refs++;
     s->precond = precond;
     // default tolerance: epsilon of the scalar type (IterativeSolverBase.h:131)
     s->tol = (A->dtype == CMCG_F64) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
@@ -1203,7 +1593,9 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
                     s->st_ws, static_cast<void*>(s->counters)})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);
+    cmcg_matrix A = s->A;
     delete s;
+    matrix_release(A);
     return CMCG_OK;
 }
 
@@ -1230,8 +1622,20 @@ cmcg_status cmcg_cg_get_settings(cmcg_solver s, double* tol, int64_t* max_iter) 
 
 cmcg_status cmcg_cg_set_path(cmcg_solver s, int32_t path) {
     CMCG_REQUIRE(s, "cmcg_cg_set_path: NULL solver");
-    CMCG_REQUIRE(path == CMCG_PATH_AUTO || path == CMCG_PATH_PERSISTENT || path == CMCG_PATH_GRID, "cmcg_cg_set_path: bad path");
-    s->path = path;
+    CMCG_REQUIRE(path == CMCG_PATH_AUTO || path == CMCG_PATH_PERSISTENT || path == CMCG_PATH_GRID ||
+                     path == CMCG_PATH_PERSISTENT_GLOBAL,
+                 "cmcg_cg_set_path: bad path");
+    s->path = path == CMCG_PATH_PERSISTENT_GLOBAL ? CMCG_PATH_PERSISTENT : path;
+    s->use_smem = path != CMCG_PATH_PERSISTENT_GLOBAL;
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_set_refinement(cmcg_solver s, int32_t method, double delta) {
+    CMCG_REQUIRE(s, "cmcg_cg_set_refinement: NULL solver");
+    CMCG_REQUIRE(method == CMCG_REFINE_RELIABLE || method == CMCG_REFINE_RESTART, "cmcg_cg_set_refinement: bad method");
+    CMCG_REQUIRE(delta > 0.0 && delta < 1.0, "cmcg_cg_set_refinement: delta must be in (0, 1)");
+    s->refine_method = method;
+    s->refine_delta = delta;
     return CMCG_OK;
 }
 
@@ -1240,9 +1644,10 @@ cmcg_status cmcg_cg_solve(cmcg_solver s, int32_t vdt, const void* b, int32_t b_b
     CMCG_REQUIRE(b_batches >= 1, "cmcg_cg_solve: b_batches must be >= 1");
     CMCG_REQUIRE(s->A->batches == 1 || b_batches == 1 || b_batches == s->A->batches,
                  "cmcg_cg_solve: batch counts of matrix and rhs must match or be 1");
+    CMCG_CUDA(cudaSetDevice(s->A->pat->ctx->device));
+    CMCG_TRY(refresh_plan(s));
     const int32_t ob = std::max(s->A->batches, b_batches);
     CMCG_REQUIRE(static_cast<int64_t>(ob) * s->n_sys <= INT32_MAX / 2, "cmcg_cg_solve: too many systems");
-    CMCG_CUDA(cudaSetDevice(s->A->pat->ctx->device));
     if (vdt == CMCG_F32)
         return solve_vt<float>(s, static_cast<const float*>(b), b_batches, static_cast<const float*>(guess), static_cast<float*>(x), ob);
     if (vdt == CMCG_F64)
@@ -1334,8 +1739,12 @@ cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b
     CMCG_REQUIRE(b_batches >= 1 && (s->A->batches == 1 || b_batches == 1 || b_batches == s->A->batches),
                  "cmcg_cg_solve_refined: batch counts must match or be 1");
     CMCG_CUDA(cudaSetDevice(s->A->pat->ctx->device));
+    CMCG_TRY(refresh_plan(s));
     const int32_t ob = std::max(s->A->batches, b_batches);
-    const int32_t path = choose_path(s, ob * s->n_sys);
+    // packed systems always run persistent (the grid refinement drives one
+    // system per batch from the host)
+    int32_t path = choose_path(s, ob * s->n_sys);
+    if (s->n_sys > 1 && s->path == CMCG_PATH_AUTO) path = CMCG_PATH_PERSISTENT;
     if (path == CMCG_PATH_GRID) {
         CMCG_REQUIRE(s->n_sys == 1, "cmcg_cg_solve_refined: the grid path refines one system per batch");
         return refined_grid(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);

@@ -22,12 +22,84 @@ enum : int32_t { ST_RUNNING = -1 };
 template <typename VT>
 __device__ __forceinline__ bool finite_(VT v) { return isfinite(v); }
 
+template <typename MT> struct RowMat;
+
 // Matrix of one instance (batch) in either format.
+template <typename MT, int FMT>
+struct InstMatrix;
+
+// Row-major access for thread-per-row products. CSR patterns are read through
+// their sliced ELLPACK copy (32-row slices, column-major inside a slice,
+// padding = own column with value 0); ELLPACK patterns directly (stride
+// rows_pad, padding index -1). Rows of a warp must be the 32 rows of one slice
+// (row i of a system handled by lane i % 32), which makes every load of the
+// warp one 128-byte access.
+template <typename MT>
+struct RowMat {
+    const int32_t* __restrict__ col;
+    const MT* __restrict__ val;
+    const int64_t* __restrict__ slice_off;   // null: ELLPACK
+    const int32_t* __restrict__ slice_w;
+    const int32_t* __restrict__ sys_slice0;
+    int32_t ell_stride, ell_w;
+};
+
+constexpr int kRowUnroll = 4;
+
+// (A x)[row] for row i (local) of system s starting at global row r0.
+template <typename VT, typename MT, typename XF>
+__device__ __forceinline__ VT row_product(const RowMat<MT>& A, int s, int r0, int i, const XF& xf) {
+    int64_t base;
+    int stride, w;
+    if (A.slice_off) {
+        const int sl = __ldg(A.sys_slice0 + s) + (i >> 5);
+        base = __ldg(A.slice_off + sl) + (i & 31);
+        stride = 32;
+        w = __ldg(A.slice_w + sl);
+    } else {
+        base = r0 + i;
+        stride = A.ell_stride;
+        w = A.ell_w;
+    }
+    VT acc = VT(0);
+    int j0 = 0;
+    for (; j0 < w; j0 += kRowUnroll) {
+        int c[kRowUnroll];
+        MT v[kRowUnroll];
+#pragma unroll
+        for (int j = 0; j < kRowUnroll; ++j) {
+            if (j0 + j < w) {
+                const int64_t o = base + static_cast<int64_t>(j0 + j) * stride;
+                c[j] = __ldg(A.col + o);
+                v[j] = A.val[o];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kRowUnroll; ++j) {
+            if (j0 + j < w) {
+                if (A.slice_off) acc += mval<VT>(v[j]) * xf(c[j]);
+                else if (c[j] >= 0) acc += mval<VT>(v[j]) * xf(c[j]);
+            }
+        }
+    }
+    return acc;
+}
+
 template <typename MT, int FMT>
 struct InstMatrix {
     CsrView<MT> csr;
     EllView<MT> ell;
+    RowMat<MT> rm;
 };
+
+// Thread-per-row product over the local rows [i0, i0 + n) of system s (first
+// global row r0) with the whole CTA: thread t takes rows i0 + t, i0 + t +
+// blockDim.x, ... (i0 a multiple of 32); f(global row, value).
+template <typename VT, typename MT, int FMT, typename XF, typename F>
+__device__ __forceinline__ void cta_rows(const InstMatrix<MT, FMT>& A, int s, int r0, int i0, int n, const XF& xf,
+                                         F&& f) {
+    for (int i = i0 + threadIdx.x; i < i0 + n; i += blockDim.x) f(r0 + i, row_product<VT>(A.rm, s, r0, i, xf));
+}
 
 // Applies the product to the rows [r0, r0 + n) of one system with the whole
 // CTA: warp w takes the 32-row blocks w, w + W, ... so thread t always owns

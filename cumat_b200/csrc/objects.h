@@ -12,12 +12,36 @@ struct cmcg_ctx_s {
     int32_t device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // private stream used only to capture CUDA graphs (capture is not allowed on
+    // the legacy default stream); the captured graphs are launched on `stream`
+    cudaStream_t capture_stream = nullptr;
     int sm_count = 148;
     // scratch for the batched dot / squared-norm combine (grown on demand)
     void* red_partial = nullptr;
     size_t red_partial_bytes = 0;
     unsigned* red_ticket = nullptr;
     size_t red_ticket_count = 0;
+    // device error word (bounded waits that ran out set bits; read and cleared by
+    // cmcg_ctx_device_errors)
+    int32_t* d_err = nullptr;
+    // handle + every pattern created on it; freed when the last one is released
+    int refs = 1;
+};
+
+// Sliced ELLPACK copy of a CSR pattern used by the CG kernels: every system's
+// rows are cut into slices of 32 consecutive rows; a slice of width w (its
+// longest row) stores entry j of its row l at slice_off[slice] + j * 32 + l, so
+// a warp reading one entry of 32 rows makes one coalesced 128-byte access.
+// Padding slots carry the row's own column and value 0.
+struct SellPlan {
+    int64_t n_slots = 0;
+    int32_t n_slices = 0;
+    int32_t* d_col = nullptr;         // n_slots, global column index
+    int32_t* d_perm = nullptr;        // n_slots, CSR entry of the slot or -1 (padding)
+    int64_t* d_slice_off = nullptr;   // n_slices + 1
+    int32_t* d_slice_w = nullptr;     // n_slices
+    int32_t* d_sys_slice0 = nullptr;  // n_sys + 1, first slice of each system
+    int64_t plan_id = 0;              // changes when the systems change
 };
 
 // Sparsity pattern. CSR: row_ptr (rows+1) + col_idx (nnz), the reference's JA /
@@ -40,6 +64,14 @@ struct cmcg_pattern_s {
     // independent systems (diagonal blocks); default one system of all rows
     std::vector<int64_t> row_off;
     int32_t* d_row_off = nullptr;     // int32 copy, n_sys + 1
+    // row tiles of the bulk-staged CSR product (built on first use): tile t
+    // covers rows [tile_row0[t], tile_row0[t+1]), at most kTileRows rows and,
+    // unless it is a single long row, at most kTileNnz entries
+    int32_t n_spmv_tiles = 0;
+    int32_t* d_spmv_tiles = nullptr;
+    // sliced ELLPACK copy for the CG kernels (CSR only, built on first use)
+    SellPlan sell;
+    int64_t systems_version = 0;      // incremented by cmcg_pattern_set_systems
     int refs = 1;
 };
 
@@ -49,6 +81,15 @@ struct cmcg_matrix_s {
     int32_t batches = 1;
     int64_t stride = 0;      // elements between batches (CSR: nnz padded to 4; ELL: width * rows_pad)
     void* d_vals = nullptr;
+    int64_t version = 0;              // incremented by every value upload
+    // values in the pattern's sliced ELLPACK layout ([batch][n_slots_pad]),
+    // regathered when `version` or the plan changes
+    void* d_sell_vals = nullptr;
+    int64_t sell_stride = 0;
+    int64_t sell_version = -1;
+    int64_t sell_plan_id = -1;
+    // handle + every solver created on it; freed when the last one is released
+    int refs = 1;
 };
 
 namespace cmcg {
@@ -57,7 +98,13 @@ cmcg_status dev_alloc(void** p, size_t bytes);
 void dev_free(void* p);
 cmcg_status ensure_buffer(void** p, size_t* cur, size_t need);
 void pattern_release(cmcg_pattern p);
+void matrix_release(cmcg_matrix m);
+void ctx_release(cmcg_ctx c);
 int64_t csr_padded_nnz(int64_t nnz);
 // converts n elements between element types on the context stream
 cmcg_status convert(cmcg_ctx ctx, int src_dt, const void* src, int dst_dt, void* dst, int64_t n);
+// builds the pattern's sliced ELLPACK plan (CSR) and the matrix's values in it
+cmcg_status ensure_sell(cmcg_pattern p);
+cmcg_status ensure_sell_values(cmcg_matrix m);
+void free_sell(SellPlan& s);
 }  // namespace cmcg

@@ -58,7 +58,22 @@ cmcg_status ensure_buffer(void** p, size_t* cur, size_t need) {
     return CMCG_OK;
 }
 
-int64_t csr_padded_nnz(int64_t nnz) { return (nnz + 3) / 4 * 4 + (nnz == 0 ? 4 : 0); }
+// entries are padded to a multiple of 8 (16 bytes of BF16) and at least 8, so
+// every 16-byte aligned bulk copy of a row range stays inside the allocation
+int64_t csr_padded_nnz(int64_t nnz) { return (nnz + 7) / 8 * 8 + 8; }
+
+void ctx_release(cmcg_ctx c) {
+    if (!c) return;
+    if (--c->refs > 0) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    dev_free(c->red_partial);
+    dev_free(c->red_ticket);
+    dev_free(c->d_err);
+    if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
 
 void pattern_release(cmcg_pattern p) {
     if (!p) return;
@@ -67,7 +82,23 @@ void pattern_release(cmcg_pattern p) {
     dev_free(p->d_col);
     dev_free(p->d_ell);
     dev_free(p->d_row_off);
+    dev_free(p->d_spmv_tiles);
+    free_sell(p->sell);
+    cmcg_ctx c = p->ctx;
     delete p;
+    ctx_release(c);
+}
+
+void matrix_release(cmcg_matrix m) {
+    if (!m) return;
+    if (--m->refs > 0) return;
+    cudaSetDevice(m->pat->ctx->device);
+    cudaStreamSynchronize(m->pat->ctx->stream);
+    dev_free(m->d_vals);
+    dev_free(m->d_sell_vals);
+    cmcg_pattern p = m->pat;
+    delete m;
+    pattern_release(p);
 }
 
 namespace {
@@ -178,18 +209,29 @@ cmcg_status cmcg_ctx_create(int32_t device, void* stream, cmcg_ctx* out) {
         }
         c->own_stream = true;
     }
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&c->d_err), 16);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_err, 0, 16, c->stream);
+    if (e != cudaSuccess) {
+        ctx_release(c);
+        return cuda_fail(e, "device error word", __FILE__, __LINE__);
+    }
     *out = c;
     return CMCG_OK;
 }
 
 cmcg_status cmcg_ctx_destroy(cmcg_ctx ctx) {
-    if (!ctx) return CMCG_OK;
-    cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    dev_free(ctx->red_partial);
-    dev_free(ctx->red_ticket);
-    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
-    delete ctx;
+    // patterns still alive keep the context (and its stream) until they go
+    ctx_release(ctx);
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_ctx_device_errors(cmcg_ctx ctx, int32_t* flags) {
+    CMCG_REQUIRE(ctx && flags, "cmcg_ctx_device_errors: NULL argument");
+    CMCG_CUDA(cudaSetDevice(ctx->device));
+    CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
+    CMCG_CUDA(cudaMemcpy(flags, ctx->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CMCG_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream));
+    CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
     return CMCG_OK;
 }
 
@@ -229,6 +271,7 @@ cmcg_status cmcg_pattern_create_csr(cmcg_ctx ctx, int32_t rows, int32_t cols, in
     CMCG_CUDA(cudaSetDevice(ctx->device));
     auto* p = new cmcg_pattern_s();
     p->ctx = ctx;
+    ctx->refs++;
     p->format = CMCG_CSR;
     p->rows = rows;
     p->cols = cols;
@@ -250,12 +293,16 @@ cmcg_status cmcg_pattern_create_csr(cmcg_ctx ctx, int32_t rows, int32_t cols, in
         if (p->h_col[k] < 0 || p->h_col[k] >= cols)
             return cleanup(fail(CMCG_ERR_INVALID_ARGUMENT, "CSR column index out of range at entry " + std::to_string(k)));
     cmcg_status st;
-    if ((st = dev_alloc(reinterpret_cast<void**>(&p->d_row_ptr), (rows + 1) * sizeof(int32_t))) != CMCG_OK) return cleanup(st);
-    // col array padded to a multiple of 4 entries for 16-byte loads; padding = 0
+    // row_ptr padded with 8 copies of nnz and col with zeros to a multiple of 8
+    // entries, so 16-byte aligned vector loads and bulk copies of any row range
+    // stay inside the arrays
+    std::vector<int32_t> rp_pad(p->h_row_ptr);
+    rp_pad.resize(static_cast<size_t>(rows) + 1 + 8, static_cast<int32_t>(nnz));
+    if ((st = dev_alloc(reinterpret_cast<void**>(&p->d_row_ptr), rp_pad.size() * sizeof(int32_t))) != CMCG_OK) return cleanup(st);
     const int64_t npad = csr_padded_nnz(nnz);
     if ((st = dev_alloc(reinterpret_cast<void**>(&p->d_col), npad * sizeof(int32_t))) != CMCG_OK) return cleanup(st);
     if (cudaMemsetAsync(p->d_col, 0, npad * sizeof(int32_t), ctx->stream) != cudaSuccess ||
-        cudaMemcpyAsync(p->d_row_ptr, p->h_row_ptr.data(), (rows + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaMemcpy(p->d_row_ptr, rp_pad.data(), rp_pad.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
         (nnz && cudaMemcpyAsync(p->d_col, p->h_col.data(), nnz * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess))
         return cleanup(fail(CMCG_ERR_CUDA, "cmcg_pattern_create_csr: upload failed"));
     if ((st = upload_default_systems(p)) != CMCG_OK) return cleanup(st);
@@ -274,6 +321,7 @@ cmcg_status cmcg_pattern_create_ell(cmcg_ctx ctx, int32_t rows, int32_t cols, in
     CMCG_CUDA(cudaSetDevice(ctx->device));
     auto* p = new cmcg_pattern_s();
     p->ctx = ctx;
+    ctx->refs++;
     p->format = CMCG_ELLPACK;
     p->rows = rows;
     p->cols = cols;
@@ -326,6 +374,11 @@ cmcg_status cmcg_pattern_set_systems(cmcg_pattern p, int64_t n_sys, const int64_
         }
     }
     p->row_off.assign(row_off, row_off + n_sys + 1);
+    // the sliced layout depends on the systems: rebuild it on next use
+    cudaStreamSynchronize(p->ctx->stream);
+    free_sell(p->sell);
+    p->sell.plan_id++;
+    p->systems_version++;
     std::vector<int32_t> h(row_off, row_off + n_sys + 1);
     dev_free(p->d_row_off);
     p->d_row_off = nullptr;
@@ -431,6 +484,7 @@ cmcg_status cmcg_matrix_set_values(cmcg_matrix m, int32_t src_dtype, const void*
         cudaStreamSynchronize(ctx->stream);
         dev_free(stage);
     }
+    m->version++;
     return st;
 }
 
@@ -460,12 +514,8 @@ cmcg_status cmcg_matrix_info(cmcg_matrix m, int32_t* dtype, int32_t* batches) {
 }
 
 cmcg_status cmcg_matrix_destroy(cmcg_matrix m) {
-    if (!m) return CMCG_OK;
-    cudaSetDevice(m->pat->ctx->device);
-    cudaStreamSynchronize(m->pat->ctx->stream);
-    dev_free(m->d_vals);
-    pattern_release(m->pat);
-    delete m;
+    // solvers still alive keep the matrix until they are destroyed
+    matrix_release(m);
     return CMCG_OK;
 }
 

@@ -17,15 +17,29 @@
 // counter, no spinning).
 
 #include <algorithm>
+#include <cstdlib>
+#include <vector>
 
 #include "common.cuh"
 #include "objects.h"
 #include "spmv_dev.cuh"
+#include "tma.cuh"
 
 namespace cmcg {
 namespace {
 
 constexpr int kSpmvThreads = 256;
+
+// Stand-alone product kernels: 0 = bulk-staged CSR / four-rows-per-thread
+// ELLPACK (default), 1 = warp row-block CSR / thread-per-row ELLPACK. Chosen
+// once per process from CUMAT_SPMV_VARIANT (a tuning and comparison knob).
+int spmv_variant() {
+    static const int v = [] {
+        const char* e = std::getenv("CUMAT_SPMV_VARIANT");
+        return e ? std::atoi(e) : 0;
+    }();
+    return v;
+}
 
 template <int MODE, typename VT>
 __device__ __forceinline__ void assign_out(VT* y, VT v) {
@@ -71,6 +85,227 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell(const int32_t* __rest
     }
 }
 
+// ---- bulk-staged CSR product ----------------------------------------------------
+//
+// Persistent CTAs walk precomputed row tiles (<= kTileRows rows, <= kTileNnz
+// entries). For each tile one thread issues three cp.async.bulk copies (the
+// tile's row pointers, column indices and values, 16-byte aligned ranges) into a
+// shared-memory stage, completing on that stage's mbarrier; two stages are in
+// flight per CTA. Threads then take rows (thread per row), read their entries
+// from shared memory, gather x through the read-only path and write y. A tile
+// that is one row longer than kTileNnz is summed by the whole CTA from global
+// memory.
+
+constexpr int kTileRows = 512;
+constexpr int kTileNnz = 2048;
+constexpr int kTmaThreads = 256;
+
+template <typename MT>
+struct TileSmem {
+    static constexpr int kEpv = 16 / static_cast<int>(sizeof(MT));   // values per 16 bytes
+    static constexpr int kRp = kTileRows + 8;
+    static constexpr int kCol = kTileNnz + 8;
+    static constexpr int kVal = kTileNnz + 2 * kEpv;
+    static constexpr size_t kStageBytes = ((kRp + kCol) * 4 + kVal * sizeof(MT) + 15) / 16 * 16;
+};
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kTmaThreads) k_spmv_csr_tma(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                             const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                             const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                             VT* __restrict__ y, int32_t rows, int32_t ob,
+                                                             const int32_t* __restrict__ tiles, int32_t ntiles,
+                                                             int32_t* err) {
+    using L = TileSmem<MT>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ VT red[kTmaThreads / 32];
+    const int tid = threadIdx.x;
+    const int64_t items = static_cast<int64_t>(ntiles) * ob;
+    const int64_t G = gridDim.x;
+
+    auto stage_ptr = [&](int s) { return smem + s * L::kStageBytes; };
+    // issue the copies of item `it` into stage s (thread 0 only)
+    auto issue = [&](int64_t it, int s) {
+        const int b = static_cast<int>(it / ntiles);
+        const int t = static_cast<int>(it - static_cast<int64_t>(b) * ntiles);
+        const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
+        const int k0 = __ldg(rp + r0), k1 = __ldg(rp + r1);
+        unsigned char* st = stage_ptr(s);
+        const int ra = r0 & ~3, rb = (r1 + 1 + 3) & ~3;
+        uint32_t bytes = static_cast<uint32_t>(rb - ra) * 4u;
+        const bool stage_entries = (k1 - k0) <= kTileNnz && k1 > k0;
+        int ca = 0, cb = 0, va = 0, vb = 0;
+        if (stage_entries) {
+            ca = k0 & ~3; cb = (k1 + 3) & ~3;
+            va = k0 & ~(L::kEpv - 1); vb = (k1 + L::kEpv - 1) & ~(L::kEpv - 1);
+            bytes += static_cast<uint32_t>(cb - ca) * 4u + static_cast<uint32_t>(vb - va) * static_cast<uint32_t>(sizeof(MT));
+        }
+        mbar_arrive_expect_tx(&bar[s], bytes);
+        bulk_g2s(st, rp + ra, static_cast<uint32_t>(rb - ra) * 4u, &bar[s]);
+        if (stage_entries) {
+            const MT* vb_ = vals + (mb == 1 ? 0 : b * vstride);
+            bulk_g2s(st + L::kRp * 4, ci + ca, static_cast<uint32_t>(cb - ca) * 4u, &bar[s]);
+            bulk_g2s(st + (L::kRp + L::kCol) * 4, vb_ + va, static_cast<uint32_t>(vb - va) * sizeof(MT), &bar[s]);
+        }
+    };
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (blockIdx.x < items) issue(blockIdx.x, 0);
+        if (blockIdx.x + G < items) issue(blockIdx.x + G, 1);
+    }
+    int j = 0;
+    for (int64_t it = blockIdx.x; it < items; it += G, ++j) {
+        const int s = j & 1;
+        const bool ok = mbar_wait(&bar[s], (j >> 1) & 1, err);
+        const int b = static_cast<int>(it / ntiles);
+        const int t = static_cast<int>(it - static_cast<int64_t>(b) * ntiles);
+        const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
+        const unsigned char* st = stage_ptr(s);
+        const int32_t* srp = reinterpret_cast<const int32_t*>(st);
+        const int32_t* sci = reinterpret_cast<const int32_t*>(st + L::kRp * 4);
+        const MT* sva = reinterpret_cast<const MT*>(st + (L::kRp + L::kCol) * 4);
+        const int ra = r0 & ~3;
+        const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        VT* yv = y + static_cast<int64_t>(b) * rows;
+        if (ok) {
+            const int k0 = srp[r0 - ra], k1 = srp[r1 - ra];
+            if (k1 - k0 <= kTileNnz) {
+                const int ca = k0 & ~3, va = k0 & ~(L::kEpv - 1);
+                for (int r = r0 + tid; r < r1; r += kTmaThreads) {
+                    const int a = srp[r - ra], e = srp[r - ra + 1];
+                    VT acc = VT(0);
+                    for (int k = a; k < e; ++k) acc += mval<VT>(sva[k - va]) * __ldg(xv + sci[k - ca]);
+                    assign_out<MODE>(yv + r, acc);
+                }
+            } else {
+                // one long row: the CTA sums it from global memory
+                const MT* vb_ = vals + (mb == 1 ? 0 : b * vstride);
+                VT acc[1] = {VT(0)};
+                for (int k = k0 + tid; k < k1; k += kTmaThreads) acc[0] += mval<VT>(vb_[k]) * __ldg(xv + __ldg(ci + k));
+                block_sum<VT, 1>(acc, red);
+                if (tid == 0) assign_out<MODE>(yv + r0, acc[0]);
+            }
+        }
+        __syncthreads();   // stage s fully consumed
+        if (tid == 0 && it + 2 * G < items) {
+            fence_proxy_async();
+            issue(it + 2 * G, s);
+        }
+    }
+}
+
+// ---- ELLPACK, four rows per thread ---------------------------------------------------
+//
+// Column-major slabs with rows padded to a multiple of 4: each thread loads one
+// 16-byte vector of column indices and the matching values per slot for four
+// consecutive rows (coalesced across the warp), skips padding (index < 0) and
+// gathers x through the read-only path.
+
+template <typename MT> struct Vec4Load;
+template <> struct Vec4Load<float> {
+    __device__ __forceinline__ static void load(const float* p, float (&v)[4]) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+};
+template <> struct Vec4Load<double> {
+    __device__ __forceinline__ static void load(const double* p, double (&v)[4]) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 c = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+    }
+};
+template <> struct Vec4Load<__nv_bfloat16> {
+    __device__ __forceinline__ static void load(const __nv_bfloat16* p, __nv_bfloat16 (&v)[4]) {
+        const uint2 t = __ldg(reinterpret_cast<const uint2*>(p));
+        const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&t.x);
+        const __nv_bfloat162 c = *reinterpret_cast<const __nv_bfloat162*>(&t.y);
+        v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+    }
+};
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell4(const int32_t* __restrict__ idx, int32_t width, int32_t rows_pad,
+                                                            const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                            const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                            VT* __restrict__ y, int32_t rows, int32_t ob) {
+    const int quads = rows_pad >> 2;
+    const int64_t items = static_cast<int64_t>(quads) * ob;
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * kSpmvThreads) {
+        const int b = static_cast<int>(it / quads);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * quads) * 4;
+        const MT* v = vals + (mb == 1 ? 0 : b * vstride);
+        const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        VT acc[4] = {VT(0), VT(0), VT(0), VT(0)};
+        for (int j = 0; j < width; ++j) {
+            const int64_t o = r + static_cast<int64_t>(j) * rows_pad;
+            const int4 c = __ldg(reinterpret_cast<const int4*>(idx + o));
+            MT w[4];
+            Vec4Load<MT>::load(v + o, w);
+            if (c.x >= 0) acc[0] += mval<VT>(w[0]) * __ldg(xv + c.x);
+            if (c.y >= 0) acc[1] += mval<VT>(w[1]) * __ldg(xv + c.y);
+            if (c.z >= 0) acc[2] += mval<VT>(w[2]) * __ldg(xv + c.z);
+            if (c.w >= 0) acc[3] += mval<VT>(w[3]) * __ldg(xv + c.w);
+        }
+        VT* yv = y + static_cast<int64_t>(b) * rows + r;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (r + q < rows) assign_out<MODE>(yv + q, acc[q]);
+    }
+}
+
+cmcg_status ensure_spmv_tiles(cmcg_pattern p) {
+    if (p->d_spmv_tiles) return CMCG_OK;
+    std::vector<int32_t> t;
+    const auto& rp = p->h_row_ptr;
+    int32_t r = 0;
+    while (r < p->rows) {
+        t.push_back(r);
+        const int32_t start = r;
+        ++r;  // a tile holds at least one row (a long row alone)
+        if (rp[r] - rp[start] > kTileNnz) continue;
+        while (r < p->rows && r - start < kTileRows && rp[r + 1] - rp[start] <= kTileNnz) ++r;
+    }
+    t.push_back(p->rows);
+    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&p->d_spmv_tiles), t.size() * sizeof(int32_t)));
+    CMCG_CUDA(cudaMemcpy(p->d_spmv_tiles, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    p->n_spmv_tiles = static_cast<int32_t>(t.size() - 1);
+    return CMCG_OK;
+}
+
+template <typename MT, typename VT, int MODE>
+cmcg_status launch_csr_tma(cmcg_matrix A, const VT* xv, int32_t xb, VT* yv, int32_t ob) {
+    cmcg_pattern p = A->pat;
+    cmcg_ctx ctx = p->ctx;
+    CMCG_TRY(ensure_spmv_tiles(p));
+    const size_t sm = 2 * TileSmem<MT>::kStageBytes;
+    auto kern = k_spmv_csr_tma<MT, VT, MODE>;
+    static thread_local bool attr_set[3][2][3] = {};
+    bool& done = attr_set[DT<MT>::id][DT<VT>::id][MODE];
+    if (!done) {
+        CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        done = true;
+    }
+    int occ = 0;
+    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTmaThreads, sm));
+    const int64_t items = static_cast<int64_t>(p->n_spmv_tiles) * ob;
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, static_cast<int64_t>(ctx->sm_count) * std::max(occ, 1))));
+    kern<<<grid, kTmaThreads, sm, ctx->stream>>>(p->d_row_ptr, p->d_col, static_cast<const MT*>(A->d_vals), A->stride,
+                                                A->batches, xv, p->cols, xb, yv, p->rows, ob, p->d_spmv_tiles,
+                                                p->n_spmv_tiles, ctx->d_err);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
 template <typename MT, typename VT>
 cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode) {
     cmcg_pattern p = A->pat;
@@ -80,6 +315,27 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     const VT* xv = static_cast<const VT*>(x);
     VT* yv = static_cast<VT*>(y);
     const int max_blocks = ctx->sm_count * 8;
+    const int variant = spmv_variant();
+    if (p->format == CMCG_CSR && variant != 1) {
+        if (mode == CMCG_ASSIGN) return launch_csr_tma<MT, VT, CMCG_ASSIGN>(A, xv, xb, yv, ob);
+        if (mode == CMCG_ADD) return launch_csr_tma<MT, VT, CMCG_ADD>(A, xv, xb, yv, ob);
+        return launch_csr_tma<MT, VT, CMCG_SUB>(A, xv, xb, yv, ob);
+    }
+    if (p->format == CMCG_ELLPACK && variant != 1) {
+        const int64_t threads = static_cast<int64_t>(p->rows_pad / 4) * ob;
+        const int blocks = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
+#define CMCG_LAUNCH_ELL4(M)                                                                                      \
+    k_spmv_ell4<MT, VT, M><<<blocks, kSpmvThreads, 0, ctx->stream>>>(p->d_ell, p->width, p->rows_pad, vals,       \
+                                                                     A->stride, A->batches, xv, p->cols, xb, yv,  \
+                                                                     p->rows, ob)
+        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_ELL4(CMCG_ASSIGN);
+        else if (mode == CMCG_ADD) CMCG_LAUNCH_ELL4(CMCG_ADD);
+        else CMCG_LAUNCH_ELL4(CMCG_SUB);
+#undef CMCG_LAUNCH_ELL4
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        return CMCG_OK;
+    }
     if (p->format == CMCG_CSR) {
         const int64_t warps = static_cast<int64_t>((p->rows + 31) / 32) * ob;
         const int blocks = static_cast<int>(std::min<int64_t>((warps + 7) / 8, max_blocks));
@@ -185,7 +441,9 @@ __global__ void k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __res
         const int b = static_cast<int>(it / nblk);
         const int r0 = static_cast<int>(it - static_cast<int64_t>(b) * nblk) * 32;
         const int nr = min(32, rows - r0);
-        if (lane <= nr) bounds[warp][lane] = __ldg(rp + r0 + lane);
+        // nr + 1 bounds (up to 33): lane j loads bound j, lane 0 also the last one
+        if (lane < nr) bounds[warp][lane] = __ldg(rp + r0 + lane);
+        if (lane == 0) bounds[warp][nr] = __ldg(rp + r0 + nr);
         __syncwarp();
         const int lo = bounds[warp][0], hi = bounds[warp][nr];
         const VT* ub_ = u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows);

@@ -53,6 +53,11 @@ class ConjugateGradient:
         N.call("cmcg_cg_set_path", self.handle, int(path))
         return self
 
+    def set_refinement(self, method: int = N.REFINE_RELIABLE, delta: float = 0.1) -> "ConjugateGradient":
+        """Mixed-precision method of solve_refined: reliable updates (default) or restarts."""
+        N.call("cmcg_cg_set_refinement", self.handle, int(method), float(delta))
+        return self
+
     def tolerance(self) -> float:
         t, m = C.c_double(), C.c_int64()
         N.call("cmcg_cg_get_settings", self.handle, C.byref(t), C.byref(m))

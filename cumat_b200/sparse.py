@@ -47,9 +47,15 @@ class Context:
 
     _per_device: dict = {}
 
+    LEGACY_DEFAULT_STREAM = 1  # cudaStreamLegacy
+
     def __init__(self, device: int = 0, stream: Optional[int] = None):
+        """stream: a cudaStream_t value; None creates a private stream; 0 (torch's
+        default stream) is taken as the legacy default stream."""
         self.device = device
         h = C.c_void_p()
+        if stream == 0:
+            stream = self.LEGACY_DEFAULT_STREAM
         N.call("cmcg_ctx_create", device, C.c_void_p(stream) if stream else None, C.byref(h))
         self.handle = h
 

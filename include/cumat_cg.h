@@ -66,8 +66,15 @@ enum {
 /* solver execution paths (cmcg_cg_set_path) */
 enum {
     CMCG_PATH_AUTO = 0,
-    CMCG_PATH_PERSISTENT = 1,   /* one CTA per system, whole loop in one launch */
-    CMCG_PATH_GRID = 2          /* grid-wide fused kernels per iteration, CUDA graph */
+    CMCG_PATH_PERSISTENT = 1,         /* one CTA per system, whole loop in one launch; FP32
+                                         vectors of systems up to 16384 rows live in shared memory */
+    CMCG_PATH_GRID = 2,               /* grid-wide fused kernels per iteration, CUDA graph */
+    CMCG_PATH_PERSISTENT_GLOBAL = 3   /* persistent, vectors in global memory (comparison) */
+};
+/* mixed-precision methods (cmcg_cg_set_refinement) */
+enum {
+    CMCG_REFINE_RELIABLE = 0,   /* FP32 CG with FP64 residual replacement ("reliable updates") */
+    CMCG_REFINE_RESTART = 1     /* classical refinement: restart FP32 CG on each FP64 residual */
 };
 
 typedef struct cmcg_ctx_s* cmcg_ctx;
@@ -86,11 +93,16 @@ int32_t cmcg_version(void);
 int64_t cmcg_launch_count(void);
 
 /* Context = device + stream (reference Context, cuMat/src/Context.h:132-214).
- * stream == NULL creates a private non-blocking stream. */
+ * stream == NULL creates a private non-blocking stream; any cudaStream_t,
+ * cudaStreamLegacy ((void*)1) included, is used as given. */
 cmcg_status cmcg_ctx_create(int32_t device, void* stream, cmcg_ctx* out);
 cmcg_status cmcg_ctx_destroy(cmcg_ctx ctx);
 cmcg_status cmcg_ctx_synchronize(cmcg_ctx ctx);
 cmcg_status cmcg_ctx_stream(cmcg_ctx ctx, void** stream);
+/* Synchronises and returns (then clears) the context's device error bits: a
+ * bounded wait inside a kernel that ran out sets bit 0 (no reference
+ * counterpart; the reference has no device-side waits). */
+cmcg_status cmcg_ctx_device_errors(cmcg_ctx ctx, int32_t* flags);
 
 /* ---- sparsity patterns --------------------------------------------------- */
 
@@ -182,6 +194,10 @@ cmcg_status cmcg_cg_set_max_iterations(cmcg_solver s, int64_t max_iter);
 cmcg_status cmcg_cg_get_settings(cmcg_solver s, double* tol, int64_t* max_iter);
 /* Execution path (default AUTO). */
 cmcg_status cmcg_cg_set_path(cmcg_solver s, int32_t path);
+/* Mixed-precision method of cmcg_cg_solve_refined (default RELIABLE, delta 0.1:
+ * the FP32 recursive residual is replaced by the FP64 one whenever it has
+ * dropped by delta since the last replacement). No reference counterpart. */
+cmcg_status cmcg_cg_set_refinement(cmcg_solver s, int32_t method, double delta);
 /* Solves A x = b for every (batch, system) with vec_dtype F32 or F64 vectors
  * (reference solve / solveWithGuess, SolverBase.h:33-37, IterativeSolverBase.h:118-124;
  * algorithm ConjugateGradient.h:123-206). guess may be NULL (zero guess).

@@ -428,6 +428,111 @@ int orc_refined_packed(int64_t n_sys, const int64_t* row_off, const int32_t* rp,
     return 0;
 }
 
+// Mixed precision with reliable updates, per system (no reference counterpart;
+// residual replacement after van der Vorst & Ye 2000, reliable updates after
+// Clark et al. 2010): FP32 Jacobi/identity PCG whose increments are folded
+// into the FP64 solution and whose recursive residual is replaced by the FP64
+// residual b - A x (FP32 values upcast) whenever |r|^2 < delta^2 |r_last|^2 or
+// |r|^2 < tol^2 |b|^2; the direction p is kept. Stops when the FP64 residual
+// satisfies |r| < tol |b|. iters[s] = FP32 iterations, updates[s] =
+// replacements, err[s] = final FP64 relative residual.
+int orc_reliable_packed(int64_t n_sys, const int64_t* row_off, const int32_t* rp, const int32_t* ci, const float* val,
+                        const double* rhs, double* x, double tol, double delta, int64_t max_iter, int32_t max_updates,
+                        int precond, int bf16_inner, int64_t* iters, int32_t* updates, double* err) {
+    std::vector<float> t32;
+    std::vector<double> t64;
+    for (int64_t s = 0; s < n_sys; ++s) {
+        const int64_t r0 = row_off[s], n = row_off[s + 1] - row_off[s];
+        const int32_t* srp = rp + r0;
+        std::vector<float> vin(val + srp[0], val + srp[n]);
+        if (bf16_inner)
+            for (auto& v : vin) v = bf16_round(v);
+        const int32_t k0 = srp[0];
+        auto apply32 = [&](const float* xin, float* y) {
+            for (int64_t i = 0; i < n; ++i) {
+                float acc = 0.0f;
+                for (int32_t k = srp[i]; k < srp[i + 1]; ++k) acc += vin[k - k0] * xin[ci[k] - r0];
+                y[i] = acc;
+            }
+        };
+        const double* b = rhs + r0;
+        double* xs = x + r0;
+        std::vector<float> d(n, 1.0f), r(n), p(n), q(n), xk(n, 0.0f);
+        if (precond == 1)
+            for (int64_t i = 0; i < n; ++i) {
+                float dv = 0.0f;
+                for (int32_t k = srp[i]; k < srp[i + 1]; ++k)
+                    if (ci[k] == r0 + i) { dv = val[k]; break; }
+                d[i] = dv != 0.0f ? 1.0f / dv : 1.0f;
+            }
+        for (int64_t i = 0; i < n; ++i) {
+            xs[i] = 0.0;
+            r[i] = static_cast<float>(b[i]);
+            p[i] = d[i] * r[i];
+        }
+        const double bb = dot(b, b, n, t64);
+        std::vector<float> z(n);
+        for (int64_t i = 0; i < n; ++i) z[i] = r[i] * (d[i] * r[i]);
+        float rz = pairwise_sum(z.data(), n);
+        const double thr = tol * tol * bb;
+        double rr64 = bb, rmax2 = bb;
+        int64_t it = 0;
+        int32_t up = 0;
+        const int64_t mi = max_iter < 0 ? 2 * n : max_iter;
+        bool done = (bb == 0.0) || (rr64 < thr);
+        while (!done && it < mi && up < max_updates) {
+            apply32(p.data(), q.data());
+            const float pq = dot(p.data(), q.data(), n, t32);
+            const float alpha = rz / pq;
+            if (!(pq > 0.0f) || !std::isfinite(alpha)) break;
+            for (int64_t i = 0; i < n; ++i) {
+                xk[i] += alpha * p[i];
+                r[i] -= alpha * q[i];
+            }
+            const float rr = dot(r.data(), r.data(), n, t32);
+            for (int64_t i = 0; i < n; ++i) z[i] = r[i] * (d[i] * r[i]);
+            float rzn = pairwise_sum(z.data(), n);
+            ++it;
+            if (rr < static_cast<float>(delta * delta) * static_cast<float>(rmax2) || rr < static_cast<float>(thr)) {
+                for (int64_t i = 0; i < n; ++i) { xs[i] += static_cast<double>(xk[i]); xk[i] = 0.0f; }
+                std::vector<double> r64(n);
+                for (int64_t i = 0; i < n; ++i) {
+                    double acc = 0.0;
+                    for (int32_t k = srp[i]; k < srp[i + 1]; ++k) acc += static_cast<double>(val[k]) * xs[ci[k] - r0];
+                    r64[i] = b[i] - acc;
+                    r[i] = static_cast<float>(r64[i]);
+                }
+                rr64 = dot(r64.data(), r64.data(), n, t64);
+                rmax2 = rr64;
+                ++up;
+                for (int64_t i = 0; i < n; ++i) z[i] = r[i] * (d[i] * r[i]);
+                rzn = pairwise_sum(z.data(), n);
+                if (rr64 < thr) { done = true; break; }
+            }
+            if (!(rzn > 0.0f)) break;
+            const float beta = rzn / rz;
+            rz = rzn;
+            for (int64_t i = 0; i < n; ++i) p[i] = d[i] * r[i] + beta * p[i];
+        }
+        bool pending = false;
+        for (int64_t i = 0; i < n; ++i)
+            if (xk[i] != 0.0f) { xs[i] += static_cast<double>(xk[i]); pending = true; }
+        if (pending) {
+            std::vector<double> r64(n);
+            for (int64_t i = 0; i < n; ++i) {
+                double acc = 0.0;
+                for (int32_t k = srp[i]; k < srp[i + 1]; ++k) acc += static_cast<double>(val[k]) * xs[ci[k] - r0];
+                r64[i] = b[i] - acc;
+            }
+            rr64 = dot(r64.data(), r64.data(), n, t64);
+        }
+        iters[s] = it;
+        updates[s] = up;
+        err[s] = bb > 0 ? std::sqrt(rr64 / bb) : 0.0;
+    }
+    return 0;
+}
+
 // out[k] = alpha * u[row(k)] * v[col(k)] at the pattern's entries.
 int orc_sddmm_csr_f64(int32_t rows, const int32_t* rp, const int32_t* ci, double alpha, const double* u,
                       const double* v, double* out) {

@@ -45,6 +45,7 @@ def lib():
             "orc_cg_packed_f32": [i64, vp, vp, vp, vp, vp, vp, vp, f64, i64, C.c_int, vp, vp],
             "orc_cg_packed_f64": [i64, vp, vp, vp, vp, vp, vp, vp, f64, i64, C.c_int, vp, vp],
             "orc_refined_packed": [i64, vp, vp, vp, vp, vp, vp, f64, f64, i64, i32, C.c_int, C.c_int, vp, vp, vp],
+            "orc_reliable_packed": [i64, vp, vp, vp, vp, vp, vp, f64, f64, i64, i32, C.c_int, C.c_int, vp, vp, vp],
             "orc_sddmm_csr_f64": [i32, vp, vp, f64, vp, vp, vp],
             "orc_sddmm_csr_f32": [i32, vp, vp, C.c_float, vp, vp, vp],
         }
@@ -208,6 +209,23 @@ def refined_packed(row_off, rp, ci, val32, rhs64, inner_tol, outer_tol, max_inne
                              _p(x), float(inner_tol), float(outer_tol), int(max_inner), int(max_outer), int(precond),
                              1 if bf16_inner else 0, _p(outer), _p(inner), _p(err))
     return x, outer, inner, err
+
+
+def reliable_packed(row_off, rp, ci, val32, rhs64, tol, delta=0.1, max_iter=-1, max_updates=1000, precond=1,
+                    bf16_inner=False):
+    """FP32 PCG with FP64 reliable updates, per system.
+    Returns (x, FP32 iterations, replacements, final FP64 relative residual)."""
+    ro = np.ascontiguousarray(row_off, np.int64)
+    b = np.ascontiguousarray(rhs64, np.float64)
+    x = np.empty_like(b)
+    S = ro.size - 1
+    it = np.empty(S, np.int64)
+    up = np.empty(S, np.int32)
+    err = np.empty(S, np.float64)
+    lib().orc_reliable_packed(S, _p(ro), _p(_i32(rp)), _p(_i32(ci)), _p(np.ascontiguousarray(val32, np.float32)), _p(b),
+                              _p(x), float(tol), float(delta), int(max_iter), int(max_updates), int(precond),
+                              1 if bf16_inner else 0, _p(it), _p(up), _p(err))
+    return x, it, up, err
 
 
 def sddmm_csr(rows, rp, ci, u, v, alpha=1.0):

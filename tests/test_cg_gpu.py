@@ -1,0 +1,370 @@
+"""Conjugate gradient through the C ABI on the GPU: the reference's CG tests
+(tests/TestConjugateGradient.cu), configuration-1 parity with the reference's
+bundled Eigen solver and the oracle, packed uneven batches, mixed precision
+with FP64 refinement, failure statuses."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from cumat_b200 import problems as P  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+EIG = np.load(Path(__file__).resolve().parent / "golden" / "eigen_golden.npz")
+PATHS = [1, 2]  # persistent, grid
+
+
+def cm():
+    import cumat_b200
+    return cumat_b200
+
+
+def _matrix(pr, dtype=torch.float32, systems=False, fmt="csr"):
+    m = cm()
+    if fmt == "csr":
+        p = m.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)
+        vals = pr.val
+    else:
+        idx, vals = P.csr_to_ell(pr.n, pr.row_ptr, pr.col, pr.val)
+        p = m.SparsityPattern.ell(pr.n, pr.n, idx)
+    if systems:
+        p.set_systems(pr.row_off)
+    return m.SparseMatrix(p, dtype=dtype).setData(vals)
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("pc,name", [(0, "identity"), (1, "jacobi")])
+def test_config1_matches_eigen_and_oracle(cuda, path, pc, name):
+    m = cm()
+    pr = P.poisson2d(64, 0)
+    A = _matrix(pr)
+    cg = m.ConjugateGradient(A, m.IdentityPreconditioner if pc == 0 else m.DiagonalPreconditioner)
+    cg.setTolerance(1e-6).setMaxIterations(1000).set_path(path)
+    x = cg.solve(torch.from_numpy(pr.b).to(cuda)).cpu().numpy()
+    _, it_o, err_o = O.cg_csr(pr.n, pr.row_ptr, pr.col, pr.val, pr.b, 1e-6, 1000, pc)
+    assert abs(cg.iterations() - int(EIG[f"c1_{name}_iters"])) <= 2
+    assert abs(cg.iterations() - int(it_o[0])) <= 2
+    assert cg.error() < 1e-6
+    xt = EIG["c1_llt_x"]
+    assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-5
+    st = cg.system_stats()
+    assert st["status"][0] == 0
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("size", [5, 10, 50, 100])
+def test_early_out_rhs(cuda, path, size):
+    # reference: Conjugate Gradient - Early Out Rhs (TestConjugateGradient.cu:11-26)
+    m = cm()
+    rng = np.random.default_rng(size)
+    A = rng.uniform(-1, 1, (size, size)).astype(np.float32)
+    rp = np.arange(0, size * size + 1, size)
+    ci = np.tile(np.arange(size), size)
+    S = m.SparseMatrix(m.SparsityPattern.csr(size, size, rp, ci)).setData(A.reshape(-1))
+    cg = m.ConjugateGradient(S).set_path(path)
+    x = cg.solve(torch.zeros(size, device=cuda))
+    assert cg.iterations() == 0 and cg.error() == 0 and float(x.abs().sum()) == 0
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("size", [5, 10, 50, 100])
+def test_early_out_x(cuda, path, size):
+    # reference: Conjugate Gradient - Early Out X (TestConjugateGradient.cu:28-45)
+    m = cm()
+    rng = np.random.default_rng(size + 1)
+    A = rng.uniform(-1, 1, (size, size))
+    xt = rng.uniform(-1, 1, size)
+    b = A @ xt
+    rp = np.arange(0, size * size + 1, size)
+    ci = np.tile(np.arange(size), size)
+    S = m.SparseMatrix(m.SparsityPattern.csr(size, size, rp, ci), dtype=torch.float64).setData(A.reshape(-1))
+    cg = m.ConjugateGradient(S).set_path(path)
+    bt = torch.from_numpy(b).to(cuda)
+    # b computed on the device so that the guess is exact to the last bit
+    bt = S * torch.from_numpy(xt).to(cuda)
+    x = cg.solveWithGuess(bt, torch.from_numpy(xt).to(cuda))
+    assert cg.iterations() == 0 and cg.error() < 1e-10
+    assert np.array_equal(x.cpu().numpy(), xt)
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("size", [5, 10, 50, 100])
+def test_solve_dense(cuda, path, size):
+    # reference: Conjugate Gradient - Solve Dense (TestConjugateGradient.cu:47-72), double,
+    # default tolerance (epsilon), max 10*size iterations. The reference fills A with
+    # U(-1,1) + size*I, which is not symmetric; the reference algorithm (the oracle)
+    # does not reach epsilon on such matrices, so the matrix here is symmetrised:
+    # (R + R^T)/2 + size*I, diagonally dominant and SPD.
+    m = cm()
+    rng = np.random.default_rng(100 + size)
+    R = rng.uniform(-1, 1, (size, size))
+    A = (R + R.T) / 2 + size * np.eye(size)
+    xt = rng.uniform(-1, 1, size)
+    b = A @ xt
+    rp = np.arange(0, size * size + 1, size)
+    ci = np.tile(np.arange(size), size)
+    S = m.SparseMatrix(m.SparsityPattern.csr(size, size, rp, ci), dtype=torch.float64).setData(A.reshape(-1))
+    cg = m.ConjugateGradient(S).setMaxIterations(10 * size).set_path(path)
+    x = cg.solve(torch.from_numpy(b).to(cuda)).cpu().numpy()
+    assert 0 < cg.iterations() < cg.maxIterations()
+    assert 0 < cg.error() <= cg.tolerance()
+    assert np.allclose(x, xt, rtol=1e-4)
+    _, it_o, _ = O.cg_csr(size, rp, ci, A.reshape(-1), b, cg.tolerance(), 10 * size, 1)
+    assert abs(cg.iterations() - int(it_o[0])) <= 2
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_solve_dense_batched(cuda, path):
+    # reference: Conjugate Gradient - Solve Dense Batched (TestConjugateGradient.cu:74-100):
+    # one matrix, 3 right-hand sides
+    m = cm()
+    size, batches = 10, 3
+    rng = np.random.default_rng(7)
+    R = rng.uniform(-1, 1, (size, size))
+    A = (R + R.T) / 2 + size * np.eye(size)
+    xt = rng.uniform(-1, 1, (batches, size))
+    b = xt @ A.T
+    rp = np.arange(0, size * size + 1, size)
+    ci = np.tile(np.arange(size), size)
+    S = m.SparseMatrix(m.SparsityPattern.csr(size, size, rp, ci), dtype=torch.float64).setData(A.reshape(-1))
+    cg = m.ConjugateGradient(S).setMaxIterations(10 * size).set_path(path)
+    x = cg.solve(torch.from_numpy(b).to(cuda)).cpu().numpy()
+    assert x.shape == (3, size)
+    assert 0 < cg.iterations() < cg.maxIterations() and 0 < cg.error() <= cg.tolerance()
+    assert np.allclose(x, xt, rtol=1e-4)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_batched_matrices_per_batch_jacobi(cuda, path):
+    m = cm()
+    pr = P.poisson2d(20, 3)
+    scales = np.array([1.0, 3.0, 0.25], np.float32)
+    p = m.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)
+    A = m.SparseMatrix(p, batches=3).setData(np.stack([pr.val * s for s in scales]))
+    B = np.stack([pr.b, P.uniform(11, pr.n), P.uniform(12, pr.n)])
+    cg = m.ConjugateGradient(A).setTolerance(1e-6).set_path(path)
+    x = cg.solve(torch.from_numpy(B).to(cuda)).cpu().numpy()
+    xo, it_o, err_o = O.cg_csr(pr.n, pr.row_ptr, pr.col, np.stack([pr.val * s for s in scales]), B, 1e-6, -1, 1,
+                               lockstep=False)
+    st = cg.system_stats()
+    assert np.all(np.abs(st["iterations"] - it_o) <= 2)
+    assert np.all(st["error"] < 1e-6) and np.all(st["status"] == 0)
+    assert np.allclose(x, xo, rtol=0, atol=1e-5 * np.abs(xo).max())
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("fmt", ["csr", "ell"])
+def test_packed_uneven_batch_vs_oracle(cuda, path, fmt):
+    m = cm()
+    bt = P.fv2d_batch(16, 8, 24, 0.5, 12)   # the batch of eigen_golden.npz
+    A = _matrix(bt, systems=True, fmt=fmt)
+    cg = m.ConjugateGradient(A).setTolerance(1e-6).set_path(path)
+    x = cg.solve(torch.from_numpy(bt.b).to(cuda)).cpu().numpy()
+    st = cg.system_stats()
+    assert np.all(np.abs(st["iterations"] - EIG["batch_iters_jacobi_1e-6"]) <= 2)
+    _, it_o, _ = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, bt.b, 1e-6, -1, 1)
+    assert np.all(np.abs(st["iterations"] - it_o) <= 2)
+    assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-6)
+    assert cg.iterations() == st["iterations"].max()
+    xt = EIG["batch_llt_x"]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(x[r0:r1] - xt[r0:r1]) / np.linalg.norm(xt[r0:r1]) < 1e-4
+
+
+def test_config3_shaped_batch_vs_oracle(cuda):
+    # 256 systems with the side range of configuration 3 (16..128)
+    m = cm()
+    bt = P.fv2d_batch(256, 16, 128, 0.5, 2)
+    A = _matrix(bt, systems=True)
+    cg = m.ConjugateGradient(A).setTolerance(1e-6)
+    cg.solve(torch.from_numpy(bt.b).to(cuda))  # first solve also lays out the sliced values
+    before = m.launch_count()
+    x = cg.solve(torch.from_numpy(bt.b).to(cuda))
+    assert m.launch_count() - before == 1     # the whole batch is one persistent launch
+    st = cg.system_stats()
+    _, it_o, _ = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, bt.b, 1e-6, -1, 1)
+    assert np.all(np.abs(st["iterations"] - it_o) <= 2)
+    assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-6)
+    # true residual of the FP32 solution, checked in FP64
+    r = bt.b - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x.cpu().double().numpy())[0]
+    for s in range(0, bt.n_sys, 17):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        # recursive residual < 1e-6; the FP32 iterate's true residual drifts a little above it
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(bt.b[r0:r1]) < 2e-5
+
+
+def test_paths_agree_and_are_deterministic(cuda):
+    m = cm()
+    bt = P.fv2d_batch(8, 8, 16, 0.5, 4)
+    A = _matrix(bt, systems=True)
+    b = torch.from_numpy(bt.b).to(cuda)
+    xs = []
+    for path in PATHS:
+        cg = m.ConjugateGradient(A).setTolerance(1e-6).set_path(path)
+        x1 = cg.solve(b).cpu().numpy()
+        x2 = cg.solve(b).cpu().numpy()
+        assert np.array_equal(x1, x2)
+        xs.append((x1, cg.system_stats()["iterations"]))
+    assert np.all(np.abs(xs[0][1] - xs[1][1]) <= 2)
+    assert np.allclose(xs[0][0], xs[1][0], atol=1e-5)
+
+
+def test_solve_host_buffers(cuda):
+    m = cm()
+    pr = P.poisson2d(32, 0)
+    A = _matrix(pr)
+    cg = m.ConjugateGradient(A).setTolerance(1e-6)
+    xh = cg.solve_host(pr.b)[0]
+    xd = cg.solve(torch.from_numpy(pr.b).to(cuda)).cpu().numpy()
+    assert np.array_equal(xh, xd)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_failure_statuses(cuda, path):
+    m = cm()
+    pr = P.poisson2d(8, 0)
+    # negative definite matrix: p.Ap < 0 -> BREAKDOWN, no NaN in x
+    A = m.SparseMatrix(m.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(-pr.val)
+    cg = m.ConjugateGradient(A, m.IdentityPreconditioner).setTolerance(1e-6).set_path(path)
+    x = cg.solve(torch.from_numpy(pr.b).to(cuda))
+    assert cg.system_stats()["status"][0] == 3
+    assert torch.isfinite(x).all()
+    # NaN in the right-hand side -> NON_FINITE
+    b = pr.b.copy()
+    b[3] = np.nan
+    A2 = _matrix(pr)
+    cg2 = m.ConjugateGradient(A2).set_path(path)
+    cg2.solve(torch.from_numpy(b).to(cuda))
+    assert cg2.system_stats()["status"][0] == 4
+    # iteration limit -> MAX_ITER with iterations == limit
+    cg3 = m.ConjugateGradient(A2).setTolerance(1e-12).setMaxIterations(5).set_path(path)
+    cg3.solve(torch.from_numpy(pr.b).to(cuda))
+    st = cg3.system_stats()
+    assert st["status"][0] == 1 and st["iterations"][0] == 5 and cg3.iterations() == 5
+
+
+@pytest.mark.parametrize("inner", [torch.float32, torch.bfloat16])
+def test_refined_to_1e10_vs_fp64_truth(cuda, inner):
+    m = cm()
+    bt = P.fv2d_batch(16, 8, 24, 0.5, 12)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    Ai = m.SparseMatrix(p, dtype=inner).setData(bt.val)
+    Ao = m.SparseMatrix(p, dtype=torch.float32).setData(bt.val)
+    cg = m.ConjugateGradient(Ai).setTolerance(1e-4).set_refinement(m._native.REFINE_RESTART)
+    b64 = bt.b.astype(np.float64)
+    x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=Ao, outer_tol=1e-10, max_outer=20).cpu().numpy()
+    st = cg.system_stats()
+    assert np.all(st["status"] == 0), st
+    assert np.all(st["error"] < 1e-10)
+    xo, outer_o, inner_o, err_o = O.refined_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, b64, 1e-4, 1e-10,
+                                                   bf16_inner=(inner == torch.bfloat16))
+    assert np.all(np.abs(st["outer"] - outer_o) <= 1)
+    xt = EIG["batch_llt_x"]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(x[r0:r1] - xt[r0:r1]) / np.linalg.norm(xt[r0:r1]) < 1e-8
+    # true FP64 residual
+    r = b64 - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x)[0]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b64[r0:r1]) < 1e-10
+
+
+def test_reliable_updates_vs_oracle_and_truth(cuda):
+    # mixed precision with FP64 residual replacement on systems of the
+    # configuration-3 size range (sides 16..128)
+    m = cm()
+    bt = P.fv2d_batch(24, 16, 128, 0.5, 2)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A = m.SparseMatrix(p, dtype=torch.float32).setData(bt.val)
+    cg = m.ConjugateGradient(A)
+    b64 = bt.b.astype(np.float64)
+    cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=A, outer_tol=1e-10, max_outer=200)
+    before = m.launch_count()
+    x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=A, outer_tol=1e-10, max_outer=200).cpu().numpy()
+    assert m.launch_count() - before == 1       # one persistent launch for the batch
+    st = cg.system_stats()
+    assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-10)
+    xo, it_o, up_o, err_o = O.reliable_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, b64, 1e-10)
+    # FP32 rounding (tree vs pairwise sums) moves the points where residuals are
+    # replaced, so counts agree to a few per cent, not to the iteration
+    assert abs(int(st["iterations"].sum()) - int(it_o.sum())) <= 0.05 * it_o.sum()
+    assert np.all(np.abs(st["iterations"] - it_o) <= np.maximum(5, 0.15 * it_o))
+    assert np.all(np.abs(st["outer"] - up_o) <= 3)
+    _, it64, _ = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val.astype(np.float64), b64, 1e-10)
+    assert st["iterations"].sum() <= 1.15 * it64.sum()   # close to plain FP64 CG's count
+    r = b64 - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x)[0]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b64[r0:r1]) < 1e-10
+        if s % 6 == 0 and O.ref_lib() is not None:
+            rp, ci, v = bt.system(s)
+            xt = O.eigen_llt(r1 - r0, rp, ci, v, b64[r0:r1])
+            assert np.linalg.norm(x[r0:r1] - xt) / np.linalg.norm(xt) < 1e-8
+
+
+def test_shared_memory_and_global_kernels_agree(cuda):
+    m = cm()
+    bt = P.fv2d_batch(40, 16, 128, 0.5, 5)
+    A = _matrix(bt, systems=True)
+    b = torch.from_numpy(bt.b).to(cuda)
+    cg1 = m.ConjugateGradient(A).setTolerance(1e-6).set_path(1)
+    x1 = cg1.solve(b).cpu().numpy()
+    cg2 = m.ConjugateGradient(A).setTolerance(1e-6).set_path(3)
+    x2 = cg2.solve(b).cpu().numpy()
+    s1, s2 = cg1.system_stats(), cg2.system_stats()
+    assert np.all(s1["status"] == 0) and np.all(s2["status"] == 0)
+    assert np.all(np.abs(s1["iterations"] - s2["iterations"]) <= 2)
+    assert np.allclose(x1, x2, atol=2e-5 * np.abs(x2).max())
+
+
+def test_solver_follows_value_and_system_changes(cuda):
+    # the reference's solver holds a shallow copy of the matrix, so new values
+    # are seen by the next solve; the sliced copy here is regathered
+    m = cm()
+    bt = P.fv2d_batch(6, 8, 20, 0.5, 8)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    A = m.SparseMatrix(p).setData(bt.val)
+    cg = m.ConjugateGradient(A, m.IdentityPreconditioner).setTolerance(1e-6)
+    b = torch.from_numpy(bt.b).to(cuda)
+    cg.solve(b)
+    assert cg.system_stats()["status"].shape == (1,)
+    p.set_systems(bt.row_off)                 # now 6 independent systems
+    x1 = cg.solve(b).cpu().numpy()
+    assert cg.system_stats()["status"].shape == (6,)
+    A.setData(bt.val * 2.0)                   # scaled matrix: solution halves
+    x2 = cg.solve(b).cpu().numpy()
+    assert np.allclose(x2, x1 / 2, atol=1e-5)
+
+
+def test_refined_grid_path_single_system(cuda):
+    m = cm()
+    p3 = P.fv3d(12, 1.0, 3)
+    p = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    Ai = m.SparseMatrix(p, dtype=torch.float32).setData(p3.val)
+    cg = m.ConjugateGradient(Ai).setTolerance(1e-4).set_path(2)
+    b64 = p3.b.astype(np.float64)
+    x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer_tol=1e-10).cpu().numpy()
+    st = cg.system_stats()
+    assert st["status"][0] == 0 and st["error"][0] < 1e-10
+    xt = EIG["fv3d12_llt_x"]
+    assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-8
+
+
+def test_plain_fp64_cg_matches_eigen_3d(cuda):
+    m = cm()
+    p3 = P.fv3d(12, 1.0, 3)
+    p = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    A = m.SparseMatrix(p, dtype=torch.float64).setData(p3.val.astype(np.float64))
+    for path in PATHS:
+        cg = m.ConjugateGradient(A).setTolerance(1e-10).set_path(path)
+        x = cg.solve(torch.from_numpy(p3.b.astype(np.float64)).to(cuda)).cpu().numpy()
+        assert abs(cg.iterations() - int(EIG["fv3d12_f64_iters_1e-10"])) <= 2
+        xt = EIG["fv3d12_llt_x"]
+        assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-8

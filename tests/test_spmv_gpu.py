@@ -1,0 +1,196 @@
+"""SpMV, reductions and the sampled outer product through the C ABI on the GPU,
+against the reference's known answers and the CPU oracle."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from cumat_b200 import problems as P  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+KAT = json.loads((Path(__file__).resolve().parent / "golden" / "reference_kats.json").read_text())
+
+
+def _cm():
+    import cumat_b200 as cm
+    return cm
+
+
+def _csr_pattern(k):
+    cm = _cm()
+    return cm.SparsityPattern.csr(k["rows"], k["cols"], k["JA"], k["IA"])
+
+
+def test_kat_csr_product(cuda):
+    cm = _cm()
+    k = KAT["spmv_csr"]
+    A = cm.SparseMatrix(_csr_pattern(k)).setData(np.array(k["values"], np.float32))
+    x = torch.tensor(k["x"], dtype=torch.float32, device=cuda)
+    before = cm.launch_count()
+    y = A * x
+    assert cm.launch_count() - before == 1          # one kernel per product
+    assert y.cpu().tolist() == k["y"]
+    k2 = KAT["spmv_csr_scaled_matrix"]
+    A2 = cm.SparseMatrix(_csr_pattern(k)).setData(np.array(k["values"], np.float32) * k2["scale"])
+    assert (A2 * x).cpu().tolist() == k2["y"]
+
+
+@pytest.mark.parametrize("case", ["spmv_csr_batched_matrix", "spmv_csr_batched_vector", "spmv_csr_batched_both"])
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+def test_kat_csr_batched(cuda, case, dt):
+    cm = _cm()
+    k = KAT[case]
+    ms, vs = k.get("matrix_scales", [1]), k.get("vector_scales", [1])
+    vals = np.stack([np.array(k["values"], np.float64) * s for s in ms])
+    A = cm.SparseMatrix(_csr_pattern(k), dtype=dt, batches=len(ms)).setData(vals)
+    X = torch.tensor(np.stack([np.array(k["x"], np.float64) * s for s in vs]), dtype=dt, device=cuda)
+    y = A.product(X)
+    expect = np.stack([np.array(k["y"], np.float64) * s for s in k["y_scales"]])
+    assert np.array_equal(y.cpu().numpy(), expect)
+
+
+@pytest.mark.parametrize("case", ["spmv_ell", "spmv_ell_batched_both"])
+def test_kat_ell(cuda, case):
+    cm = _cm()
+    k = KAT[case]
+    p = cm.SparsityPattern.ell(k["rows"], k["cols"], k["indices"])
+    ms, vs = k.get("matrix_scales", [1]), k.get("vector_scales", [1])
+    vals = np.stack([np.array(k["values"], np.float32) * s for s in ms])
+    A = cm.SparseMatrix(p, batches=len(ms)).setData(vals)
+    X = torch.tensor(np.stack([np.array(k["x"], np.float32) * s for s in vs]), device=cuda)
+    y = A.product(X)
+    expect = np.stack([np.array(k["y"], np.float32) * s for s in k.get("y_scales", [1])])
+    assert np.array_equal(y.cpu().numpy().reshape(expect.shape), expect)
+    # the pattern round-trips bit-exactly, padding -1 included
+    assert np.array_equal(p.download(), np.array(k["indices"], np.int32))
+
+
+def _random_csr(rng, rows, cols, max_len, empty_frac=0.1):
+    lens = rng.integers(0, max_len + 1, rows)
+    lens[rng.random(rows) < empty_frac] = 0
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(cols, l, replace=False)) for l in lens]).astype(np.int32) if lens.sum() else np.zeros(0, np.int32)
+    return rp, ci
+
+
+@pytest.mark.parametrize("max_len", [1, 5, 40, 300])
+@pytest.mark.parametrize("mdt", [torch.float32, torch.float64, torch.bfloat16])
+def test_random_csr_vs_oracle(cuda, max_len, mdt):
+    cm = _cm()
+    rng = np.random.default_rng(max_len)
+    rows, cols = 777, 901
+    rp, ci = _random_csr(rng, rows, cols, max_len)
+    vals = rng.uniform(-1, 1, (2, ci.size)).astype(np.float32)
+    if mdt == torch.bfloat16:
+        vals = O.bf16_round(vals)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(rows, cols, rp, ci), dtype=mdt, batches=2).setData(vals)
+    for vdt, npdt, tol in [(torch.float32, np.float32, 1e-6), (torch.float64, np.float64, 1e-13)]:
+        x = rng.uniform(-1, 1, (2, cols)).astype(npdt)
+        y = A.product(torch.from_numpy(x).to(cuda)).cpu().numpy()
+        ref = O.spmv_csr(rows, cols, rp, ci, vals.astype(np.float64), x.astype(np.float64))
+        scale = O.spmv_csr(rows, cols, rp, ci, np.abs(vals).astype(np.float64), np.abs(x).astype(np.float64))
+        assert np.all(np.abs(y - ref) <= tol * np.maximum(scale, 1e-30) + 1e-30)
+        assert np.all(y[:, np.diff(rp) == 0] == 0)   # empty rows give 0
+
+
+def test_assignment_modes(cuda):
+    cm = _cm()
+    k = KAT["spmv_csr"]
+    A = cm.SparseMatrix(_csr_pattern(k)).setData(np.array(k["values"], np.float32))
+    x = torch.tensor(k["x"], dtype=torch.float32, device=cuda)
+    y = torch.ones(4, device=cuda)
+    A.product(x, out=y, mode=1)
+    assert y.cpu().tolist() == [v + 1 for v in k["y"]]
+    A.product(x, out=y, mode=2)
+    assert y.cpu().tolist() == [1.0] * 4
+
+
+def test_poisson_1024_product_and_ell_agree(cuda):
+    cm = _cm()
+    pr = P.poisson2d(1024, 1)
+    p = cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)
+    A = cm.SparseMatrix(p).setData(pr.val)
+    idx, ev = P.csr_to_ell(pr.n, pr.row_ptr, pr.col, pr.val)
+    E = cm.SparseMatrix(cm.SparsityPattern.ell(pr.n, pr.n, idx)).setData(ev)
+    x = torch.from_numpy(pr.b).to(cuda)
+    y = A * x
+    ye = E * x
+    ref = O.spmv_csr(pr.n, pr.n, pr.row_ptr, pr.col, pr.val, pr.b)[0]
+    assert np.array_equal(y.cpu().numpy(), ref)       # exact: integer-valued stencil, one rounding per row
+    assert np.array_equal(ye.cpu().numpy(), ref)
+    ja, ia = p.download()
+    assert np.array_equal(ja, pr.row_ptr) and np.array_equal(ia, pr.col)
+    assert np.array_equal(A.getData()[0], pr.val)
+
+
+def test_kat_dot_norm(cuda):
+    cm = _cm()
+    k = KAT["dot"]
+    x = torch.tensor(k["x"], dtype=torch.float64, device=cuda)
+    y = torch.tensor(k["y"][0], dtype=torch.float64, device=cuda)
+    assert cm.dot(x, y.unsqueeze(0)).cpu().tolist() == k["out"]
+    assert cm.dot(y.unsqueeze(0), x).cpu().tolist() == k["out"]
+    k = KAT["squared_norm"]
+    x = torch.tensor(k["x"], dtype=torch.float64, device=cuda)
+    assert cm.squaredNorm(x).cpu().tolist() == k["out"]
+    assert np.allclose(cm.norm(x).cpu().numpy(), k["norm"], rtol=1e-15)
+
+
+@pytest.mark.parametrize("n", [1, 10, 1000, 100000, 1000000, 10000001])
+def test_large_reductions(cuda, n):
+    cm = _cm()
+    rng = np.random.default_rng(n)
+    a = rng.uniform(-1, 1, (3, n))
+    b = rng.uniform(-1, 1, (3, n))
+    ref = (a * b).sum(1)
+    for dt, tol in [(torch.float64, 1e-12), (torch.float32, 2e-5)]:
+        xa = torch.from_numpy(a).to(dt).to(cuda)
+        xb = torch.from_numpy(b).to(dt).to(cuda)
+        got = cm.dot(xa, xb).cpu().double().numpy()
+        scale = (np.abs(a) * np.abs(b)).sum(1)
+        assert np.all(np.abs(got - ref) <= tol * scale + 1e-300)
+        r1 = cm.dot(xa, xb).cpu().numpy()
+        assert np.array_equal(r1, cm.dot(xa, xb).cpu().numpy())   # deterministic
+
+
+def test_kat_outer_product_on_pattern(cuda):
+    cm = _cm()
+    k = KAT["outer_product_on_pattern"]
+    p = cm.SparsityPattern.csr(k["rows"], k["cols"], k["JA"], k["IA"])
+    A = cm.SparseMatrix(p, dtype=torch.float64)
+    u = torch.tensor(k["u"], dtype=torch.float64, device=cuda)
+    v = torch.tensor(k["v"], dtype=torch.float64, device=cuda)
+    vals = cm.sddmm(A, u, v)[0].cpu().numpy()
+    dense = np.zeros((5, 5))
+    for r in range(5):
+        for j in range(k["JA"][r], k["JA"][r + 1]):
+            dense[r, k["IA"][j]] = vals[j]
+    assert np.array_equal(dense, np.array(k["dense"]))
+
+
+def test_sddmm_random_vs_oracle(cuda):
+    cm = _cm()
+    rng = np.random.default_rng(5)
+    rp, ci = _random_csr(rng, 500, 600, 20)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(500, 600, rp, ci), dtype=torch.float64)
+    u = rng.standard_normal(500)
+    v = rng.standard_normal(600)
+    got = cm.sddmm(A, torch.from_numpy(u).to(cuda), torch.from_numpy(v).to(cuda), alpha=-1.0)[0].cpu().numpy()
+    assert np.array_equal(got, O.sddmm_csr(500, rp, ci, u, v, alpha=-1.0))
+
+
+def test_invalid_patterns_raise(cuda):
+    cm = _cm()
+    with pytest.raises(cm.CuMatError):
+        cm.SparsityPattern.csr(2, 2, [0, 2, 1], [0, 1])        # decreasing row_ptr
+    with pytest.raises(cm.CuMatError):
+        cm.SparsityPattern.csr(2, 2, [0, 1, 2], [0, 2])        # column out of range
+    with pytest.raises(cm.CuMatError):
+        cm.SparsityPattern.ell(2, 2, [[0, -2], [1, 0]])        # bad padding index
+    p = cm.SparsityPattern.csr(4, 4, [0, 1, 2, 3, 4], [0, 2, 1, 3])
+    with pytest.raises(cm.CuMatError):
+        p.set_systems([0, 2, 4])                                # (1, 2) couples two systems
