@@ -18,6 +18,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -566,6 +568,89 @@ cmcg_status cmcg_dot(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int3
 
 cmcg_status cmcg_squared_norm(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t batches, void* out) {
     return cmcg_dot(ctx, dtype, n, x, batches, x, batches, out);
+}
+
+}  // extern "C"
+
+// ---- batched dot product without any allocation ----------------------------------
+//
+// cmcg_dot keeps its per-CTA partial sums and per-batch tickets in a context
+// buffer that it allocates with cudaMalloc the first time (and grows). Some
+// callers cannot let a library allocate: a host that has handed all device
+// memory to its own pool or framework allocator (a cudaMalloc from the library
+// would fail or fragment that memory), or a loop with a latency budget in which
+// cudaMalloc / cudaFree and the synchronisation they can imply are not allowed.
+// For them cmcg_dot_noalloc runs the same kernel with its scratch in the
+// fixed-size device array below, which exists once per GPU that loads this
+// library and stays allocated until the process exits.
+
+namespace {
+
+constexpr int kNoAllocMaxBatches = 1024;     // largest batch count accepted
+constexpr int kNoAllocMaxPartials = 4096;    // partial sums (all batches together)
+
+// [partials: kNoAllocMaxPartials doubles (room for floats too)][tickets: one
+// unsigned per batch]. In host code this name is only a stand-in: its device
+// address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_dot_scratch[kNoAllocMaxPartials * sizeof(double) +
+                                                             kNoAllocMaxBatches * sizeof(unsigned)];
+
+std::mutex g_dot_scratch_mu;
+void* g_dot_scratch_addr[1024] = {};   // device address per device ordinal
+
+// Address of the scratch array on `device`, looked up once per device with that
+// device current (the caller has made it current).
+cmcg_status dot_scratch_address(int device, void** out) {
+    CMCG_REQUIRE(device >= 0 && device < 1024, "cmcg_dot_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_dot_scratch_mu);
+    if (!g_dot_scratch_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_dot_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_dot_scratch)", __FILE__, __LINE__);
+        g_dot_scratch_addr[device] = p;
+    }
+    *out = g_dot_scratch_addr[device];
+    return CMCG_OK;
+}
+
+template <typename VT>
+cmcg_status launch_dot_noalloc(cmcg_ctx ctx, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb,
+                               void* out, int32_t ob) {
+    void* base = nullptr;
+    CMCG_TRY(dot_scratch_address(ctx->device, &base));
+    VT* partial = static_cast<VT*>(base);
+    unsigned* ticket = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(base) + kNoAllocMaxPartials * sizeof(double));
+    const int64_t want = std::max<int64_t>(1, (n + kRedThreads * 4 - 1) / (kRedThreads * 4));
+    const int cap = std::max(1, std::min(kNoAllocMaxPartials / ob, (ctx->sm_count * 4) / std::max(1, ob) + 1));
+    const int gx = static_cast<int>(std::min<int64_t>(want, cap));
+    // the tickets must start at zero; every call clears them (no allocation)
+    CMCG_CUDA(cudaMemsetAsync(ticket, 0, ob * sizeof(unsigned), ctx->stream));
+    dim3 grid(gx, ob);
+    k_dot<VT><<<grid, kRedThreads, 0, ctx->stream>>>(n, static_cast<const VT*>(x), xb, static_cast<const VT*>(y), yb,
+                                                     static_cast<VT*>(out), partial, ticket);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cmcg_status cmcg_dot_noalloc(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t xb, const void* y,
+                             int32_t yb, void* out) {
+    CMCG_REQUIRE(ctx && x && y && out, "cmcg_dot_noalloc: NULL argument");
+    CMCG_REQUIRE(n >= 0 && xb >= 1 && yb >= 1, "cmcg_dot_noalloc: bad size");
+    CMCG_REQUIRE(xb == 1 || yb == 1 || xb == yb, "cmcg_dot_noalloc: batch counts must match or be 1");
+    const int32_t ob = std::max(xb, yb);
+    if (ob > kNoAllocMaxBatches)
+        return fail(CMCG_ERR_INVALID_ARGUMENT, "cmcg_dot_noalloc: " + std::to_string(ob) +
+                                                   " batches requested, the fixed scratch holds at most " +
+                                                   std::to_string(kNoAllocMaxBatches) + " (use cmcg_dot)");
+    CMCG_CUDA(cudaSetDevice(ctx->device));
+    if (dtype == CMCG_F32) return launch_dot_noalloc<float>(ctx, n, x, xb, y, yb, out, ob);
+    if (dtype == CMCG_F64) return launch_dot_noalloc<double>(ctx, n, x, xb, y, yb, out, ob);
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "cmcg_dot_noalloc: dtype must be F32 or F64");
 }
 
 cmcg_status cmcg_sddmm(cmcg_matrix M, int32_t vec_dtype, double alpha, const void* u, int32_t ub, const void* v,

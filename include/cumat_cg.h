@@ -167,6 +167,20 @@ cmcg_status cmcg_dot(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int3
                      int32_t y_batches, void* out);
 /* out[b] = sum_i x[b][i]^2 (reference squaredNorm, ReductionOpsPlugin.inl:300-315). */
 cmcg_status cmcg_squared_norm(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t batches, void* out);
+/* Same result as cmcg_dot, but this entry point allocates nothing: no cudaMalloc,
+ * cudaFree or allocating library call. It has no counterpart in the reference.
+ * It is for callers that may not let a library allocate device memory, for
+ * instance because their own pool or framework allocator owns the device
+ * memory, or because allocation and the synchronisation it can bring are not
+ * allowed inside their loop. Its scratch is a fixed device array of about
+ * 36 KB that every GPU loading this library holds until the process exits;
+ * at most 1024 batches per call (more is rejected with CMCG_ERR_INVALID_ARGUMENT).
+ * The first call on a device looks up the array's address with that device
+ * current, so make that first call before any stream capture. All calls on a
+ * device share the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller. */
+cmcg_status cmcg_dot_noalloc(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t x_batches, const void* y,
+                             int32_t y_batches, void* out);
 
 /* out[k] = alpha * u[row(k)] * v[col(k)] for every stored entry k of batch b
  * (u: [u_batches][rows], v: [v_batches][cols], out: [out_batches][nnz] in the
