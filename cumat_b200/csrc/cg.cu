@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -688,6 +689,457 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_reliable_smem(RefineArgs<MI
 }
 
 // ---------------------------------------------------------------------------
+// Fast shared-memory kernels over the compact sliced layout (CSR patterns whose
+// systems have at most 65536 rows): 16-bit system-local column indices, the
+// slice offsets / widths a warp visits cached in shared memory once per system
+// (no dependent global loads per row), 32-bit offsets.
+// ---------------------------------------------------------------------------
+
+struct SliceEnt {
+    int32_t off;
+    int32_t w;
+};
+
+// tab[w][k]: slice w + 32 k of the system (local rows 32 (w + 32 k) ...), the
+// slice holding the rows tid + k * 1024 of warp w.
+__device__ __forceinline__ void load_slice_table(SliceEnt (*tab)[kSmemNK], const int32_t* __restrict__ off32,
+                                                 const int32_t* __restrict__ sw, int sl0, int nsl) {
+    for (int t = threadIdx.x; t < 32 * kSmemNK; t += blockDim.x) {
+        const int w = t / kSmemNK, k = t - (t / kSmemNK) * kSmemNK, sl = w + 32 * k;
+        tab[w][k] = sl < nsl ? SliceEnt{__ldg(off32 + sl0 + sl), __ldg(sw + sl0 + sl)} : SliceEnt{0, 0};
+    }
+}
+
+template <typename T>
+struct LocalX {
+    const T* p;
+    __device__ __forceinline__ T operator()(int c) const { return p[c]; }
+};
+
+// Entries of the lane's row in one compact slice, summed in entry order.
+template <typename VT, typename MT, typename XF>
+__device__ __forceinline__ VT fast_row(const uint16_t* __restrict__ col, const MT* __restrict__ val, SliceEnt e, int lane,
+                                       const XF& xf) {
+    const uint16_t* c = col + e.off + lane;
+    const MT* v = val + e.off + lane;
+    VT acc = VT(0);
+    int j = 0;
+    for (; j + 4 <= e.w; j += 4) {
+        const int c0 = __ldg(c + 32 * j), c1 = __ldg(c + 32 * (j + 1)), c2 = __ldg(c + 32 * (j + 2)),
+                  c3 = __ldg(c + 32 * (j + 3));
+        const MT v0 = v[32 * j], v1 = v[32 * (j + 1)], v2 = v[32 * (j + 2)], v3 = v[32 * (j + 3)];
+        acc += mval<VT>(v0) * xf(c0);
+        acc += mval<VT>(v1) * xf(c1);
+        acc += mval<VT>(v2) * xf(c2);
+        acc += mval<VT>(v3) * xf(c3);
+    }
+    for (; j < e.w; ++j) acc += mval<VT>(v[32 * j]) * xf(__ldg(c + 32 * j));
+    return acc;
+}
+
+struct CompactArgs {
+    const uint16_t* col16;
+    const int32_t* off32;
+    const int32_t* sw;
+    const int32_t* sys_slice0;
+};
+
+// Plain PCG (the reference's algorithm and stopping rule) on the compact layout.
+// p always lives in shared memory (it is gathered); r and x live there too when
+// RX_SMEM, else in global memory (coalesced, one access per row and pass).
+template <typename VT, typename MT, bool RX_SMEM>
+__global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a, CompactArgs c, int nmax) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ SliceEnt tab[32][kSmemNK];
+    __shared__ VT red[2 * (kSmemThreads / 32)];
+    __shared__ int slot;
+    VT* P = reinterpret_cast<VT*>(smraw);
+    VT* Rs = P + nmax;
+    VT* Xs = P + 2 * nmax;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n_inst = a.n_sys * a.ob;
+    const VT tol = static_cast<VT>(a.tol);
+    for (;;) {
+        const int item = fetch_item(a.next, &slot);
+        if (item >= n_inst) return;
+        const int s = a.order[item / a.ob], b = item % a.ob, inst = b * a.n_sys + s;
+        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
+        const int sl0 = __ldg(c.sys_slice0 + s), nsl = __ldg(c.sys_slice0 + s + 1) - sl0;
+        load_slice_table(tab, c.off32, c.sw, sl0, nsl);
+        const int64_t vo = static_cast<int64_t>(b) * a.rows;
+        const MT* vals = a.m.sell_vals + (a.m.mb == 1 ? 0 : static_cast<int64_t>(b) * a.m.sell_vstride);
+        const VT* bv = a.b + (a.b_b == 1 ? 0 : vo) + r0;
+        VT* xg = a.x + vo + r0;
+        VT* R = RX_SMEM ? Rs : a.r + vo + r0;
+        VT* X = RX_SMEM ? Xs : xg;
+        const VT* dg = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) + r0 : nullptr;
+        auto dv = [&](int i) { return dg ? __ldg(dg + i) : VT(1); };
+        __syncthreads();   // slice table ready
+        // q = A p: registers for FP32; for FP64 (twice the registers) a global
+        // buffer written and read back by the same thread (L1 / L2 resident)
+        constexpr bool kQReg = sizeof(VT) == 4;
+        VT* Qg = a.q + vo + r0;
+        VT q[kQReg ? kSmemNK : 1];
+        VT acc[2] = {VT(0), VT(0)};
+        if (a.guess) {
+            const VT* g = a.guess + (a.g_b == 1 ? 0 : vo) + r0;
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const VT ag = fast_row<VT>(c.col16, vals, tab[warp][k], lane, LocalX<VT>{g});
+                    const VT bi = bv[i], ri = bi - ag;
+                    X[i] = g[i];
+                    R[i] = ri;
+                    acc[0] += bi * bi;
+                    acc[1] += ri * ri;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const VT bi = bv[i];
+                    R[i] = bi;
+                    X[i] = VT(0);
+                    acc[0] += bi * bi;
+                }
+            }
+            acc[1] = acc[0];
+        }
+        block_sum<VT, 2>(acc, red);
+        const VT bb = acc[0];
+        VT rr = acc[1];
+        const VT thr = tol * tol * bb;
+        int32_t status = ST_RUNNING, it = 0;
+        if ((a.abs_zero_test && bb < tol * tol) || bb == VT(0)) {
+            status = CMCG_SOLVE_ZERO_RHS;
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) X[i] = VT(0);
+            }
+        } else if (!finite_(rr) || !finite_(bb)) {
+            status = CMCG_SOLVE_NON_FINITE;
+        } else if (rr < thr) {
+            status = CMCG_SOLVE_CONVERGED;
+        } else {
+            VT rz1[1] = {VT(0)};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const VT ri = R[i], zi = dv(i) * ri;
+                    P[i] = zi;
+                    rz1[0] += ri * zi;
+                }
+            }
+            block_sum<VT, 1>(rz1, red);
+            VT rz = rz1[0];
+            if (!finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
+            else if (!(rz > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
+            const int64_t maxit = sys_max_iter(a.max_iter, n);
+            while (status == ST_RUNNING) {
+                if (it >= maxit) { status = CMCG_SOLVE_MAX_ITER; break; }
+                VT pq[1] = {VT(0)};
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        const VT qi = fast_row<VT>(c.col16, vals, tab[warp][k], lane, LocalX<VT>{P});
+                        if constexpr (kQReg) q[k] = qi; else Qg[i] = qi;
+                        pq[0] += P[i] * qi;
+                    }
+                }
+                block_sum<VT, 1>(pq, red);
+                const VT alpha = rz / pq[0];
+                if (!finite_(pq[0]) || !finite_(alpha)) { status = CMCG_SOLVE_NON_FINITE; break; }
+                if (!(pq[0] > VT(0))) { status = CMCG_SOLVE_BREAKDOWN; break; }
+                VT s2[2] = {VT(0), VT(0)};
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        X[i] += alpha * P[i];
+                        VT qi;
+                        if constexpr (kQReg) qi = q[kQReg ? k : 0]; else qi = Qg[i];
+                        const VT ri = R[i] - alpha * qi;
+                        R[i] = ri;
+                        s2[0] += ri * ri;
+                        s2[1] += ri * (dv(i) * ri);
+                    }
+                }
+                block_sum<VT, 2>(s2, red);
+                rr = s2[0];
+                if (!finite_(rr) || !finite_(s2[1])) { status = CMCG_SOLVE_NON_FINITE; break; }
+                if (rr < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+                if (!(s2[1] > VT(0))) { status = CMCG_SOLVE_BREAKDOWN; break; }
+                const VT beta = s2[1] / rz;
+                rz = s2[1];
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) P[i] = dv(i) * R[i] + beta * P[i];
+                }
+                __syncthreads();
+                ++it;
+            }
+        }
+        if (RX_SMEM) {
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) xg[i] = X[i];
+            }
+        }
+        if (tid == 0) {
+            a.st.it[inst] = it;
+            a.st.status[inst] = status;
+            a.st.rr[inst] = static_cast<double>(rr);
+            a.st.bb[inst] = static_cast<double>(bb);
+            a.st.outer[inst] = 0;
+            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(static_cast<double>(rr) / static_cast<double>(bb));
+        }
+        __syncthreads();
+    }
+}
+
+template <typename MI, typename MO>
+struct MixArgs {
+    int32_t rows, n_sys, ob, mb;
+    const int32_t* row_off;
+    const int32_t* order;
+    int32_t* next;
+    CompactArgs c;
+    const MI* vin;          // Jacobi-scaled inner values, sliced layout
+    int64_t vin_stride;
+    const MO* vout;         // unscaled outer values, sliced layout
+    int64_t vout_stride;
+    const double* s;        // scale 1/sqrt(a_ii) (or 1), [mb][rows]
+    const double* b;
+    int32_t b_b;
+    double* x;
+    double outer_tol;
+    int64_t max_inner;
+    int32_t max_updates;
+    float delta;
+    InstState st;
+};
+
+// Mixed precision with reliable updates on the compact layout. The inner FP32
+// CG runs on the symmetrically Jacobi-scaled system S A S (S = diag(s)), which
+// is Jacobi PCG in exact arithmetic but needs no diagonal inside the loop; the
+// FP64 parts use the unscaled values: x += S xh at every fold and the inner
+// residual is S (b - A x). Residual replacement as in k_reliable_smem, the
+// trigger compared in the scaled norm.
+template <typename MI, typename MO>
+__global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
+    extern __shared__ __align__(16) float smf[];
+    __shared__ SliceEnt tab[32][kSmemNK];
+    __shared__ float red[2 * (kSmemThreads / 32)];
+    __shared__ double red64[2 * (kSmemThreads / 32)];
+    __shared__ int slot;
+    float* P = smf;
+    float* R = smf + nmax;
+    float* XH = smf + 2 * nmax;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n_inst = a.n_sys * a.ob;
+    const float d2 = a.delta * a.delta;
+    for (;;) {
+        const int item = fetch_item(a.next, &slot);
+        if (item >= n_inst) return;
+        const int s = a.order[item / a.ob], bi = item % a.ob, inst = bi * a.n_sys + s;
+        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
+        const int sl0 = __ldg(a.c.sys_slice0 + s), nsl = __ldg(a.c.sys_slice0 + s + 1) - sl0;
+        load_slice_table(tab, a.c.off32, a.c.sw, sl0, nsl);
+        const int64_t vo = static_cast<int64_t>(bi) * a.rows;
+        const MI* vin = a.vin + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vin_stride);
+        const MO* vout = a.vout + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vout_stride);
+        const double* sv = a.s + (a.mb == 1 ? 0 : vo) + r0;
+        const double* bv = a.b + (a.b_b == 1 ? 0 : vo) + r0;
+        double* x = a.x + vo + r0;
+        __syncthreads();   // slice table ready
+        float q[kSmemNK];
+        double acc[1] = {0.0};
+        float rz1[1] = {0.0f};
+#pragma unroll
+        for (int k = 0; k < kSmemNK; ++k) {
+            const int i = tid + k * kSmemThreads;
+            if (i < n) {
+                const double b_i = bv[i];
+                x[i] = 0.0;
+                const float rh = static_cast<float>(__ldg(sv + i) * b_i);
+                R[i] = rh;
+                P[i] = rh;
+                XH[i] = 0.0f;
+                acc[0] += b_i * b_i;
+                rz1[0] += rh * rh;
+            }
+        }
+        block_sum<double, 1>(acc, red64);
+        block_sum<float, 1>(rz1, red);
+        const double bb = acc[0];
+        const double thr = a.outer_tol * a.outer_tol * bb;
+        double rr64 = bb;
+        float rz = rz1[0];
+        float rmax = rz;            // scaled |r|^2 at the last replacement
+        int32_t status = ST_RUNNING, it = 0, updates = 0;
+        if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
+        else if (!finite_(bb)) status = CMCG_SOLVE_NON_FINITE;
+        else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
+        else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+        const int64_t maxit = sys_max_iter(a.max_inner, n);
+        bool folded = true;
+        while (status == ST_RUNNING) {
+            if (it >= maxit || updates >= a.max_updates) { status = CMCG_SOLVE_MAX_ITER; break; }
+            float pq[1] = {0.0f};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                q[k] = 0.0f;
+                if (i < n) {
+                    q[k] = fast_row<float>(a.c.col16, vin, tab[warp][k], lane, LocalX<float>{P});
+                    pq[0] += P[i] * q[k];
+                }
+            }
+            block_sum<float, 1>(pq, red);
+            const float alpha = rz / pq[0];
+            if (!finite_(pq[0]) || !finite_(alpha)) { status = CMCG_SOLVE_NON_FINITE; break; }
+            if (!(pq[0] > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
+            float s1[1] = {0.0f};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    XH[i] += alpha * P[i];
+                    const float ri = R[i] - alpha * q[k];
+                    R[i] = ri;
+                    s1[0] += ri * ri;
+                }
+            }
+            block_sum<float, 1>(s1, red);
+            ++it;
+            folded = false;
+            float rzn = s1[0];
+            if (!finite_(rzn)) { status = CMCG_SOLVE_NON_FINITE; break; }
+            // replace the residual when it dropped by delta, or when it suggests
+            // that the FP64 residual may have reached the target
+            if (rzn < d2 * rmax || static_cast<double>(rzn) < thr / rr64 * static_cast<double>(rmax)) {
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
+                        XH[i] = 0.0f;
+                    }
+                }
+                __syncthreads();
+                double t2[2] = {0.0, 0.0};
+#pragma unroll
+                for (int k = 0; k < kSmemNK; ++k) {
+                    const int i = tid + k * kSmemThreads;
+                    if (i < n) {
+                        const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
+                        const float rh = static_cast<float>(__ldg(sv + i) * r64);
+                        R[i] = rh;
+                        t2[0] += r64 * r64;
+                        t2[1] += static_cast<double>(rh) * static_cast<double>(rh);
+                    }
+                }
+                block_sum<double, 2>(t2, red64);
+                ++updates;
+                folded = true;
+                rr64 = t2[0];
+                rzn = static_cast<float>(t2[1]);
+                rmax = rzn;
+                if (!finite_(rr64)) { status = CMCG_SOLVE_NON_FINITE; break; }
+                if (rr64 < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+            }
+            if (!(rzn > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
+            const float beta = rzn / rz;
+            rz = rzn;
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) P[i] = R[i] + beta * P[i];
+            }
+            __syncthreads();
+        }
+        if (!folded) {
+            // fold the pending increments and report the true residual
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
+            }
+            __syncthreads();
+            double t1[1] = {0.0};
+#pragma unroll
+            for (int k = 0; k < kSmemNK; ++k) {
+                const int i = tid + k * kSmemThreads;
+                if (i < n) {
+                    const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
+                    t1[0] += r64 * r64;
+                }
+            }
+            block_sum<double, 1>(t1, red64);
+            rr64 = t1[0];
+        }
+        if (tid == 0) {
+            a.st.it[inst] = it;
+            a.st.status[inst] = status;
+            a.st.rr[inst] = rr64;
+            a.st.bb[inst] = bb;
+            a.st.outer[inst] = updates;
+            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(rr64 / bb);
+        }
+        __syncthreads();
+    }
+}
+
+// s = 1/sqrt(a_ii) where a_ii > 0 (Jacobi), else 1; [mb][rows]
+template <typename MT>
+__global__ void k_jacobi_scale(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const MT* __restrict__ vals,
+                               int64_t vstride, int32_t rows, int32_t mb, int32_t jacobi, double* __restrict__ out) {
+    const int64_t items = static_cast<int64_t>(rows) * mb;
+    for (int64_t it = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(it / rows);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * rows);
+        double d = 0.0;
+        if (jacobi)
+            for (int k = rp[r]; k < rp[r + 1]; ++k)
+                if (ci[k] == r) { d = mval<double>(vals[b * vstride + k]); break; }
+        out[it] = d > 0.0 ? 1.0 / sqrt(d) : 1.0;
+    }
+}
+
+// out[b][slot] = a * s_row * s_col for every slot of the sliced layout (warp per slice)
+template <typename MS, typename MD>
+__global__ void k_scale_sell(const int32_t* __restrict__ col, const int32_t* __restrict__ off32,
+                             const int32_t* __restrict__ sw, const int32_t* __restrict__ row0, int32_t n_slices,
+                             const MS* __restrict__ src, int64_t sstride, const double* __restrict__ sc, int32_t rows,
+                             int32_t mb, MD* __restrict__ dst, int64_t dstride) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t item = wid; item < static_cast<int64_t>(n_slices) * mb; item += nw) {
+        const int b = static_cast<int>(item / n_slices);
+        const int sl = static_cast<int>(item - static_cast<int64_t>(b) * n_slices);
+        const int row = row0[sl] + lane, w = sw[sl], off = off32[sl];
+        const double* sb = sc + static_cast<int64_t>(b) * rows;
+        for (int j = 0; j < w; ++j) {
+            const int64_t o = off + 32 * j + lane;
+            const double v = mval<double>(src[b * sstride + o]);
+            double out = 0.0;
+            if (v != 0.0 && row < rows) out = v * sb[row] * sb[col[o]];
+            dst[b * dstride + o] = from_f64<MD>(out);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Grid path kernels
 // ---------------------------------------------------------------------------
 
@@ -1017,6 +1469,7 @@ struct cmcg_solver_s {
     double refine_delta = 0.1;
     bool use_smem = true;     // shared-memory-resident kernels where the systems fit
     bool inner_solve = false; // set while the solver runs the inner solves of a refinement
+    bool fast_kernels = true; // compact-layout kernels where available (CUMAT_CG_FAST=0 disables)
     int64_t systems_version = -1;  // pattern systems the plan was built for
     // plan
     int32_t n_sys = 0, max_sys_rows = 0, n_tiles = 0;
@@ -1033,6 +1486,14 @@ struct cmcg_solver_s {
     void* st_ws = nullptr;    size_t st_ws_bytes = 0;
     int32_t* counters = nullptr;  // next, active, loops
     void* host_io = nullptr;  size_t host_io_bytes = 0;
+    // mixed solver, fast path: Jacobi-scaled copy of the inner values in the
+    // sliced layout ([batch][mix_stride]) and the scale s = 1/sqrt(a_ii)
+    // ([batch][rows], FP64); rebuilt when the values or the systems change
+    void* mix_vals = nullptr;
+    int64_t mix_stride = 0;
+    double* mix_s = nullptr;
+    int64_t mix_version = -1, mix_plan_id = -1;
+    int32_t mix_dtype = -1;
     InstState st{};
     int32_t st_inst = 0;
     // graph cache of the grid path
@@ -1211,9 +1672,83 @@ cmcg_status allow_smem(K kern, size_t bytes) {
 
 inline int smem_rows(int32_t max_rows) { return (max_rows + 3) / 4 * 4; }
 
+// Compact sliced layout available for the fast shared-memory kernels?
+inline bool compact_ok(cmcg_solver s) {
+    const cmcg_pattern p = s->A->pat;
+    return p->format == CMCG_CSR && p->sell.d_col16 != nullptr && s->max_sys_rows <= kSmemMaxRows && s->use_smem &&
+           s->fast_kernels;
+}
+
+inline CompactArgs compact_args(cmcg_pattern p) {
+    return CompactArgs{p->sell.d_col16, p->sell.d_slice_off32, p->sell.d_slice_w, p->sell.d_sys_slice0};
+}
+
+template <typename MT>
+cmcg_status build_mix(cmcg_solver s) {
+    cmcg_matrix A = s->A;
+    cmcg_pattern p = A->pat;
+    cmcg_ctx ctx = p->ctx;
+    const SellPlan& S = p->sell;
+    const int blocks = ctx->sm_count * 8;
+    k_jacobi_scale<MT><<<blocks, 256, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, static_cast<const MT*>(A->d_vals), A->stride,
+                                                      p->rows, A->batches, s->precond == CMCG_PRECOND_JACOBI ? 1 : 0, s->mix_s);
+    k_scale_sell<MT, MT><<<blocks, 256, 0, ctx->stream>>>(S.d_col, S.d_slice_off32, S.d_slice_w, S.d_slice_row0, S.n_slices,
+                                                         static_cast<const MT*>(A->d_sell_vals), A->sell_stride, s->mix_s,
+                                                         p->rows, A->batches, static_cast<MT*>(s->mix_vals), s->mix_stride);
+    count_launch(2);
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
+// Jacobi-scaled inner values and the scale vector of the mixed solver's fast
+// path, rebuilt when the matrix values or the systems changed.
+cmcg_status ensure_mix(cmcg_solver s) {
+    cmcg_matrix A = s->A;
+    cmcg_pattern p = A->pat;
+    CMCG_TRY(ensure_sell_values(A));
+    const SellPlan& S = p->sell;
+    if (s->mix_vals && s->mix_version == A->version && s->mix_plan_id == S.plan_id && s->mix_dtype == A->dtype)
+        return CMCG_OK;
+    dev_free(s->mix_vals);
+    dev_free(s->mix_s);
+    s->mix_vals = nullptr;
+    s->mix_s = nullptr;
+    s->mix_stride = A->sell_stride;
+    CMCG_TRY(dev_alloc(&s->mix_vals, static_cast<size_t>(s->mix_stride) * A->batches * dtype_size(A->dtype)));
+    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->mix_s), static_cast<size_t>(p->rows) * A->batches * sizeof(double)));
+    cmcg_status st = A->dtype == CMCG_F32 ? build_mix<float>(s) : A->dtype == CMCG_BF16 ? build_mix<__nv_bfloat16>(s)
+                                                                                        : build_mix<double>(s);
+    if (st != CMCG_OK) return st;
+    s->mix_version = A->version;
+    s->mix_plan_id = S.plan_id;
+    s->mix_dtype = A->dtype;
+    return CMCG_OK;
+}
+
+template <typename VT, typename MT, bool RX>
+cmcg_status launch_cg_fast(cmcg_solver s, SolveArgs<VT, MT>& a, int nmax) {
+    cmcg_ctx ctx = s->A->pat->ctx;
+    const size_t sm = static_cast<size_t>(nmax) * sizeof(VT) * (RX ? 3 : 1);
+    CMCG_TRY(allow_smem(k_cg_fast<VT, MT, RX>, sm));
+    const int n_inst = a.n_sys * a.ob;
+    const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+    k_cg_fast<VT, MT, RX><<<grid, kSmemThreads, sm, ctx->stream>>>(a, compact_args(s->A->pat), nmax);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    return CMCG_OK;
+}
+
 template <typename VT, typename MT, int FMT>
 cmcg_status run_persistent(cmcg_solver s, SolveArgs<VT, MT>& a) {
     cmcg_ctx ctx = s->A->pat->ctx;
+    if (FMT == CMCG_CSR && compact_ok(s)) {
+        const int nmax = smem_rows(s->max_sys_rows);
+        // FP32: p, r, x in shared memory (12 B/row); FP64: all three when they
+        // fit (24 B/row, up to 8192 rows), else p only and r, x in global memory
+        if (sizeof(VT) == 4 || nmax <= kSmemMaxRows / 2) return launch_cg_fast<VT, MT, true>(s, a, nmax);
+        return launch_cg_fast<VT, MT, false>(s, a, nmax);
+    }
     if constexpr (std::is_same<VT, float>::value) {
         if (s->max_sys_rows <= kSmemMaxRows && s->use_smem) {
             const int nmax = smem_rows(s->max_sys_rows);
@@ -1415,6 +1950,41 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     a.max_outer = max_outer;
     a.st = s->st;
     CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+    if (s->refine_method == CMCG_REFINE_RELIABLE && FMT == CMCG_CSR && compact_ok(s)) {
+        CMCG_TRY(ensure_mix(s));
+        MixArgs<MI, MO> m{};
+        m.rows = p->rows;
+        m.n_sys = s->n_sys;
+        m.ob = ob;
+        m.mb = s->A->batches;
+        m.row_off = p->d_row_off;
+        m.order = s->d_order;
+        m.next = s->counters;
+        m.c = compact_args(p);
+        m.vin = static_cast<const MI*>(s->mix_vals);
+        m.vin_stride = s->mix_stride;
+        m.vout = static_cast<const MO*>(Ao->d_sell_vals);
+        m.vout_stride = Ao->sell_stride;
+        m.s = s->mix_s;
+        m.b = b;
+        m.b_b = b_b;
+        m.x = x;
+        m.outer_tol = outer_tol;
+        m.max_inner = s->max_iter;
+        m.max_updates = max_outer;
+        m.delta = static_cast<float>(s->refine_delta);
+        m.st = s->st;
+        const int nmax = smem_rows(s->max_sys_rows);
+        const size_t sm = smem_bytes(nmax);
+        CMCG_TRY(allow_smem(k_mixed_fast<MI, MO>, sm));
+        const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
+        k_mixed_fast<MI, MO><<<grid, kSmemThreads, sm, ctx->stream>>>(m, nmax);
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        s->last_inst = n_inst;
+        s->last_refined = true;
+        return CMCG_OK;
+    }
     if (s->refine_method == CMCG_REFINE_RELIABLE && s->max_sys_rows <= kSmemMaxRows && s->use_smem) {
         const int nmax = smem_rows(s->max_sys_rows);
         const size_t sm = smem_bytes(nmax);
@@ -1568,6 +2138,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     s->precond = precond;
     // default tolerance: epsilon of the scalar type (IterativeSolverBase.h:131)
     s->tol = (A->dtype == CMCG_F64) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+    if (const char* e = std::getenv("CUMAT_CG_FAST")) s->fast_kernels = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);
     if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);
     if (st == CMCG_OK && cudaMemsetAsync(s->counters, 0, 64, A->pat->ctx->stream) != cudaSuccess) st = fail(CMCG_ERR_CUDA, "memset");
@@ -1590,7 +2161,7 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
     if (s->graph) cudaGraphDestroy(s->graph);
     for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_tile_sys),
                     static_cast<void*>(s->d_sys_tile_begin), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
-                    s->st_ws, static_cast<void*>(s->counters)})
+                    s->st_ws, static_cast<void*>(s->counters), s->mix_vals, static_cast<void*>(s->mix_s)})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);
     cmcg_matrix A = s->A;

@@ -75,6 +75,12 @@ template <> __device__ __forceinline__ double mval<double, float>(float v) { ret
 template <> __device__ __forceinline__ double mval<double, double>(double v) { return v; }
 template <> __device__ __forceinline__ double mval<double, __nv_bfloat16>(__nv_bfloat16 v) { return static_cast<double>(__bfloat162float(v)); }
 
+// Rounds an FP64 value to the storage type T.
+template <typename T> __device__ __forceinline__ T from_f64(double v);
+template <> __device__ __forceinline__ float from_f64<float>(double v) { return static_cast<float>(v); }
+template <> __device__ __forceinline__ double from_f64<double>(double v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f64<__nv_bfloat16>(double v) { return __double2bfloat16(v); }
+
 // Four consecutive stored values starting at a 4-entry aligned index.
 template <typename MT> struct Vals4;
 template <> struct Vals4<float> {

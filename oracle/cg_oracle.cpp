@@ -533,6 +533,109 @@ int orc_reliable_packed(int64_t n_sys, const int64_t* row_off, const int32_t* rp
     return 0;
 }
 
+// The same reliable-update method in the Jacobi-scaled form used by the CUDA
+// fast path: the inner FP32 CG (no preconditioner) runs on S A S with
+// S = diag(1/sqrt(a_ii)) (1 where a_ii <= 0 or precond == 0), scaled values
+// rounded to FP32 (or BF16); x += S xh at every fold; the inner residual is
+// S (b - A x); replacement when |r^|^2 < delta^2 |r^_last|^2 or
+// |r^|^2 < (tol^2 |b|^2 / |r_last|^2) |r^_last|^2.
+int orc_reliable_scaled_packed(int64_t n_sys, const int64_t* row_off, const int32_t* rp, const int32_t* ci,
+                               const float* val, const double* rhs, double* x, double tol, double delta,
+                               int64_t max_iter, int32_t max_updates, int precond, int bf16_inner, int64_t* iters,
+                               int32_t* updates, double* err) {
+    std::vector<float> t32;
+    std::vector<double> t64;
+    for (int64_t s = 0; s < n_sys; ++s) {
+        const int64_t r0 = row_off[s], n = row_off[s + 1] - row_off[s];
+        const int32_t* srp = rp + r0;
+        const int32_t k0 = srp[0];
+        std::vector<double> sc(n, 1.0);
+        if (precond == 1)
+            for (int64_t i = 0; i < n; ++i)
+                for (int32_t k = srp[i]; k < srp[i + 1]; ++k)
+                    if (ci[k] == r0 + i) { if (val[k] > 0.0f) sc[i] = 1.0 / std::sqrt(static_cast<double>(val[k])); break; }
+        std::vector<float> vin(srp[n] - k0);
+        for (int64_t i = 0; i < n; ++i)
+            for (int32_t k = srp[i]; k < srp[i + 1]; ++k) {
+                const float v = static_cast<float>(static_cast<double>(bf16_inner ? bf16_round(val[k]) : val[k]) * sc[i] *
+                                                   sc[ci[k] - r0]);
+                vin[k - k0] = bf16_inner ? bf16_round(v) : v;
+            }
+        const double* b = rhs + r0;
+        double* xs = x + r0;
+        std::vector<float> r(n), p(n), q(n), xh(n, 0.0f), sq(n);
+        for (int64_t i = 0; i < n; ++i) {
+            xs[i] = 0.0;
+            r[i] = static_cast<float>(sc[i] * b[i]);
+            p[i] = r[i];
+        }
+        const double bb = dot(b, b, n, t64);
+        float rz = dot(r.data(), r.data(), n, t32);
+        const double thr = tol * tol * bb;
+        double rr64 = bb;
+        float rmax = rz;
+        int64_t it = 0;
+        int32_t up = 0;
+        const int64_t mi = max_iter < 0 ? 2 * n : max_iter;
+        bool folded = true;
+        auto residual = [&](std::vector<double>& r64) {
+            for (int64_t i = 0; i < n; ++i) {
+                double acc = 0.0;
+                for (int32_t k = srp[i]; k < srp[i + 1]; ++k) acc += static_cast<double>(val[k]) * xs[ci[k] - r0];
+                r64[i] = b[i] - acc;
+            }
+        };
+        bool done = (bb == 0.0) || (rr64 < thr);
+        while (!done && it < mi && up < max_updates) {
+            for (int64_t i = 0; i < n; ++i) {
+                float acc = 0.0f;
+                for (int32_t k = srp[i]; k < srp[i + 1]; ++k) acc += vin[k - k0] * p[ci[k] - r0];
+                q[i] = acc;
+            }
+            const float pq = dot(p.data(), q.data(), n, t32);
+            const float alpha = rz / pq;
+            if (!(pq > 0.0f) || !std::isfinite(alpha)) break;
+            for (int64_t i = 0; i < n; ++i) {
+                xh[i] += alpha * p[i];
+                r[i] -= alpha * q[i];
+            }
+            float rzn = dot(r.data(), r.data(), n, t32);
+            ++it;
+            folded = false;
+            if (rzn < static_cast<float>(delta * delta) * rmax ||
+                static_cast<double>(rzn) < thr / rr64 * static_cast<double>(rmax)) {
+                for (int64_t i = 0; i < n; ++i) { xs[i] += sc[i] * static_cast<double>(xh[i]); xh[i] = 0.0f; }
+                std::vector<double> r64(n), rh2(n);
+                residual(r64);
+                for (int64_t i = 0; i < n; ++i) {
+                    r[i] = static_cast<float>(sc[i] * r64[i]);
+                    rh2[i] = static_cast<double>(r[i]) * static_cast<double>(r[i]);
+                }
+                rr64 = dot(r64.data(), r64.data(), n, t64);
+                rzn = static_cast<float>(pairwise_sum(rh2.data(), n));
+                rmax = rzn;
+                ++up;
+                folded = true;
+                if (rr64 < thr) { done = true; break; }
+            }
+            if (!(rzn > 0.0f)) break;
+            const float beta = rzn / rz;
+            rz = rzn;
+            for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
+        }
+        if (!folded) {
+            for (int64_t i = 0; i < n; ++i) xs[i] += sc[i] * static_cast<double>(xh[i]);
+            std::vector<double> r64(n);
+            residual(r64);
+            rr64 = dot(r64.data(), r64.data(), n, t64);
+        }
+        iters[s] = it;
+        updates[s] = up;
+        err[s] = bb > 0 ? std::sqrt(rr64 / bb) : 0.0;
+    }
+    return 0;
+}
+
 // out[k] = alpha * u[row(k)] * v[col(k)] at the pattern's entries.
 int orc_sddmm_csr_f64(int32_t rows, const int32_t* rp, const int32_t* ci, double alpha, const double* u,
                       const double* v, double* out) {

@@ -46,6 +46,8 @@ def lib():
             "orc_cg_packed_f64": [i64, vp, vp, vp, vp, vp, vp, vp, f64, i64, C.c_int, vp, vp],
             "orc_refined_packed": [i64, vp, vp, vp, vp, vp, vp, f64, f64, i64, i32, C.c_int, C.c_int, vp, vp, vp],
             "orc_reliable_packed": [i64, vp, vp, vp, vp, vp, vp, f64, f64, i64, i32, C.c_int, C.c_int, vp, vp, vp],
+            "orc_reliable_scaled_packed": [i64, vp, vp, vp, vp, vp, vp, f64, f64, i64, i32, C.c_int, C.c_int, vp, vp,
+                                           vp],
             "orc_sddmm_csr_f64": [i32, vp, vp, f64, vp, vp, vp],
             "orc_sddmm_csr_f32": [i32, vp, vp, C.c_float, vp, vp, vp],
         }
@@ -212,8 +214,9 @@ def refined_packed(row_off, rp, ci, val32, rhs64, inner_tol, outer_tol, max_inne
 
 
 def reliable_packed(row_off, rp, ci, val32, rhs64, tol, delta=0.1, max_iter=-1, max_updates=1000, precond=1,
-                    bf16_inner=False):
-    """FP32 PCG with FP64 reliable updates, per system.
+                    bf16_inner=False, scaled=True):
+    """FP32 CG with FP64 reliable updates, per system; scaled=True is the
+    Jacobi-scaled form of the CUDA fast path, scaled=False explicit Jacobi PCG.
     Returns (x, FP32 iterations, replacements, final FP64 relative residual)."""
     ro = np.ascontiguousarray(row_off, np.int64)
     b = np.ascontiguousarray(rhs64, np.float64)
@@ -222,9 +225,9 @@ def reliable_packed(row_off, rp, ci, val32, rhs64, tol, delta=0.1, max_iter=-1, 
     it = np.empty(S, np.int64)
     up = np.empty(S, np.int32)
     err = np.empty(S, np.float64)
-    lib().orc_reliable_packed(S, _p(ro), _p(_i32(rp)), _p(_i32(ci)), _p(np.ascontiguousarray(val32, np.float32)), _p(b),
-                              _p(x), float(tol), float(delta), int(max_iter), int(max_updates), int(precond),
-                              1 if bf16_inner else 0, _p(it), _p(up), _p(err))
+    f = lib().orc_reliable_scaled_packed if scaled else lib().orc_reliable_packed
+    f(S, _p(ro), _p(_i32(rp)), _p(_i32(ci)), _p(np.ascontiguousarray(val32, np.float32)), _p(b), _p(x), float(tol),
+      float(delta), int(max_iter), int(max_updates), int(precond), 1 if bf16_inner else 0, _p(it), _p(up), _p(err))
     return x, it, up, err
 
 

@@ -309,6 +309,49 @@ def test_reliable_updates_vs_oracle_and_truth(cuda):
             assert np.linalg.norm(x[r0:r1] - xt) / np.linalg.norm(xt) < 1e-8
 
 
+def test_generic_kernels_match_oracle(cuda, monkeypatch):
+    # CUMAT_CG_FAST=0 (read when a solver is created) selects the generic
+    # shared-memory kernels: explicit Jacobi PCG inside the reliable updates
+    m = cm()
+    monkeypatch.setenv("CUMAT_CG_FAST", "0")
+    bt = P.fv2d_batch(12, 16, 128, 0.5, 9)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A = m.SparseMatrix(p, dtype=torch.float32).setData(bt.val)
+    cg = m.ConjugateGradient(A)
+    b64 = bt.b.astype(np.float64)
+    cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=A, outer_tol=1e-10, max_outer=200)
+    st = cg.system_stats()
+    assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-10)
+    _, it_o, up_o, _ = O.reliable_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, b64, 1e-10, scaled=False)
+    assert abs(int(st["iterations"].sum()) - int(it_o.sum())) <= 0.05 * it_o.sum()
+    cgp = m.ConjugateGradient(A).setTolerance(1e-6)
+    cgp.solve(torch.from_numpy(bt.b).to(cuda))
+    monkeypatch.setenv("CUMAT_CG_FAST", "1")
+    cgf = m.ConjugateGradient(A).setTolerance(1e-6)
+    cgf.solve(torch.from_numpy(bt.b).to(cuda))
+    assert np.all(np.abs(cgp.system_stats()["iterations"] - cgf.system_stats()["iterations"]) <= 2)
+
+
+@pytest.mark.parametrize("side_hi", [64, 128])   # FP64 vectors all in shared memory / p only
+def test_fp64_fast_kernel_vs_oracle(cuda, side_hi):
+    m = cm()
+    bt = P.fv2d_batch(20, 16, side_hi, 0.5, 13)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A = m.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
+    cg = m.ConjugateGradient(A).setTolerance(1e-10)
+    b64 = bt.b.astype(np.float64)
+    x = cg.solve(torch.from_numpy(b64).to(cuda)).cpu().numpy()
+    st = cg.system_stats()
+    _, it_o, _ = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val.astype(np.float64), b64, 1e-10)
+    assert np.all(st["status"] == 0) and np.all(np.abs(st["iterations"] - it_o) <= 2)
+    r = b64 - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x)[0]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b64[r0:r1]) < 2e-10
+
+
 def test_shared_memory_and_global_kernels_agree(cuda):
     m = cm()
     bt = P.fv2d_batch(40, 16, 128, 0.5, 5)
