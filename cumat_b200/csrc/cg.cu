@@ -716,12 +716,42 @@ struct LocalX {
     __device__ __forceinline__ T operator()(int c) const { return p[c]; }
 };
 
+// W entries of a row, fully unrolled: every load is the row's base pointer
+// plus an immediate offset; all loads issue before the first product; the
+// products are summed in entry order.
+template <int W, typename VT, typename MT, typename XF>
+__device__ __forceinline__ VT row_w(const uint16_t* __restrict__ c, const MT* __restrict__ v, const XF& xf) {
+    int ci[W];
+    MT vi[W];
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+        ci[j] = __ldg(c + 32 * j);
+        vi[j] = v[32 * j];
+    }
+    VT acc = VT(0);
+#pragma unroll
+    for (int j = 0; j < W; ++j) acc += mval<VT>(vi[j]) * xf(ci[j]);
+    return acc;
+}
+
 // Entries of the lane's row in one compact slice, summed in entry order.
 template <typename VT, typename MT, typename XF>
 __device__ __forceinline__ VT fast_row(const uint16_t* __restrict__ col, const MT* __restrict__ val, SliceEnt e, int lane,
                                        const XF& xf) {
     const uint16_t* c = col + e.off + lane;
     const MT* v = val + e.off + lane;
+    switch (e.w) {   // warp-uniform: one slice per warp
+        case 0: return VT(0);
+        case 1: return row_w<1, VT>(c, v, xf);
+        case 2: return row_w<2, VT>(c, v, xf);
+        case 3: return row_w<3, VT>(c, v, xf);
+        case 4: return row_w<4, VT>(c, v, xf);
+        case 5: return row_w<5, VT>(c, v, xf);
+        case 6: return row_w<6, VT>(c, v, xf);
+        case 7: return row_w<7, VT>(c, v, xf);
+        case 8: return row_w<8, VT>(c, v, xf);
+        default: break;
+    }
     VT acc = VT(0);
     int j = 0;
     for (; j + 4 <= e.w; j += 4) {
@@ -785,6 +815,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
             const VT* g = a.guess + (a.g_b == 1 ? 0 : vo) + r0;
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) {
                     const VT ag = fast_row<VT>(c.col16, vals, tab[warp][k], lane, LocalX<VT>{g});
@@ -798,6 +829,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
         } else {
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) {
                     const VT bi = bv[i];
@@ -817,6 +849,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
             status = CMCG_SOLVE_ZERO_RHS;
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) X[i] = VT(0);
             }
@@ -828,6 +861,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
             VT rz1[1] = {VT(0)};
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) {
                     const VT ri = R[i], zi = dv(i) * ri;
@@ -845,6 +879,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
                 VT pq[1] = {VT(0)};
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
+                    if (k * kSmemThreads >= n) break;
                     const int i = tid + k * kSmemThreads;
                     if (i < n) {
                         const VT qi = fast_row<VT>(c.col16, vals, tab[warp][k], lane, LocalX<VT>{P});
@@ -859,6 +894,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
                 VT s2[2] = {VT(0), VT(0)};
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
+                    if (k * kSmemThreads >= n) break;
                     const int i = tid + k * kSmemThreads;
                     if (i < n) {
                         X[i] += alpha * P[i];
@@ -879,6 +915,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
                 rz = s2[1];
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
+                    if (k * kSmemThreads >= n) break;
                     const int i = tid + k * kSmemThreads;
                     if (i < n) P[i] = dv(i) * R[i] + beta * P[i];
                 }
@@ -889,6 +926,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
         if (RX_SMEM) {
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) xg[i] = X[i];
             }
@@ -965,6 +1003,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         float rz1[1] = {0.0f};
 #pragma unroll
         for (int k = 0; k < kSmemNK; ++k) {
+            if (k * kSmemThreads >= n) break;
             const int i = tid + k * kSmemThreads;
             if (i < n) {
                 const double b_i = bv[i];
@@ -984,6 +1023,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         double rr64 = bb;
         float rz = rz1[0];
         float rmax = rz;            // scaled |r|^2 at the last replacement
+        float goal = static_cast<float>(thr / rr64) * rmax;   // scaled |r|^2 that would meet the target
         int32_t status = ST_RUNNING, it = 0, updates = 0;
         if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
         else if (!finite_(bb)) status = CMCG_SOLVE_NON_FINITE;
@@ -996,6 +1036,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             float pq[1] = {0.0f};
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 q[k] = 0.0f;
                 if (i < n) {
@@ -1010,6 +1051,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             float s1[1] = {0.0f};
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) {
                     XH[i] += alpha * P[i];
@@ -1025,9 +1067,10 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             if (!finite_(rzn)) { status = CMCG_SOLVE_NON_FINITE; break; }
             // replace the residual when it dropped by delta, or when it suggests
             // that the FP64 residual may have reached the target
-            if (rzn < d2 * rmax || static_cast<double>(rzn) < thr / rr64 * static_cast<double>(rmax)) {
+            if (rzn < d2 * rmax || rzn < goal) {
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
+                    if (k * kSmemThreads >= n) break;
                     const int i = tid + k * kSmemThreads;
                     if (i < n) {
                         x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
@@ -1038,6 +1081,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
                 double t2[2] = {0.0, 0.0};
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
+                    if (k * kSmemThreads >= n) break;
                     const int i = tid + k * kSmemThreads;
                     if (i < n) {
                         const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
@@ -1053,6 +1097,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
                 rr64 = t2[0];
                 rzn = static_cast<float>(t2[1]);
                 rmax = rzn;
+                goal = static_cast<float>(thr / rr64) * rmax;
                 if (!finite_(rr64)) { status = CMCG_SOLVE_NON_FINITE; break; }
                 if (rr64 < thr) { status = CMCG_SOLVE_CONVERGED; break; }
             }
@@ -1061,6 +1106,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             rz = rzn;
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) P[i] = R[i] + beta * P[i];
             }
@@ -1070,6 +1116,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             // fold the pending increments and report the true residual
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
             }
@@ -1077,6 +1124,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             double t1[1] = {0.0};
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
+                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
                 const int i = tid + k * kSmemThreads;
                 if (i < n) {
                     const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});

@@ -602,8 +602,7 @@ int orc_reliable_scaled_packed(int64_t n_sys, const int64_t* row_off, const int3
             float rzn = dot(r.data(), r.data(), n, t32);
             ++it;
             folded = false;
-            if (rzn < static_cast<float>(delta * delta) * rmax ||
-                static_cast<double>(rzn) < thr / rr64 * static_cast<double>(rmax)) {
+            if (rzn < static_cast<float>(delta * delta) * rmax || rzn < static_cast<float>(thr / rr64) * rmax) {
                 for (int64_t i = 0; i < n; ++i) { xs[i] += sc[i] * static_cast<double>(xh[i]); xh[i] = 0.0f; }
                 std::vector<double> r64(n), rh2(n);
                 residual(r64);
