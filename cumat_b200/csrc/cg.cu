@@ -48,6 +48,7 @@ using namespace cmcg;
 namespace {
 
 constexpr int kTile = 256;          // rows per tile of the grid path (= threads per CTA)
+constexpr int kGridCtasPerSm = 4;   // grid path CTAs per SM (segment plan size)
 constexpr int kPersistThreads = 256;
 
 // ---------------------------------------------------------------------------
@@ -111,8 +112,12 @@ struct SolveArgs {
     // grid path tiles
     int32_t n_tiles;
     const int32_t* tile_row0;
-    const int32_t* tile_sys;
-    const int32_t* sys_tile_begin;
+    int32_t n_seg;
+    const int32_t* seg_t0;       // segment = tiles [seg_t0, seg_t1) of one CTA in one system
+    const int32_t* seg_t1;
+    const int32_t* seg_sys;
+    const int32_t* cta_seg0;     // segments of CTA c: [cta_seg0[c], cta_seg0[c+1])
+    const int32_t* sys_seg0;     // segments of system s: [sys_seg0[s], sys_seg0[s+1])
     VT* part1;
     VT* part2;
     int32_t* active;
@@ -1221,75 +1226,87 @@ __device__ bool tile_ticket(const VT (&v)[NV], VT* const (&part)[NV], int64_t pb
     return true;
 }
 
-struct TileInfo {
-    int b, t, s, inst, r0, r1, sr0, t_begin, t_count;   // sr0: first row of the system
+// The grid path's work plan: the tiles are split into gridDim.x contiguous
+// ranges, one per CTA; a "segment" is the part of one CTA's range that lies in
+// one system. Each CTA keeps its running sums in registers over a segment's
+// tiles and publishes one partial per segment; the last segment of a system
+// instance to finish (ticket) adds that system's partials in segment order.
+// A system's segments have consecutive ids, so the closing sum reads at most
+// gridDim.x values.
+struct SegInfo {
+    int s, inst, t0, t1, sr0, send, pidx, pbase, count;
 };
 
 template <typename VT, typename MT>
-__device__ __forceinline__ TileInfo tile_info(const SolveArgs<VT, MT>& a, int64_t item) {
-    TileInfo ti;
-    ti.b = static_cast<int>(item / a.n_tiles);
-    ti.t = static_cast<int>(item - static_cast<int64_t>(ti.b) * a.n_tiles);
-    ti.s = a.tile_sys[ti.t];
-    ti.inst = ti.b * a.n_sys + ti.s;
-    ti.r0 = a.tile_row0[ti.t];
-    ti.r1 = min(ti.r0 + kTile, a.row_off[ti.s + 1]);
-    ti.sr0 = a.row_off[ti.s];
-    ti.t_begin = a.sys_tile_begin[ti.s];
-    ti.t_count = a.sys_tile_begin[ti.s + 1] - ti.t_begin;
-    return ti;
+__device__ __forceinline__ SegInfo seg_info(const SolveArgs<VT, MT>& a, int b, int seg) {
+    SegInfo g;
+    g.s = a.seg_sys[seg];
+    g.inst = b * a.n_sys + g.s;
+    g.t0 = a.seg_t0[seg];
+    g.t1 = a.seg_t1[seg];
+    g.sr0 = a.row_off[g.s];
+    g.send = a.row_off[g.s + 1];
+    g.pidx = b * a.n_seg + seg;
+    g.pbase = b * a.n_seg + a.sys_seg0[g.s];
+    g.count = a.sys_seg0[g.s + 1] - a.sys_seg0[g.s];
+    return g;
 }
+
+#define CMCG_FOR_SEGMENTS(a)                                                     \
+    for (int b_ = 0; b_ < (a).ob; ++b_)                                          \
+        for (int seg_ = (a).cta_seg0[blockIdx.x]; seg_ < (a).cta_seg0[blockIdx.x + 1]; ++seg_)
 
 // init A: x = guess or 0, r = b - A x, |b|^2, |r|^2 -> status
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
-    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const TileInfo ti = tile_info(a, item);
-        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const VT* bv = a.b + (a.b_b == 1 ? 0 : vo);
         VT* x = a.x + vo;
         VT* r = a.r + vo;
         VT acc[2] = {VT(0), VT(0)};
-        if (a.guess) {
-            const VT* g = a.guess + (a.g_b == 1 ? 0 : vo);
-            const auto A = inst_matrix<MT, FMT>(a.m, ti.b);
-            cta_rows<VT>(A, ti.s, ti.sr0, ti.r0 - ti.sr0, ti.r1 - ti.r0, GlobalX<VT>{g}, [&](int row, VT v) {
-                const VT bi = bv[row];
-                const VT ri = bi - v;
-                r[row] = ri;
-                x[row] = g[row];
-                acc[0] += bi * bi;
-                acc[1] += ri * ri;
-            });
-        } else {
-            const int i = ti.r0 + threadIdx.x;
-            if (i < ti.r1) {
-                const VT bi = bv[i];
-                r[i] = bi;
-                x[i] = VT(0);
-                acc[0] = bi * bi;
-                acc[1] = acc[0];
+        const auto A = inst_matrix<MT, FMT>(a.m, b_);
+        const VT* gv = a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr;
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
+            if (gv) {
+                cta_rows<VT>(A, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<VT>{gv}, [&](int row, VT v) {
+                    const VT bi = bv[row];
+                    const VT ri = bi - v;
+                    r[row] = ri;
+                    x[row] = gv[row];
+                    acc[0] += bi * bi;
+                    acc[1] += ri * ri;
+                });
+            } else {
+                const int i = r0 + threadIdx.x;
+                if (i < r1) {
+                    const VT bi = bv[i];
+                    r[i] = bi;
+                    x[i] = VT(0);
+                    acc[0] += bi * bi;
+                    acc[1] += bi * bi;
+                }
             }
         }
         block_sum<VT, 2>(acc, red);
         VT tot[2];
         VT* const parts[2] = {a.part1, a.part2};
-        if (tile_ticket<VT, 2>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
-                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk1, ti.inst, tot, red, &last_s) &&
+        if (tile_ticket<VT, 2>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk1, g.inst, tot, red, &last_s) &&
             threadIdx.x == 0) {
             const VT bb = tot[0], rr = tot[1], tol = static_cast<VT>(a.tol);
-            a.st.bb[ti.inst] = bb;
-            a.st.rr[ti.inst] = rr;
-            a.st.it[ti.inst] = 0;
-            a.st.outer[ti.inst] = 0;
+            a.st.bb[g.inst] = bb;
+            a.st.rr[g.inst] = rr;
+            a.st.it[g.inst] = 0;
+            a.st.outer[g.inst] = 0;
             int32_t status = ST_RUNNING;
             if ((a.abs_zero_test && bb < tol * tol) || bb == VT(0)) status = CMCG_SOLVE_ZERO_RHS;
             else if (!finite_(bb) || !finite_(rr)) status = CMCG_SOLVE_NON_FINITE;
             else if (rr < tol * tol * bb) status = CMCG_SOLVE_CONVERGED;
-            a.st.status[ti.inst] = status;
+            a.st.status[g.inst] = status;
             if (status == ST_RUNNING) atomicAdd(a.active, 1);
         }
     }
@@ -1300,38 +1317,41 @@ template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
-    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const TileInfo ti = tile_info(a, item);
-        const int32_t st = ld_status(a.st.status + ti.inst);
-        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
-        const int i = ti.r0 + threadIdx.x;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        const int32_t st = ld_status(a.st.status + g.inst);
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         if (st == CMCG_SOLVE_ZERO_RHS) {
-            if (i < ti.r1) a.x[vo + i] = VT(0);
+            for (int t = g.t0; t < g.t1; ++t) {
+                const int i = a.tile_row0[t] + threadIdx.x;
+                if (i < min(a.tile_row0[t] + kTile, g.send)) a.x[vo + i] = VT(0);
+            }
             continue;
         }
         if (st != ST_RUNNING) continue;
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
         VT acc[1] = {VT(0)};
-        if (i < ti.r1) {
-            const VT ri = a.r[vo + i];
-            const VT zi = dinv ? dinv[i] * ri : ri;
-            a.p[vo + i] = zi;
-            acc[0] = ri * zi;
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) {
+                const VT ri = a.r[vo + i];
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                a.p[vo + i] = zi;
+                acc[0] += ri * zi;
+            }
         }
         block_sum<VT, 1>(acc, red);
         VT tot[1];
         VT* const parts[1] = {a.part1};
-        if (tile_ticket<VT, 1>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
-                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk2, ti.inst, tot, red, &last_s) &&
+        if (tile_ticket<VT, 1>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk2, g.inst, tot, red, &last_s) &&
             threadIdx.x == 0) {
             const VT rz = tot[0];
-            a.st.rz[ti.inst] = rz;
+            a.st.rz[g.inst] = rz;
             int32_t status = ST_RUNNING;
             if (!finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
             else if (!(rz > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
             if (status != ST_RUNNING) {
-                a.st.status[ti.inst] = status;
+                a.st.status[g.inst] = status;
                 atomicSub(a.active, 1);
             }
         }
@@ -1343,35 +1363,36 @@ template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
     __shared__ VT red[kTile / 32];
     __shared__ bool last_s;
-    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const TileInfo ti = tile_info(a, item);
-        if (ld_status(a.st.status + ti.inst) != ST_RUNNING) continue;
-        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const VT* p = a.p + vo;
         VT* q = a.q + vo;
-        const auto A = inst_matrix<MT, FMT>(a.m, ti.b);
+        const auto A = inst_matrix<MT, FMT>(a.m, b_);
         VT acc[1] = {VT(0)};
-        cta_rows<VT>(A, ti.s, ti.sr0, ti.r0 - ti.sr0, ti.r1 - ti.r0, GlobalX<VT>{p}, [&](int row, VT v) {
-            q[row] = v;
-            acc[0] += p[row] * v;
-        });
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
+            cta_rows<VT>(A, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<VT>{p}, [&](int row, VT v) {
+                q[row] = v;
+                acc[0] += p[row] * v;
+            });
+        }
         block_sum<VT, 1>(acc, red);
         VT tot[1];
         VT* const parts[1] = {a.part1};
-        if (tile_ticket<VT, 1>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
-                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk1, ti.inst, tot, red, &last_s) &&
+        if (tile_ticket<VT, 1>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk1, g.inst, tot, red, &last_s) &&
             threadIdx.x == 0) {
             const VT pq = tot[0];
-            const VT alpha = static_cast<VT>(a.st.rz[ti.inst]) / pq;
+            const VT alpha = static_cast<VT>(a.st.rz[g.inst]) / pq;
             int32_t status = ST_RUNNING;
             if (!finite_(pq) || !finite_(alpha)) status = CMCG_SOLVE_NON_FINITE;
             else if (!(pq > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
             if (status != ST_RUNNING) {
-                a.st.status[ti.inst] = status;
+                a.st.status[g.inst] = status;
                 atomicSub(a.active, 1);
             } else {
-                a.st.alpha[ti.inst] = alpha;
+                a.st.alpha[g.inst] = alpha;
             }
         }
     }
@@ -1382,48 +1403,48 @@ template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
-    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const TileInfo ti = tile_info(a, item);
-        if (ld_status(a.st.status + ti.inst) != ST_RUNNING) continue;
-        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
-        const VT alpha = static_cast<VT>(a.st.alpha[ti.inst]);
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const VT alpha = static_cast<VT>(a.st.alpha[g.inst]);
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
-        const int i = ti.r0 + threadIdx.x;
         VT acc[2] = {VT(0), VT(0)};
-        if (i < ti.r1) {
-            a.x[vo + i] += alpha * a.p[vo + i];
-            const VT ri = a.r[vo + i] - alpha * a.q[vo + i];
-            a.r[vo + i] = ri;
-            const VT zi = dinv ? dinv[i] * ri : ri;
-            acc[0] = ri * ri;
-            acc[1] = ri * zi;
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) {
+                a.x[vo + i] += alpha * a.p[vo + i];
+                const VT ri = a.r[vo + i] - alpha * a.q[vo + i];
+                a.r[vo + i] = ri;
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                acc[0] += ri * ri;
+                acc[1] += ri * zi;
+            }
         }
         block_sum<VT, 2>(acc, red);
         VT tot[2];
         VT* const parts[2] = {a.part1, a.part2};
-        if (tile_ticket<VT, 2>(acc, parts, static_cast<int64_t>(ti.b) * a.n_tiles, ti.t_begin, ti.t_count,
-                               static_cast<int64_t>(ti.b) * a.n_tiles + ti.t, a.st.tk2, ti.inst, tot, red, &last_s) &&
+        if (tile_ticket<VT, 2>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk2, g.inst, tot, red, &last_s) &&
             threadIdx.x == 0) {
             const VT rr = tot[0], rzn = tot[1];
             const VT tol = static_cast<VT>(a.tol);
-            const VT bb = static_cast<VT>(a.st.bb[ti.inst]);
-            a.st.rr[ti.inst] = rr;
+            const VT bb = static_cast<VT>(a.st.bb[g.inst]);
+            a.st.rr[g.inst] = rr;
             int32_t status = ST_RUNNING;
-            const int n = a.row_off[ti.s + 1] - a.row_off[ti.s];
+            const int n = g.send - g.sr0;
             if (!finite_(rr) || !finite_(rzn)) status = CMCG_SOLVE_NON_FINITE;
             else if (rr < tol * tol * bb) status = CMCG_SOLVE_CONVERGED;
             else if (!(rzn > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
             else {
-                const VT rz = static_cast<VT>(a.st.rz[ti.inst]);
-                a.st.beta[ti.inst] = rzn / rz;
-                a.st.rz[ti.inst] = rzn;
-                const int32_t it = a.st.it[ti.inst] + 1;
-                a.st.it[ti.inst] = it;
+                const VT rz = static_cast<VT>(a.st.rz[g.inst]);
+                a.st.beta[g.inst] = rzn / rz;
+                a.st.rz[g.inst] = rzn;
+                const int32_t it = a.st.it[g.inst] + 1;
+                a.st.it[g.inst] = it;
                 if (it >= sys_max_iter(a.max_iter, n)) status = CMCG_SOLVE_MAX_ITER;
             }
             if (status != ST_RUNNING) {
-                a.st.status[ti.inst] = status;
+                a.st.status[g.inst] = status;
                 atomicSub(a.active, 1);
             }
         }
@@ -1433,17 +1454,19 @@ __global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
 // iteration kernel 3: p = M^-1 r + beta p
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile) k_grid_pupdate(SolveArgs<VT, MT> a) {
-    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const TileInfo ti = tile_info(a, item);
-        if (ld_status(a.st.status + ti.inst) != ST_RUNNING) continue;
-        const int64_t vo = static_cast<int64_t>(ti.b) * a.rows;
-        const int i = ti.r0 + threadIdx.x;
-        if (i < ti.r1) {
-            const VT beta = static_cast<VT>(a.st.beta[ti.inst]);
-            const VT ri = a.r[vo + i];
-            const VT zi = a.dinv ? a.dinv[(a.dinv_b == 1 ? 0 : vo) + i] * ri : ri;
-            a.p[vo + i] = zi + beta * a.p[vo + i];
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const VT beta = static_cast<VT>(a.st.beta[g.inst]);
+        const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) {
+                const VT ri = a.r[vo + i];
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                a.p[vo + i] = zi + beta * a.p[vo + i];
+            }
         }
     }
 }
@@ -1523,8 +1546,13 @@ struct cmcg_solver_s {
     int32_t n_sys = 0, max_sys_rows = 0, n_tiles = 0;
     int32_t* d_order = nullptr;
     int32_t* d_tile_row0 = nullptr;
-    int32_t* d_tile_sys = nullptr;
-    int32_t* d_sys_tile_begin = nullptr;
+    // grid path segment plan (see SegInfo)
+    int32_t grid_ctas = 1, n_seg = 0;
+    int32_t* d_seg_t0 = nullptr;
+    int32_t* d_seg_t1 = nullptr;
+    int32_t* d_seg_sys = nullptr;
+    int32_t* d_cta_seg0 = nullptr;
+    int32_t* d_sys_seg0 = nullptr;
     // Jacobi inverse diagonal per vector type (F32, F64), [matrix batches][rows]
     void* dinv[2] = {nullptr, nullptr};
     // workspace
@@ -1582,19 +1610,42 @@ cmcg_status build_plan(cmcg_solver s) {
     s->max_sys_rows = maxr;
     s->n_tiles = static_cast<int32_t>(t_row0.size());
     s->systems_version = p->systems_version;
-    cudaStream_t st = p->ctx->stream;
-    for (int32_t** d : {&s->d_order, &s->d_tile_row0, &s->d_tile_sys, &s->d_sys_tile_begin}) {
-        dev_free(*d);
-        *d = nullptr;
+    // grid path: contiguous tile ranges per CTA, cut into segments at system
+    // boundaries (segment ids of one system are consecutive)
+    const int32_t G = std::max<int32_t>(1, std::min<int32_t>(s->n_tiles, p->ctx->sm_count * kGridCtasPerSm));
+    std::vector<int32_t> seg_t0, seg_t1, seg_sys, cta_seg0(G + 1), sys_seg0(n_sys + 1, -1);
+    for (int32_t c = 0; c < G; ++c) {
+        cta_seg0[c] = static_cast<int32_t>(seg_t0.size());
+        const int32_t a = static_cast<int32_t>(static_cast<int64_t>(c) * s->n_tiles / G);
+        const int32_t e = static_cast<int32_t>(static_cast<int64_t>(c + 1) * s->n_tiles / G);
+        for (int32_t t = a; t < e;) {
+            const int32_t sys = t_sys[t];
+            int32_t u = t;
+            while (u < e && t_sys[u] == sys) ++u;
+            if (sys_seg0[sys] < 0) sys_seg0[sys] = static_cast<int32_t>(seg_t0.size());
+            seg_t0.push_back(t);
+            seg_t1.push_back(u);
+            seg_sys.push_back(sys);
+            t = u;
+        }
     }
-    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_order), order.size() * 4));
-    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_tile_row0), t_row0.size() * 4));
-    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_tile_sys), t_sys.size() * 4));
-    CMCG_TRY(dev_alloc(reinterpret_cast<void**>(&s->d_sys_tile_begin), t_begin.size() * 4));
-    CMCG_CUDA(cudaMemcpyAsync(s->d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
-    CMCG_CUDA(cudaMemcpyAsync(s->d_tile_row0, t_row0.data(), t_row0.size() * 4, cudaMemcpyHostToDevice, st));
-    CMCG_CUDA(cudaMemcpyAsync(s->d_tile_sys, t_sys.data(), t_sys.size() * 4, cudaMemcpyHostToDevice, st));
-    CMCG_CUDA(cudaMemcpyAsync(s->d_sys_tile_begin, t_begin.data(), t_begin.size() * 4, cudaMemcpyHostToDevice, st));
+    cta_seg0[G] = static_cast<int32_t>(seg_t0.size());
+    sys_seg0[n_sys] = static_cast<int32_t>(seg_t0.size());
+    for (int32_t i = n_sys - 1; i >= 0; --i)
+        if (sys_seg0[i] < 0) sys_seg0[i] = sys_seg0[i + 1];   // (every system has at least one tile)
+    s->grid_ctas = G;
+    s->n_seg = static_cast<int32_t>(seg_t0.size());
+    cudaStream_t st = p->ctx->stream;
+    int32_t** bufs[] = {&s->d_order, &s->d_tile_row0, &s->d_seg_t0, &s->d_seg_t1, &s->d_seg_sys, &s->d_cta_seg0,
+                        &s->d_sys_seg0};
+    const std::vector<int32_t>* src[] = {&order, &t_row0, &seg_t0, &seg_t1, &seg_sys, &cta_seg0, &sys_seg0};
+    for (int k = 0; k < 7; ++k) {
+        dev_free(*bufs[k]);
+        *bufs[k] = nullptr;
+        CMCG_TRY(dev_alloc(reinterpret_cast<void**>(bufs[k]), std::max<size_t>(src[k]->size(), 1) * 4));
+        if (!src[k]->empty())
+            CMCG_CUDA(cudaMemcpyAsync(*bufs[k], src[k]->data(), src[k]->size() * 4, cudaMemcpyHostToDevice, st));
+    }
     CMCG_CUDA(cudaStreamSynchronize(st));
     return CMCG_OK;
 }
@@ -1702,8 +1753,12 @@ SolveArgs<VT, MT> base_args(cmcg_solver s, int32_t ob) {
     a.loops = s->counters + 2;
     a.n_tiles = s->n_tiles;
     a.tile_row0 = s->d_tile_row0;
-    a.tile_sys = s->d_tile_sys;
-    a.sys_tile_begin = s->d_sys_tile_begin;
+    a.n_seg = s->n_seg;
+    a.seg_t0 = s->d_seg_t0;
+    a.seg_t1 = s->d_seg_t1;
+    a.seg_sys = s->d_seg_sys;
+    a.cta_seg0 = s->d_cta_seg0;
+    a.sys_seg0 = s->d_sys_seg0;
     a.tol = s->tol;
     a.max_iter = s->max_iter;
     a.abs_zero_test = s->inner_solve ? 0 : 1;
@@ -1826,10 +1881,9 @@ template <typename VT, typename MT, int FMT>
 cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     cmcg_ctx ctx = s->A->pat->ctx;
     cudaStream_t st = ctx->stream;
-    const int64_t items = static_cast<int64_t>(a.n_tiles) * a.ob;
-    int occ = 0;
-    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_grid_spmv_pq<VT, MT, FMT>, kTile, 0));
-    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, static_cast<int64_t>(ctx->sm_count) * std::max(occ, 1))));
+    // one partial per (batch, segment); the grid is the plan's CTA count
+    const int64_t items = static_cast<int64_t>(a.n_seg) * a.ob;
+    const int grid = s->grid_ctas;
     const size_t need = 2 * sizeof(VT) * static_cast<size_t>(items) + 64;
     if (s->part_ws_bytes < need) {
         CMCG_TRY(ensure_buffer(&s->part_ws, &s->part_ws_bytes, need));
@@ -2207,8 +2261,9 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
     cudaStreamSynchronize(s->A->pat->ctx->stream);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
-    for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_tile_sys),
-                    static_cast<void*>(s->d_sys_tile_begin), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
+    for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_seg_t0),
+                    static_cast<void*>(s->d_seg_t1), static_cast<void*>(s->d_seg_sys), static_cast<void*>(s->d_cta_seg0),
+                    static_cast<void*>(s->d_sys_seg0), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
                     s->st_ws, static_cast<void*>(s->counters), s->mix_vals, static_cast<void*>(s->mix_s)})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);
