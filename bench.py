@@ -371,12 +371,16 @@ def run_reference(args):
     b64 = bt.b.astype(np.float64)
     x64 = np.zeros_like(b64)
     threads = O.ref_threads()
-    # each step: a contiguous slice of systems (steps rotate through the batch),
-    # sized to keep the whole run within a few minutes
-    per_step = max(threads * 2, 64)
+    # each step solves the whole batch (a few seconds on a server host); a host
+    # so slow that K + W such steps would exceed the time budget gets a prefix
+    # of the batch per step instead (sides are i.i.d., a prefix is a sample)
+    t_probe, _, _ = ep.solve(0, min(N_SYS, 64), b64, x64, OUTER_TOL, -1, 1, threads)
+    est_full = t_probe * N_SYS / min(N_SYS, 64)
+    per_step = N_SYS if est_full * (args.steps + args.warmup) < 180 else \
+        max(64, int(N_SYS * 180 / (est_full * (args.steps + args.warmup))))
     times, solved = [], 0
     for i in range(args.warmup + args.steps):
-        s0 = (i * per_step) % (N_SYS - per_step)
+        s0 = 0
         dt, it, err = ep.solve(s0, s0 + per_step, b64, x64, OUTER_TOL, -1, 1, threads)
         if i >= args.warmup:
             times.append(dt)
@@ -390,9 +394,59 @@ def run_reference(args):
             "config": {"workload": "4096 uneven 2D FV diffusion systems (sides 16..128, kappa=exp(N(0,0.25))), "
                                    "Eigen FP64 Jacobi-CG to 1e-10", "systems_per_step": per_step},
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{per_step} consecutive systems per step of {N_SYS}"},
+                             "sample": f"first {per_step} of {N_SYS} systems per step, Eigen 3.3.90 "
+                                       f"ConjugateGradient<SparseMatrix<double,RowMajor>, Lower|Upper, "
+                                       f"DiagonalPreconditioner> to 1e-10, OpenMP over systems"},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_profile_small():
+    """The small case for ncu captures (a few hundred MB on the device): three
+    SpMV calls per format on the 1024^2 Poisson matrix, then one mixed and one
+    FP64 batched solve of the first 512 systems of the batch. Prints the
+    algorithmic bytes of the mixed launch so that its DRAM traffic can be
+    compared per unit with the full batch."""
+    import torch
+
+    import cumat_b200 as cm
+    from cumat_b200 import problems as P
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    pr = P.poisson2d(1024, 1)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    idx, ev = P.csr_to_ell(pr.n, pr.row_ptr, pr.col, pr.val)
+    E = cm.SparseMatrix(cm.SparsityPattern.ell(pr.n, pr.n, idx)).setData(ev)
+    x = torch.from_numpy(pr.b).to(dev)
+    y = torch.empty_like(x)
+    for _ in range(3):
+        A.product(x, out=y)
+        E.product(x, out=y)
+    bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED)
+    k = int(bt.row_off[512])
+    kz = int(bt.row_ptr[k])
+    row_off = bt.row_off[:513]
+    p = cm.SparsityPattern.csr(k, k, bt.row_ptr[:k + 1], bt.col[:kz])
+    p.set_systems(row_off)
+    A32 = cm.SparseMatrix(p).setData(bt.val[:kz])
+    cg = cm.ConjugateGradient(A32).setTolerance(INNER_TOL)
+    b64 = torch.from_numpy(bt.b[:k].astype(np.float64)).to(dev)
+    cg.solve_refined(b64, outer=A32, outer_tol=OUTER_TOL, max_outer=MAX_OUTER)
+    A64 = cm.SparseMatrix(p, dtype=torch.float64).setData(bt.val[:kz].astype(np.float64))
+    cg64 = cm.ConjugateGradient(A64).setTolerance(OUTER_TOL)
+    cg64.solve(b64)
+    torch.cuda.synchronize()
+    st = cg.system_stats()
+
+    class _Sub:
+        pass
+    sub = _Sub()
+    sub.row_off, sub.row_ptr = row_off, bt.row_ptr[:k + 1]
+    print(json.dumps({"profile_small": True, "systems": 512, "rows": k, "nnz": kz,
+                      "mixed_alg_bytes": refined_bytes(sub, st["iterations"].astype(np.float64),
+                                                       st["outer"].astype(np.float64)),
+                      "mixed_converged": bool(np.all(st["status"] == 0)),
+                      "fp64_converged": bool(np.all(cg64.system_stats()["status"] == 0))}))
 
 
 def main():
@@ -404,10 +458,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-spmv", action="store_true", help="skip the SpMV GB/s sub-benchmark")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--profile-small", action="store_true",
+                    help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "
+                         "mixed and FP64 solvers on the first 512 systems of the batch")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile_small:
+        run_profile_small()
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -100,6 +100,9 @@ struct InstState {
     double* err;     // sqrt(rr / bb) written by the finaliser
     unsigned* tk1;
     unsigned* tk2;
+    double* rmax;    // mixed solver: scaled |r|^2 at the last residual replacement
+    double* goal;    //   scaled |r|^2 that would meet the FP64 target
+    int32_t* flag;   //   1: replace the residual in this iteration
 };
 
 template <typename VT, typename MT>
@@ -1170,7 +1173,7 @@ __global__ void k_jacobi_scale(const int32_t* __restrict__ rp, const int32_t* __
 
 // out[b][slot] = a * s_row * s_col for every slot of the sliced layout (warp per slice)
 template <typename MS, typename MD>
-__global__ void k_scale_sell(const int32_t* __restrict__ col, const int32_t* __restrict__ off32,
+__global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __restrict__ off64,
                              const int32_t* __restrict__ sw, const int32_t* __restrict__ row0, int32_t n_slices,
                              const MS* __restrict__ src, int64_t sstride, const double* __restrict__ sc, int32_t rows,
                              int32_t mb, MD* __restrict__ dst, int64_t dstride) {
@@ -1180,7 +1183,8 @@ __global__ void k_scale_sell(const int32_t* __restrict__ col, const int32_t* __r
     for (int64_t item = wid; item < static_cast<int64_t>(n_slices) * mb; item += nw) {
         const int b = static_cast<int>(item / n_slices);
         const int sl = static_cast<int>(item - static_cast<int64_t>(b) * n_slices);
-        const int row = row0[sl] + lane, w = sw[sl], off = off32[sl];
+        const int row = row0[sl] + lane, w = sw[sl];
+        const int64_t off = off64[sl];
         const double* sb = sc + static_cast<int64_t>(b) * rows;
         for (int j = 0; j < w; ++j) {
             const int64_t o = off + 32 * j + lane;
@@ -1471,6 +1475,279 @@ __global__ void __launch_bounds__(kTile) k_grid_pupdate(SolveArgs<VT, MT> a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Grid path, mixed precision with reliable updates (large systems)
+//
+// The same method as k_mixed_fast, spread over the whole GPU: FP32 CG on the
+// Jacobi-scaled system S A S (scaled copy of the values in the sliced
+// layout), FP32 increments xh folded into the FP64 solution x with x += S xh,
+// and the recursive residual replaced by S (b - A x) computed in FP64 with the
+// unscaled outer values whenever it dropped by delta (or looks converged).
+// Per iteration the CUDA graph runs: product + p.q, update + |r|^2 (decides
+// whether to replace), fold, FP64 residual (both no-ops unless a replacement is
+// due), p update, loop condition.
+// ---------------------------------------------------------------------------
+
+template <typename MI, typename MO>
+struct GMixArgs {
+    SolveArgs<float, MI> g;   // plan, segments, inner vectors r/p/q (FP32), state; g.m = scaled inner values
+    MatArgs<MO> mo;           // outer values (unscaled) in the sliced layout
+    const double* s;          // [mb][rows]
+    const double* b64;
+    double* x64;
+    float* xh;
+    double* p1;               // FP64 partials of the residual replacement
+    double* p2;
+    double outer_tol;
+    int32_t max_updates;
+    float delta;
+};
+
+template <typename MI, typename MO>
+__global__ void __launch_bounds__(kTile) k_gmix_init(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    __shared__ double red[2 * (kTile / 32)];
+    __shared__ bool last_s;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const double* bv = m.b64 + (a.b_b == 1 ? 0 : vo);
+        const double* sv = m.s + (a.m.mb == 1 ? 0 : vo);
+        double acc[2] = {0.0, 0.0};
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) {
+                const double bi = bv[i];
+                const float rh = static_cast<float>(sv[i] * bi);
+                m.x64[vo + i] = 0.0;
+                m.xh[vo + i] = 0.0f;
+                a.r[vo + i] = rh;
+                a.p[vo + i] = rh;
+                acc[0] += bi * bi;
+                acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
+            }
+        }
+        block_sum<double, 2>(acc, red);
+        double tot[2];
+        double* const parts[2] = {m.p1, m.p2};
+        if (tile_ticket<double, 2>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk1, g.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const double bb = tot[0];
+            const float rz = static_cast<float>(tot[1]);
+            const double thr = m.outer_tol * m.outer_tol * bb;
+            a.st.bb[g.inst] = bb;
+            a.st.rr[g.inst] = bb;
+            a.st.rz[g.inst] = rz;
+            a.st.rmax[g.inst] = rz;
+            a.st.goal[g.inst] = static_cast<double>(static_cast<float>(thr / bb) * rz);
+            a.st.it[g.inst] = 0;
+            a.st.outer[g.inst] = 0;
+            a.st.flag[g.inst] = 0;
+            int32_t status = ST_RUNNING;
+            if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
+            else if (!finite_(bb) || !finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
+            else if (bb < thr) status = CMCG_SOLVE_CONVERGED;
+            else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+            a.st.status[g.inst] = status;
+            if (status == ST_RUNNING) atomicAdd(a.active, 1);
+        }
+    }
+}
+
+// Instances that stopped without a final replacement (breakdown, non-finite
+// values, loop cap) still hold FP32 increments: the closing fold + FP64
+// residual runs for them.
+__device__ __forceinline__ bool gmix_tail_status(int32_t st) {
+    return st == ST_RUNNING || st == CMCG_SOLVE_BREAKDOWN || st == CMCG_SOLVE_NON_FINITE;
+}
+
+// product q = (S A S) p and p.q -> alpha
+template <typename MI, typename MO>
+__global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    __shared__ float red[kTile / 32];
+    __shared__ bool last_s;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const float* p = a.p + vo;
+        float* q = a.q + vo;
+        const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
+        float acc[1] = {0.0f};
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
+            cta_rows<float>(A, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<float>{p}, [&](int row, float v) {
+                q[row] = v;
+                acc[0] += p[row] * v;
+            });
+        }
+        block_sum<float, 1>(acc, red);
+        float tot[1];
+        float* const parts[1] = {a.part1};
+        if (tile_ticket<float, 1>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk1, g.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const float pq = tot[0];
+            const float alpha = static_cast<float>(a.st.rz[g.inst]) / pq;
+            int32_t status = ST_RUNNING;
+            if (!finite_(pq) || !finite_(alpha)) status = CMCG_SOLVE_NON_FINITE;
+            else if (!(pq > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+            if (status != ST_RUNNING) {
+                a.st.status[g.inst] = status;
+                atomicSub(a.active, 1);
+            } else {
+                a.st.alpha[g.inst] = alpha;
+            }
+        }
+    }
+}
+
+// xh += alpha p, r -= alpha q, |r|^2 -> replacement decision or beta
+template <typename MI, typename MO>
+__global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    __shared__ float red[kTile / 32];
+    __shared__ bool last_s;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const float alpha = static_cast<float>(a.st.alpha[g.inst]);
+        float acc[1] = {0.0f};
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) {
+                m.xh[vo + i] += alpha * a.p[vo + i];
+                const float ri = a.r[vo + i] - alpha * a.q[vo + i];
+                a.r[vo + i] = ri;
+                acc[0] += ri * ri;
+            }
+        }
+        block_sum<float, 1>(acc, red);
+        float tot[1];
+        float* const parts[1] = {a.part2};
+        if (tile_ticket<float, 1>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk2, g.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            const float rzn = tot[0];
+            const int32_t it = a.st.it[g.inst] + 1;
+            a.st.it[g.inst] = it;
+            const float d2 = m.delta * m.delta;
+            const int n = g.send - g.sr0;
+            if (!finite_(rzn)) {
+                a.st.status[g.inst] = CMCG_SOLVE_NON_FINITE;
+                atomicSub(a.active, 1);
+            } else if (rzn < d2 * static_cast<float>(a.st.rmax[g.inst]) || rzn < static_cast<float>(a.st.goal[g.inst]) ||
+                       it >= sys_max_iter(a.max_iter, n)) {
+                a.st.flag[g.inst] = 1;   // fold and replace in this iteration
+            } else if (!(rzn > 0.0f)) {
+                a.st.status[g.inst] = CMCG_SOLVE_BREAKDOWN;
+                atomicSub(a.active, 1);
+            } else {
+                a.st.beta[g.inst] = rzn / static_cast<float>(a.st.rz[g.inst]);
+                a.st.rz[g.inst] = rzn;
+            }
+        }
+    }
+}
+
+// x += S xh where a replacement is due (TAIL: where the solve stopped unfolded)
+template <typename MI, typename MO, bool TAIL>
+__global__ void __launch_bounds__(kTile) k_gmix_fold(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        const int32_t st = ld_status(a.st.status + g.inst);
+        if (TAIL ? !gmix_tail_status(st) : (st != ST_RUNNING || !ld_status(a.st.flag + g.inst))) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const double* sv = m.s + (a.m.mb == 1 ? 0 : vo);
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) {
+                m.x64[vo + i] += sv[i] * static_cast<double>(m.xh[vo + i]);
+                m.xh[vo + i] = 0.0f;
+            }
+        }
+    }
+}
+
+// r = S (b - A x) in FP64 where a replacement is due -> convergence, beta
+// (TAIL: only the final |b - A x|^2 of the instances folded by the tail)
+template <typename MI, typename MO, bool TAIL>
+__global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    __shared__ double red[2 * (kTile / 32)];
+    __shared__ bool last_s;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        const int32_t st = ld_status(a.st.status + g.inst);
+        if (TAIL ? !gmix_tail_status(st) : (st != ST_RUNNING || !ld_status(a.st.flag + g.inst))) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const double* bv = m.b64 + (a.b_b == 1 ? 0 : vo);
+        const double* sv = m.s + (a.m.mb == 1 ? 0 : vo);
+        const double* xv = m.x64 + vo;
+        const auto Ao = inst_matrix<MO, CMCG_CSR>(m.mo, b_);
+        double acc[2] = {0.0, 0.0};
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
+            cta_rows<double>(Ao, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<double>{xv}, [&](int row, double v) {
+                const double r64 = bv[row] - v;
+                const float rh = static_cast<float>(sv[row] * r64);
+                if (!TAIL) a.r[vo + row] = rh;
+                acc[0] += r64 * r64;
+                acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
+            });
+        }
+        block_sum<double, 2>(acc, red);
+        double tot[2];
+        double* const parts[2] = {m.p1, m.p2};
+        if (tile_ticket<double, 2>(acc, parts, g.pbase, 0, g.count, g.pidx, a.st.tk1, g.inst, tot, red, &last_s) &&
+            threadIdx.x == 0) {
+            if (TAIL) {
+                a.st.rr[g.inst] = tot[0];
+                continue;
+            }
+            const double rr64 = tot[0], bb = a.st.bb[g.inst];
+            const float rzn = static_cast<float>(tot[1]);
+            const double thr = m.outer_tol * m.outer_tol * bb;
+            const int32_t outer = a.st.outer[g.inst] + 1;
+            a.st.outer[g.inst] = outer;
+            a.st.rr[g.inst] = rr64;
+            a.st.rmax[g.inst] = rzn;
+            a.st.goal[g.inst] = static_cast<double>(static_cast<float>(thr / rr64) * rzn);
+            a.st.flag[g.inst] = 0;
+            const int n = g.send - g.sr0;
+            int32_t status = ST_RUNNING;
+            if (!finite_(rr64)) status = CMCG_SOLVE_NON_FINITE;
+            else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
+            else if (a.st.it[g.inst] >= sys_max_iter(a.max_iter, n) || outer >= m.max_updates) status = CMCG_SOLVE_MAX_ITER;
+            else if (!(rzn > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+            if (status != ST_RUNNING) {
+                a.st.status[g.inst] = status;
+                atomicSub(a.active, 1);
+            } else {
+                a.st.beta[g.inst] = rzn / static_cast<float>(a.st.rz[g.inst]);
+                a.st.rz[g.inst] = rzn;
+            }
+        }
+    }
+}
+
+// p = r + beta p
+template <typename MI, typename MO>
+__global__ void __launch_bounds__(kTile) k_gmix_pupdate(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const float beta = static_cast<float>(a.st.beta[g.inst]);
+        for (int t = g.t0; t < g.t1; ++t) {
+            const int i = a.tile_row0[t] + threadIdx.x;
+            if (i < min(a.tile_row0[t] + kTile, g.send)) a.p[vo + i] = a.r[vo + i] + beta * a.p[vo + i];
+        }
+    }
+}
+
 // loop condition of the graph's WHILE node (one thread)
 __global__ void k_grid_cond(const int32_t* active, int32_t* loops, int32_t cap, cudaGraphConditionalHandle h) {
     const int32_t l = ++(*loops);
@@ -1576,6 +1853,10 @@ struct cmcg_solver_s {
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     std::vector<char> gkey;
+    // graph cache of the grid path's mixed solve (keyed by its kernel arguments)
+    cudaGraphExec_t gexec_mix = nullptr;
+    cudaGraph_t graph_mix = nullptr;
+    std::vector<char> gkey_mix;
     // last solve
     int32_t last_inst = 0;
     bool last_refined = false;
@@ -1700,7 +1981,7 @@ cmcg_status get_dinv(cmcg_solver s, int32_t vdt, const void** out) {
 }
 
 cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
-    const size_t per = 6 * sizeof(double) + 3 * sizeof(int32_t) + 2 * sizeof(unsigned);
+    const size_t per = 8 * sizeof(double) + 4 * sizeof(int32_t) + 2 * sizeof(unsigned);
     const size_t need = per * static_cast<size_t>(n_inst) + 256;
     if (s->st_inst >= n_inst && s->st_ws) return CMCG_OK;
     dev_free(s->st_ws);
@@ -1716,6 +1997,9 @@ cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
     s->st.alpha = reinterpret_cast<double*>(b); b += 8 * n;
     s->st.beta = reinterpret_cast<double*>(b); b += 8 * n;
     s->st.err = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.rmax = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.goal = reinterpret_cast<double*>(b); b += 8 * n;
+    s->st.flag = reinterpret_cast<int32_t*>(b); b += 4 * n;
     s->st.it = reinterpret_cast<int32_t*>(b); b += 4 * n;
     s->st.status = reinterpret_cast<int32_t*>(b); b += 4 * n;
     s->st.outer = reinterpret_cast<int32_t*>(b); b += 4 * n;
@@ -1795,7 +2079,7 @@ cmcg_status build_mix(cmcg_solver s) {
     const int blocks = ctx->sm_count * 8;
     k_jacobi_scale<MT><<<blocks, 256, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, static_cast<const MT*>(A->d_vals), A->stride,
                                                       p->rows, A->batches, s->precond == CMCG_PRECOND_JACOBI ? 1 : 0, s->mix_s);
-    k_scale_sell<MT, MT><<<blocks, 256, 0, ctx->stream>>>(S.d_col, S.d_slice_off32, S.d_slice_w, S.d_slice_row0, S.n_slices,
+    k_scale_sell<MT, MT><<<blocks, 256, 0, ctx->stream>>>(S.d_col, S.d_slice_off, S.d_slice_w, S.d_slice_row0, S.n_slices,
                                                          static_cast<const MT*>(A->d_sell_vals), A->sell_stride, s->mix_s,
                                                          p->rows, A->batches, static_cast<MT*>(s->mix_vals), s->mix_stride);
     count_launch(2);
@@ -2216,6 +2500,110 @@ cmcg_status refined_grid(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t
     return cleanup(CMCG_OK);
 }
 
+// Reliable-update mixed solve on the grid path (CSR patterns): the iteration is
+// one WHILE-node graph (product, update, fold, FP64 residual, p update, loop
+// condition); b and x go through internal copies so the graph's arguments do
+// not depend on the caller's buffers.
+template <typename MI, typename MO>
+cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_b, double* x, int32_t ob,
+                               double outer_tol, int32_t max_outer) {
+    cmcg_pattern p = s->A->pat;
+    cmcg_ctx ctx = p->ctx;
+    cudaStream_t st = ctx->stream;
+    const int32_t n_inst = ob * s->n_sys;
+    CMCG_TRY(ensure_state(s, n_inst));
+    CMCG_TRY(ensure_sell_values(s->A));
+    if (Ao != s->A) CMCG_TRY(ensure_sell_values(Ao));
+    CMCG_TRY(ensure_mix(s));
+    const size_t nv = static_cast<size_t>(p->rows) * ob, nb = static_cast<size_t>(p->rows) * b_b;
+    const size_t need = (nv + nb) * sizeof(double) + 4 * nv * sizeof(float) + 512;
+    CMCG_TRY(ensure_buffer(&s->ref_ws, &s->ref_ws_bytes, need));
+    double* x64 = static_cast<double*>(s->ref_ws);
+    double* b64 = x64 + nv;
+    float* f = reinterpret_cast<float*>(b64 + nb);
+    const int64_t items = static_cast<int64_t>(s->n_seg) * ob;
+    CMCG_TRY(ensure_buffer(&s->part_ws, &s->part_ws_bytes, items * (2 * sizeof(double) + 2 * sizeof(float)) + 256));
+    double* p1 = static_cast<double*>(s->part_ws);
+    GMixArgs<MI, MO> m{};
+    m.g = base_args<float, MI>(s, ob);
+    m.g.m.sell_vals = static_cast<const MI*>(s->mix_vals);
+    m.g.m.sell_vstride = s->mix_stride;
+    m.g.b_b = b_b;
+    m.g.r = f; m.g.p = f + nv; m.g.q = f + 2 * nv;
+    m.g.part1 = reinterpret_cast<float*>(p1 + 2 * items);
+    m.g.part2 = m.g.part1 + items;
+    m.g.abs_zero_test = 0;
+    int64_t cap = s->max_iter >= 0 ? s->max_iter : 2 * static_cast<int64_t>(s->max_sys_rows);
+    m.g.loop_cap = static_cast<int32_t>(std::min<int64_t>(cap + 2, INT32_MAX - 1));
+    m.mo = mat_args<MO>(Ao);
+    m.s = s->mix_s;
+    m.b64 = b64;
+    m.x64 = x64;
+    m.xh = f + 3 * nv;
+    m.p1 = p1;
+    m.p2 = p1 + items;
+    m.outer_tol = outer_tol;
+    m.max_updates = max_outer;
+    m.delta = static_cast<float>(s->refine_delta);
+    const int grid = s->grid_ctas;
+
+    CMCG_CUDA(cudaMemcpyAsync(b64, b, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), st));
+    k_gmix_init<MI, MO><<<grid, kTile, 0, st>>>(m);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    std::vector<char> key(sizeof(m) + sizeof(int) * 2);
+    {
+        GMixArgs<MI, MO> k = m;
+        k.g.cond = 0;
+        std::memcpy(key.data(), &k, sizeof(k));
+        const int ids[2] = {DT<MI>::id, DT<MO>::id};
+        std::memcpy(key.data() + sizeof(k), ids, sizeof(ids));
+    }
+    if (!s->gexec_mix || key != s->gkey_mix) {
+        if (s->gexec_mix) { cudaGraphExecDestroy(s->gexec_mix); s->gexec_mix = nullptr; }
+        if (s->graph_mix) { cudaGraphDestroy(s->graph_mix); s->graph_mix = nullptr; }
+        cudaGraph_t g;
+        CMCG_CUDA(cudaGraphCreate(&g, 0));
+        s->graph_mix = g;
+        cudaGraphConditionalHandle h;
+        CMCG_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CMCG_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        m.g.cond = h;
+        if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
+        cudaStream_t cs = ctx->capture_stream;
+        CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        k_gmix_spmv<MI, MO><<<grid, kTile, 0, cs>>>(m);
+        k_gmix_update<MI, MO><<<grid, kTile, 0, cs>>>(m);
+        k_gmix_fold<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
+        k_gmix_residual<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
+        k_gmix_pupdate<MI, MO><<<grid, kTile, 0, cs>>>(m);
+        k_grid_cond<<<1, 1, 0, cs>>>(m.g.active, m.g.loops, m.g.loop_cap, h);
+        cudaGraph_t captured = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+        if (ce != cudaSuccess) return cuda_fail(ce, "capture of the mixed CG iteration", __FILE__, __LINE__);
+        CMCG_CUDA(cudaGraphInstantiate(&s->gexec_mix, g, 0));
+        s->gkey_mix = key;
+    }
+    CMCG_CUDA(cudaGraphLaunch(s->gexec_mix, st));
+    k_gmix_fold<MI, MO, true><<<grid, kTile, 0, st>>>(m);
+    k_gmix_residual<MI, MO, true><<<grid, kTile, 0, st>>>(m);
+    k_finalize<<<(n_inst + 255) / 256, 256, 0, st>>>(s->st, n_inst);
+    count_launch(4);
+    CMCG_CHECK_LAUNCH();
+    CMCG_CUDA(cudaMemcpyAsync(x, x64, nv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    s->last_inst = n_inst;
+    s->last_refined = true;
+    return CMCG_OK;
+}
+
 template <typename MI, int FMT>
 cmcg_status refined_mi(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_b, double* x, int32_t ob, double ot,
                        int32_t mo) {
@@ -2261,6 +2649,8 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
     cudaStreamSynchronize(s->A->pat->ctx->stream);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->gexec_mix) cudaGraphExecDestroy(s->gexec_mix);
+    if (s->graph_mix) cudaGraphDestroy(s->graph_mix);
     for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_seg_t0),
                     static_cast<void*>(s->d_seg_t1), static_cast<void*>(s->d_seg_sys), static_cast<void*>(s->d_cta_seg0),
                     static_cast<void*>(s->d_sys_seg0), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
@@ -2415,15 +2805,27 @@ cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b
     CMCG_CUDA(cudaSetDevice(s->A->pat->ctx->device));
     CMCG_TRY(refresh_plan(s));
     const int32_t ob = std::max(s->A->batches, b_batches);
-    // packed systems always run persistent (the grid refinement drives one
-    // system per batch from the host)
+    const int fmt = s->A->pat->format;
     int32_t path = choose_path(s, ob * s->n_sys);
-    if (s->n_sys > 1 && s->path == CMCG_PATH_AUTO) path = CMCG_PATH_PERSISTENT;
+    // the grid path's reliable-update solver needs the sliced layout (CSR)
+    const bool grid_mixed = fmt == CMCG_CSR && s->refine_method == CMCG_REFINE_RELIABLE;
+    // packed systems run persistent (one CTA per system, vectors in shared
+    // memory where they fit) unless they are too large for shared memory and
+    // the grid solver handles them
+    if (s->n_sys > 1 && s->path == CMCG_PATH_AUTO && (!grid_mixed || s->max_sys_rows <= kSmemMaxRows))
+        path = CMCG_PATH_PERSISTENT;
     if (path == CMCG_PATH_GRID) {
-        CMCG_REQUIRE(s->n_sys == 1, "cmcg_cg_solve_refined: the grid path refines one system per batch");
+        if (grid_mixed) {
+            if (s->A->dtype == CMCG_F32)
+                return Ao->dtype == CMCG_F64 ? refined_grid_mixed<float, double>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer)
+                                             : refined_grid_mixed<float, float>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
+            return Ao->dtype == CMCG_F64
+                       ? refined_grid_mixed<__nv_bfloat16, double>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer)
+                       : refined_grid_mixed<__nv_bfloat16, float>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
+        }
+        CMCG_REQUIRE(s->n_sys == 1, "cmcg_cg_solve_refined: the grid path's restart refinement takes one system per batch");
         return refined_grid(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
     }
-    const int fmt = s->A->pat->format;
     if (s->A->dtype == CMCG_F32)
         return fmt == CMCG_CSR ? refined_mi<float, CMCG_CSR>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer)
                                : refined_mi<float, CMCG_ELLPACK>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);

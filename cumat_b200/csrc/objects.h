@@ -41,12 +41,12 @@ struct SellPlan {
     int64_t* d_slice_off = nullptr;   // n_slices + 1
     int32_t* d_slice_w = nullptr;     // n_slices
     int32_t* d_sys_slice0 = nullptr;  // n_sys + 1, first slice of each system
+    int32_t* d_slice_row0 = nullptr;  // n_slices, first global row of each slice
     // compact form for the fast kernels (present when every system has at most
-    // 65536 rows and n_slots < 2^31): 16-bit column indices local to the system,
-    // 32-bit slice offsets, the first global row of every slice
+    // 65536 rows and n_slots < 2^31): 16-bit column indices local to the
+    // system, 32-bit slice offsets
     uint16_t* d_col16 = nullptr;
     int32_t* d_slice_off32 = nullptr;
-    int32_t* d_slice_row0 = nullptr;
     int64_t plan_id = 0;              // changes when the systems change
 };
 

@@ -61,11 +61,11 @@ cmcg_status ensure_sell(cmcg_pattern p) {
     for (int64_t s = 0; s < n_sys; ++s) max_rows = std::max(max_rows, ro[s + 1] - ro[s]);
     const bool compact = max_rows <= 65536 && slots < INT32_MAX;
     std::vector<uint16_t> col16(compact ? static_cast<size_t>(slots) : 0);
-    std::vector<int32_t> off32(compact ? off.size() : 0), row0(compact ? width.size() : 0);
+    std::vector<int32_t> off32(compact ? off.size() : 0), row0(width.size());
     size_t sl = 0;
     for (int64_t s = 0; s < n_sys; ++s) {
         for (int64_t r = ro[s]; r < ro[s + 1]; r += 32, ++sl) {
-            if (compact) row0[sl] = static_cast<int32_t>(r);
+            row0[sl] = static_cast<int32_t>(r);
             const int64_t e = std::min<int64_t>(r + 32, ro[s + 1]);
             const int32_t w = width[sl];
             for (int64_t q = r; q < r + 32; ++q) {
@@ -95,15 +95,15 @@ cmcg_status ensure_sell(cmcg_pattern p) {
         (st = up(reinterpret_cast<void**>(&S.d_perm), perm.data(), perm.size() * 4)) != CMCG_OK ||
         (st = up(reinterpret_cast<void**>(&S.d_slice_off), off.data(), off.size() * 8)) != CMCG_OK ||
         (st = up(reinterpret_cast<void**>(&S.d_slice_w), width.data(), width.size() * 4)) != CMCG_OK ||
-        (st = up(reinterpret_cast<void**>(&S.d_sys_slice0), sys0.data(), sys0.size() * 4)) != CMCG_OK) {
+        (st = up(reinterpret_cast<void**>(&S.d_sys_slice0), sys0.data(), sys0.size() * 4)) != CMCG_OK ||
+        (st = up(reinterpret_cast<void**>(&S.d_slice_row0), row0.data(), row0.size() * 4)) != CMCG_OK) {
         free_sell(S);
         return st;
     }
     if (compact) {
         for (size_t i = 0; i < off.size(); ++i) off32[i] = static_cast<int32_t>(off[i]);
         if ((st = up(reinterpret_cast<void**>(&S.d_col16), col16.data(), col16.size() * 2)) != CMCG_OK ||
-            (st = up(reinterpret_cast<void**>(&S.d_slice_off32), off32.data(), off32.size() * 4)) != CMCG_OK ||
-            (st = up(reinterpret_cast<void**>(&S.d_slice_row0), row0.data(), row0.size() * 4)) != CMCG_OK) {
+            (st = up(reinterpret_cast<void**>(&S.d_slice_off32), off32.data(), off32.size() * 4)) != CMCG_OK) {
             free_sell(S);
             return st;
         }

@@ -400,6 +400,85 @@ def test_refined_grid_path_single_system(cuda):
     assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-8
 
 
+def test_grid_reliable_updates_packed_vs_oracle(cuda):
+    # the grid path's reliable-update solver on packed systems: same method as
+    # the persistent kernel, whole-GPU reductions per system
+    m = cm()
+    bt = P.fv2d_batch(10, 16, 96, 0.5, 21)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A = m.SparseMatrix(p, dtype=torch.float32).setData(bt.val)
+    A64 = m.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
+    cg = m.ConjugateGradient(A).set_path(2)
+    b64 = bt.b.astype(np.float64)
+    x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=A64, outer_tol=1e-10, max_outer=200).cpu().numpy()
+    st = cg.system_stats()
+    assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-10)
+    _, it_o, up_o, _ = O.reliable_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, b64, 1e-10)
+    assert abs(int(st["iterations"].sum()) - int(it_o.sum())) <= 0.05 * it_o.sum()
+    assert np.all(np.abs(st["iterations"] - it_o) <= np.maximum(5, 0.15 * it_o))
+    assert np.all(np.abs(st["outer"] - up_o) <= 3)
+    r = b64 - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x)[0]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b64[r0:r1]) < 1e-10
+    # the persistent kernel on the same batch agrees to the solution tolerance
+    xp = m.ConjugateGradient(A).set_path(1).solve_refined(torch.from_numpy(b64).to(cuda), outer=A64,
+                                                          outer_tol=1e-10, max_outer=200).cpu().numpy()
+    assert np.linalg.norm(x - xp) / np.linalg.norm(xp) < 1e-8
+
+
+@pytest.mark.parametrize("inner", [torch.float32, torch.bfloat16])
+def test_grid_reliable_updates_3d_vs_eigen(cuda, inner):
+    m = cm()
+    p3 = P.fv3d(12, 1.0, 3)
+    p = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    Ai = m.SparseMatrix(p, dtype=inner).setData(p3.val)
+    Ao = m.SparseMatrix(p, dtype=torch.float64).setData(p3.val.astype(np.float64))
+    cg = m.ConjugateGradient(Ai).set_path(2)
+    b64 = p3.b.astype(np.float64)
+    x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=Ao, outer_tol=1e-10, max_outer=100).cpu().numpy()
+    st = cg.system_stats()
+    assert st["status"][0] == 0 and st["error"][0] < 1e-10
+    xt = EIG["fv3d12_llt_x"]
+    assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-8
+    # FP32 inner: close to plain FP64 CG's iteration count
+    if inner == torch.float32:
+        assert cg.iterations() <= 1.15 * int(EIG["fv3d12_f64_iters_1e-10"])
+
+
+def test_grid_refinement_limits_and_restart(cuda):
+    m = cm()
+    p3 = P.fv3d(12, 1.0, 3)
+    p = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    Ai = m.SparseMatrix(p, dtype=torch.float32).setData(p3.val)
+    Ao = m.SparseMatrix(p, dtype=torch.float64).setData(p3.val.astype(np.float64))
+    b64 = torch.from_numpy(p3.b.astype(np.float64)).to(cuda)
+    xt = EIG["fv3d12_llt_x"]
+    # too few residual replacements: MAX_ITER with the folded solution and
+    # its true residual reported
+    cg = m.ConjugateGradient(Ai).set_path(2)
+    x = cg.solve_refined(b64, outer=Ao, outer_tol=1e-10, max_outer=2).cpu().numpy()
+    st = cg.system_stats()
+    assert st["status"][0] == 1 and st["outer"][0] == 2
+    r = p3.b.astype(np.float64) - O.spmv_csr_f32_in_f64(p3.n, p3.n, p3.row_ptr, p3.col, p3.val, x)[0]
+    assert np.isclose(st["error"][0], np.linalg.norm(r) / np.linalg.norm(p3.b.astype(np.float64)), rtol=1e-6)
+    # iteration cap: stops with MAX_ITER after exactly that many inner steps
+    cg2 = m.ConjugateGradient(Ai).set_path(2).setMaxIterations(7)
+    cg2.solve_refined(b64, outer=Ao, outer_tol=1e-10, max_outer=100)
+    st2 = cg2.system_stats()
+    assert st2["status"][0] == 1 and st2["iterations"][0] == 7 and np.isfinite(st2["error"][0])
+    # zero rhs: x = 0
+    cg3 = m.ConjugateGradient(Ai).set_path(2)
+    x3 = cg3.solve_refined(torch.zeros_like(b64), outer=Ao, outer_tol=1e-10)
+    assert cg3.system_stats()["status"][0] == 2 and float(x3.abs().max()) == 0.0
+    # restart refinement (host-driven inner solves) still available
+    cg4 = m.ConjugateGradient(Ai).setTolerance(1e-4).set_path(2).set_refinement(1)
+    x4 = cg4.solve_refined(b64, outer=Ao, outer_tol=1e-10).cpu().numpy()
+    assert cg4.system_stats()["status"][0] == 0
+    assert np.linalg.norm(x4 - xt) / np.linalg.norm(xt) < 1e-8
+
+
 def test_plain_fp64_cg_matches_eigen_3d(cuda):
     m = cm()
     p3 = P.fv3d(12, 1.0, 3)
