@@ -38,6 +38,10 @@ SIGNATURES = {
     "cmcg_ctx_synchronize": (_i32, [_vp]),
     "cmcg_ctx_stream": (_i32, [_vp, C.POINTER(_vp)]),
     "cmcg_ctx_device_errors": (_i32, [_vp, _pi32]),
+    "cmcg_device_alloc": (_i32, [_vp, _i64, C.POINTER(_vp)]),
+    "cmcg_device_free": (_i32, [_vp, _vp]),
+    "cmcg_memcpy": (_i32, [_vp, _vp, _vp, _i64, _i32]),
+    "cmcg_memset_zero": (_i32, [_vp, _vp, _i64]),
     "cmcg_pattern_create_csr": (_i32, [_vp, _i32, _i32, _i64, _vp, _vp, _i32, C.POINTER(_vp)]),
     "cmcg_pattern_create_ell": (_i32, [_vp, _i32, _i32, _i32, _vp, _i32, C.POINTER(_vp)]),
     "cmcg_pattern_set_systems": (_i32, [_vp, _i64, _vp]),
@@ -81,7 +85,7 @@ class CuMatError(RuntimeError):
 
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cumat_b200.build` "
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python cumat_b200/build.py` "
                           "(the library has no CPU fallback)")
     lib = C.CDLL(str(LIB_PATH))
     for name, (res, args) in SIGNATURES.items():

@@ -247,6 +247,48 @@ cmcg_status cmcg_ctx_stream(cmcg_ctx ctx, void** stream) {
     return CMCG_OK;
 }
 
+// ---- device memory for callers without a CUDA runtime of their own ---------------
+
+cmcg_status cmcg_device_alloc(cmcg_ctx ctx, int64_t bytes, void** out) {
+    CMCG_REQUIRE(ctx && out, "cmcg_device_alloc: NULL argument");
+    CMCG_REQUIRE(bytes >= 0, "cmcg_device_alloc: negative size");
+    *out = nullptr;
+    CMCG_CUDA(cudaSetDevice(ctx->device));
+    return dev_alloc(out, static_cast<size_t>(bytes));
+}
+
+cmcg_status cmcg_device_free(cmcg_ctx ctx, void* p) {
+    CMCG_REQUIRE(ctx, "cmcg_device_free: NULL context");
+    if (!p) return CMCG_OK;
+    CMCG_CUDA(cudaSetDevice(ctx->device));
+    // work queued on the context may still read the buffer
+    CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
+    CMCG_CUDA(cudaFree(p));
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_memcpy(cmcg_ctx ctx, void* dst, const void* src, int64_t bytes, int32_t kind) {
+    CMCG_REQUIRE(ctx && (bytes == 0 || (dst && src)), "cmcg_memcpy: NULL argument");
+    CMCG_REQUIRE(bytes >= 0, "cmcg_memcpy: negative size");
+    CMCG_REQUIRE(kind == CMCG_HOST_TO_DEVICE || kind == CMCG_DEVICE_TO_HOST || kind == CMCG_DEVICE_TO_DEVICE,
+                 "cmcg_memcpy: bad kind");
+    if (bytes == 0) return CMCG_OK;
+    const cudaMemcpyKind k = kind == CMCG_HOST_TO_DEVICE   ? cudaMemcpyHostToDevice
+                             : kind == CMCG_DEVICE_TO_HOST ? cudaMemcpyDeviceToHost
+                                                           : cudaMemcpyDeviceToDevice;
+    CMCG_CUDA(cudaMemcpyAsync(dst, src, static_cast<size_t>(bytes), k, ctx->stream));
+    // host buffers are the caller's again when the call returns
+    if (kind != CMCG_DEVICE_TO_DEVICE) CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_memset_zero(cmcg_ctx ctx, void* dst, int64_t bytes) {
+    CMCG_REQUIRE(ctx && (bytes == 0 || dst), "cmcg_memset_zero: NULL argument");
+    CMCG_REQUIRE(bytes >= 0, "cmcg_memset_zero: negative size");
+    if (bytes) CMCG_CUDA(cudaMemsetAsync(dst, 0, static_cast<size_t>(bytes), ctx->stream));
+    return CMCG_OK;
+}
+
 // ---- patterns -----------------------------------------------------------------
 
 static cmcg_status upload_default_systems(cmcg_pattern p) {

@@ -98,6 +98,18 @@ int64_t cmcg_launch_count(void);
 cmcg_status cmcg_ctx_create(int32_t device, void* stream, cmcg_ctx* out);
 cmcg_status cmcg_ctx_destroy(cmcg_ctx ctx);
 cmcg_status cmcg_ctx_synchronize(cmcg_ctx ctx);
+
+/* Device memory for callers that do not link a CUDA runtime themselves (the
+ * C++ facade's dense vectors). Reference: Context::mallocDevice / freeDevice
+ * (cuMat/src/Context.h:271-286) and Matrix::copyFromHost / copyToHost
+ * (cuMat/src/Matrix.h:847-858). cmcg_device_free waits for the context's
+ * queued work; cmcg_memcpy returns after host<->device copies completed and
+ * queues device-to-device copies on the context stream. */
+enum { CMCG_HOST_TO_DEVICE = 0, CMCG_DEVICE_TO_HOST = 1, CMCG_DEVICE_TO_DEVICE = 2 };
+cmcg_status cmcg_device_alloc(cmcg_ctx ctx, int64_t bytes, void** out);
+cmcg_status cmcg_device_free(cmcg_ctx ctx, void* p);
+cmcg_status cmcg_memcpy(cmcg_ctx ctx, void* dst, const void* src, int64_t bytes, int32_t kind);
+cmcg_status cmcg_memset_zero(cmcg_ctx ctx, void* dst, int64_t bytes);
 cmcg_status cmcg_ctx_stream(cmcg_ctx ctx, void** stream);
 /* Synchronises and returns (then clears) the context's device error bits: a
  * bounded wait inside a kernel that ran out sets bit 0 (no reference

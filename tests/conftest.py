@@ -16,8 +16,13 @@ def pytest_configure(config):
 @pytest.fixture(scope="session", autouse=True)
 def _built_libraries():
     """Builds the generators and the oracle when missing (CPU only, seconds);
-    the CUDA library is built by __graft_entry__.build() / cumat_b200.build."""
-    from cumat_b200 import build
+    the CUDA library is built by __graft_entry__.build() / cumat_b200/build.py.
+    The build script is loaded by path, so that this works before the CUDA
+    library (which the package loads on import) exists."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_cumat_build", ROOT / "cumat_b200" / "build.py")
+    build = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(build)
     build.build_problems()
     if not (ROOT / "oracle" / "liboracle.so").exists():
         build.build_oracle()
