@@ -2014,11 +2014,16 @@ cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
     return CMCG_OK;
 }
 
-int32_t choose_path(cmcg_solver s, int32_t n_inst) {
+// smem_ok: a shared-memory-resident persistent kernel exists for the solve
+int32_t choose_path(cmcg_solver s, int32_t n_inst, bool smem_ok) {
     if (s->path != CMCG_PATH_AUTO) return s->path;
     const int sms = s->A->pat->ctx->sm_count;
     // many independent systems of moderate size: one CTA per system
     if (s->max_sys_rows <= 65536 && n_inst >= sms) return CMCG_PATH_PERSISTENT;
+    // a few systems that fit in shared memory: one CTA each still beats the
+    // grid path's per-iteration launches (2D Poisson 100^2, one system:
+    // 9.5 us vs 18.7 us per iteration on the B200)
+    if (smem_ok && s->max_sys_rows <= kSmemMaxRows) return CMCG_PATH_PERSISTENT;
     return CMCG_PATH_GRID;
 }
 
@@ -2252,9 +2257,10 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
     CMCG_TRY(ensure_state(s, n_inst));
     const void* dinv = nullptr;
     CMCG_TRY(get_dinv(s, DT<VT>::id, &dinv));
-    const int32_t path = choose_path(s, n_inst);
-    const size_t vbytes = sizeof(VT) * static_cast<size_t>(p->rows) * ob;
     CMCG_TRY(ensure_sell_values(s->A));
+    const bool smem_ok = (FMT == CMCG_CSR && compact_ok(s)) || (sizeof(VT) == 4 && s->use_smem);
+    const int32_t path = choose_path(s, n_inst, smem_ok);
+    const size_t vbytes = sizeof(VT) * static_cast<size_t>(p->rows) * ob;
     SolveArgs<VT, MT> a = base_args<VT, MT>(s, ob);
     a.dinv = static_cast<const VT*>(dinv);
     a.dinv_b = s->A->batches;
@@ -2806,7 +2812,7 @@ cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b
     CMCG_TRY(refresh_plan(s));
     const int32_t ob = std::max(s->A->batches, b_batches);
     const int fmt = s->A->pat->format;
-    int32_t path = choose_path(s, ob * s->n_sys);
+    int32_t path = choose_path(s, ob * s->n_sys, s->use_smem && s->refine_method == CMCG_REFINE_RELIABLE);
     // the grid path's reliable-update solver needs the sliced layout (CSR)
     const bool grid_mixed = fmt == CMCG_CSR && s->refine_method == CMCG_REFINE_RELIABLE;
     // packed systems run persistent (one CTA per system, vectors in shared

@@ -32,9 +32,10 @@ namespace {
 
 constexpr int kSpmvThreads = 256;
 
-// Stand-alone product kernels: 0 = bulk-staged CSR / four-rows-per-thread
-// ELLPACK (default), 1 = warp row-block CSR / thread-per-row ELLPACK. Chosen
-// once per process from CUMAT_SPMV_VARIANT (a tuning and comparison knob).
+// Stand-alone product kernels: 0 = row-unrolled CSR / four-rows-per-thread
+// ELLPACK (default), 1 = warp row-block CSR / thread-per-row ELLPACK,
+// 2 = bulk-staged CSR / four-rows-per-thread ELLPACK. Chosen once per process
+// from CUMAT_SPMV_VARIANT (a tuning and comparison knob).
 int spmv_variant() {
     static const int v = [] {
         const char* e = std::getenv("CUMAT_SPMV_VARIANT");
@@ -87,6 +88,49 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell(const int32_t* __rest
     }
 }
 
+// ---- CSR, thread per row, unrolled ------------------------------------------------
+//
+// The reference's thread-per-row loop (SparseProductEvaluation.h:55-87) with
+// the loads taken out of the dependency chain: a thread loads up to
+// kCsrUnroll column indices and values of its row (predicated on the row end)
+// before the first gather, so each thread keeps 2 * kCsrUnroll independent
+// loads and then kCsrUnroll gathers in flight. The scattered 4-byte loads of
+// neighbouring rows fall into the same cache lines, which L1 merges. Sums are
+// in entry order with fused multiply-adds, like the reference.
+
+constexpr int kCsrUnroll = 8;
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_rows(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                                const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                                const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                                VT* __restrict__ y, int32_t rows, int32_t ob) {
+    const int64_t items = static_cast<int64_t>(rows) * ob;
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * kSpmvThreads) {
+        const int b = static_cast<int>(it / rows);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * rows);
+        const MT* v = vals + (mb == 1 ? 0 : b * vstride);
+        const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        const int e = __ldg(rp + r + 1);
+        VT acc = VT(0);
+        for (int k = __ldg(rp + r); k < e; k += kCsrUnroll) {
+            int c[kCsrUnroll];
+            MT w[kCsrUnroll];
+#pragma unroll
+            for (int u = 0; u < kCsrUnroll; ++u) {
+                const bool in = k + u < e;
+                c[u] = in ? __ldg(ci + k + u) : -1;
+                w[u] = in ? v[k + u] : MT{};
+            }
+#pragma unroll
+            for (int u = 0; u < kCsrUnroll; ++u)
+                if (c[u] >= 0) acc += mval<VT>(w[u]) * __ldg(xv + c[u]);
+        }
+        assign_out<MODE>(y + it, acc);
+    }
+}
+
 // ---- bulk-staged CSR product ----------------------------------------------------
 //
 // Persistent CTAs walk precomputed row tiles (<= kTileRows rows, <= kTileNnz
@@ -96,7 +140,8 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell(const int32_t* __rest
 // flight per CTA. Threads then take rows (thread per row), read their entries
 // from shared memory, gather x through the read-only path and write y. A tile
 // that is one row longer than kTileNnz is summed by the whole CTA from global
-// memory.
+// memory. (Kept as a selectable variant: with two stages the copies stall
+// behind the gathers, so the row-unrolled kernel below is the default.)
 
 constexpr int kTileRows = 512;
 constexpr int kTileNnz = 2048;
@@ -165,7 +210,8 @@ __global__ void __launch_bounds__(kTmaThreads) k_spmv_csr_tma(const int32_t* __r
     int j = 0;
     for (int64_t it = blockIdx.x; it < items; it += G, ++j) {
         const int s = j & 1;
-        const bool ok = mbar_wait(&bar[s], (j >> 1) & 1, err);
+        // uniform over the CTA: the compute below has barriers
+        const bool ok = __syncthreads_and(mbar_wait(&bar[s], (j >> 1) & 1, err)) != 0;
         const int b = static_cast<int>(it / ntiles);
         const int t = static_cast<int>(it - static_cast<int64_t>(b) * ntiles);
         const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
@@ -233,7 +279,19 @@ template <> struct Vec4Load<__nv_bfloat16> {
     }
 };
 
-template <typename MT, typename VT, int MODE>
+// one slot of four rows: padding (index < 0) contributes nothing
+template <typename MT, typename VT>
+__device__ __forceinline__ void ell4_slot(const int4 c, const MT (&w)[4], const VT* __restrict__ xv, VT (&acc)[4]) {
+    if (c.x >= 0) acc[0] += mval<VT>(w[0]) * __ldg(xv + c.x);
+    if (c.y >= 0) acc[1] += mval<VT>(w[1]) * __ldg(xv + c.y);
+    if (c.z >= 0) acc[2] += mval<VT>(w[2]) * __ldg(xv + c.z);
+    if (c.w >= 0) acc[3] += mval<VT>(w[3]) * __ldg(xv + c.w);
+}
+
+// W > 0: the width is a compile-time constant and every slot's index and value
+// vectors are loaded before the first gather (2 W independent 16-byte loads in
+// flight per thread); W == 0: any width, slot by slot
+template <typename MT, typename VT, int MODE, int W>
 __global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell4(const int32_t* __restrict__ idx, int32_t width, int32_t rows_pad,
                                                             const MT* __restrict__ vals, int64_t vstride, int32_t mb,
                                                             const VT* __restrict__ x, int32_t cols, int32_t xb,
@@ -247,15 +305,25 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell4(const int32_t* __res
         const MT* v = vals + (mb == 1 ? 0 : b * vstride);
         const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
         VT acc[4] = {VT(0), VT(0), VT(0), VT(0)};
-        for (int j = 0; j < width; ++j) {
-            const int64_t o = r + static_cast<int64_t>(j) * rows_pad;
-            const int4 c = __ldg(reinterpret_cast<const int4*>(idx + o));
-            MT w[4];
-            Vec4Load<MT>::load(v + o, w);
-            if (c.x >= 0) acc[0] += mval<VT>(w[0]) * __ldg(xv + c.x);
-            if (c.y >= 0) acc[1] += mval<VT>(w[1]) * __ldg(xv + c.y);
-            if (c.z >= 0) acc[2] += mval<VT>(w[2]) * __ldg(xv + c.z);
-            if (c.w >= 0) acc[3] += mval<VT>(w[3]) * __ldg(xv + c.w);
+        if constexpr (W > 0) {
+            int4 c[W];
+            MT w[W][4];
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                const int64_t o = r + static_cast<int64_t>(j) * rows_pad;
+                c[j] = __ldg(reinterpret_cast<const int4*>(idx + o));
+                Vec4Load<MT>::load(v + o, w[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < W; ++j) ell4_slot<MT, VT>(c[j], w[j], xv, acc);
+        } else {
+            for (int j = 0; j < width; ++j) {
+                const int64_t o = r + static_cast<int64_t>(j) * rows_pad;
+                const int4 c = __ldg(reinterpret_cast<const int4*>(idx + o));
+                MT w[4];
+                Vec4Load<MT>::load(v + o, w);
+                ell4_slot<MT, VT>(c, w, xv, acc);
+            }
         }
         VT* yv = y + static_cast<int64_t>(b) * rows + r;
 #pragma unroll
@@ -308,6 +376,37 @@ cmcg_status launch_csr_tma(cmcg_matrix A, const VT* xv, int32_t xb, VT* yv, int3
     return CMCG_OK;
 }
 
+// ELLPACK widths 1..8 get the width-specialised kernel; the grid is at most one
+// wave of resident CTAs (grid-stride loop over the row quads)
+template <typename K>
+int resident_grid(K kern, int needed, int sm_count) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSpmvThreads, 0) != cudaSuccess || occ < 1) occ = 1;
+    return std::max(1, std::min(needed, sm_count * occ));
+}
+
+template <typename MT, typename VT, int MODE>
+void launch_ell4(cmcg_matrix A, int blocks, const MT* vals, const VT* xv, int32_t xb, VT* yv, int32_t ob) {
+    cmcg_pattern p = A->pat;
+    cudaStream_t st = p->ctx->stream;
+    const int sms = p->ctx->sm_count;
+#define CMCG_ELL4_W(W)                                                                                            \
+    k_spmv_ell4<MT, VT, MODE, W><<<resident_grid(k_spmv_ell4<MT, VT, MODE, W>, blocks, sms), kSpmvThreads, 0, st>>>( \
+        p->d_ell, p->width, p->rows_pad, vals, A->stride, A->batches, xv, p->cols, xb, yv, p->rows, ob)
+    switch (p->width) {
+        case 1: CMCG_ELL4_W(1); break;
+        case 2: CMCG_ELL4_W(2); break;
+        case 3: CMCG_ELL4_W(3); break;
+        case 4: CMCG_ELL4_W(4); break;
+        case 5: CMCG_ELL4_W(5); break;
+        case 6: CMCG_ELL4_W(6); break;
+        case 7: CMCG_ELL4_W(7); break;
+        case 8: CMCG_ELL4_W(8); break;
+        default: CMCG_ELL4_W(0);
+    }
+#undef CMCG_ELL4_W
+}
+
 template <typename MT, typename VT>
 cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode) {
     cmcg_pattern p = A->pat;
@@ -318,22 +417,32 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     VT* yv = static_cast<VT*>(y);
     const int max_blocks = ctx->sm_count * 8;
     const int variant = spmv_variant();
-    if (p->format == CMCG_CSR && variant != 1) {
+    if (p->format == CMCG_CSR && variant == 2) {
         if (mode == CMCG_ASSIGN) return launch_csr_tma<MT, VT, CMCG_ASSIGN>(A, xv, xb, yv, ob);
         if (mode == CMCG_ADD) return launch_csr_tma<MT, VT, CMCG_ADD>(A, xv, xb, yv, ob);
         return launch_csr_tma<MT, VT, CMCG_SUB>(A, xv, xb, yv, ob);
     }
+    if (p->format == CMCG_CSR && variant == 0) {
+        const int64_t threads = static_cast<int64_t>(p->rows) * ob;
+        const int needed = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
+#define CMCG_LAUNCH_CSR_ROWS(M)                                                                                  \
+    k_spmv_csr_rows<MT, VT, M><<<resident_grid(k_spmv_csr_rows<MT, VT, M>, needed, ctx->sm_count), kSpmvThreads, 0, \
+                                 ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride, A->batches, xv, p->cols, xb, \
+                                                yv, p->rows, ob)
+        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR_ROWS(CMCG_ASSIGN);
+        else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR_ROWS(CMCG_ADD);
+        else CMCG_LAUNCH_CSR_ROWS(CMCG_SUB);
+#undef CMCG_LAUNCH_CSR_ROWS
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        return CMCG_OK;
+    }
     if (p->format == CMCG_ELLPACK && variant != 1) {
         const int64_t threads = static_cast<int64_t>(p->rows_pad / 4) * ob;
         const int blocks = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
-#define CMCG_LAUNCH_ELL4(M)                                                                                      \
-    k_spmv_ell4<MT, VT, M><<<blocks, kSpmvThreads, 0, ctx->stream>>>(p->d_ell, p->width, p->rows_pad, vals,       \
-                                                                     A->stride, A->batches, xv, p->cols, xb, yv,  \
-                                                                     p->rows, ob)
-        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_ELL4(CMCG_ASSIGN);
-        else if (mode == CMCG_ADD) CMCG_LAUNCH_ELL4(CMCG_ADD);
-        else CMCG_LAUNCH_ELL4(CMCG_SUB);
-#undef CMCG_LAUNCH_ELL4
+        if (mode == CMCG_ASSIGN) launch_ell4<MT, VT, CMCG_ASSIGN>(A, blocks, vals, xv, xb, yv, ob);
+        else if (mode == CMCG_ADD) launch_ell4<MT, VT, CMCG_ADD>(A, blocks, vals, xv, xb, yv, ob);
+        else launch_ell4<MT, VT, CMCG_SUB>(A, blocks, vals, xv, xb, yv, ob);
         count_launch();
         CMCG_CHECK_LAUNCH();
         return CMCG_OK;
