@@ -4,14 +4,17 @@
 Workload (one "step"): the batching configuration's 4096 independent 2D
 variable-coefficient diffusion systems (5-point finite volume, kappa = exp(g),
 g ~ N(0, 0.5^2), sides ~ U{16..128}, seed 2, FP32 CSR packed into one buffer)
-solved to a relative residual of 1e-10 by the mixed-precision solver: FP32
-Jacobi-CG inner solves to 1e-4 with FP64 residual / update / norms, one
-persistent launch for the whole batch. Metric: solves/s. The same line also
-carries plain FP64 batched CG on the same batch (the comparison named by the
-metric), SpMV GB/s on the 1024^2 Poisson matrix (CSR and ELLPACK), the HBM
-roofline of the dominant kernel, the CPU baseline (the reference's bundled
-Eigen FP64 Jacobi-CG, all host threads, a bounded sample) and the end-to-end
-number through the public API with host buffers.
+solved to a relative residual of 1e-10 by the mixed-precision solver: FP32 CG
+on the Jacobi-scaled systems whose residual is replaced by the FP64 residual
+b - A x whenever it has dropped by 0.1 (reliable updates), FP64 solution and
+norms, one persistent launch for the whole batch. Metric: solves/s. The same
+line also carries plain FP64 batched CG on the same batch (the comparison named
+by the metric), SpMV GB/s on the 1024^2 Poisson matrix (CSR and ELLPACK), the
+reference's own benchmark shapes (SpMV on 2D Poisson grids 10..10000, CG on
+grids 10..1000) beside its published times, the HBM roofline of the dominant
+kernel, the CPU baseline (the reference's bundled Eigen FP64 Jacobi-CG, all
+host threads) and the end-to-end number through the public API with host
+buffers.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 N > 1: launch with torch.distributed.run; every rank solves its own batch
@@ -235,6 +238,113 @@ def spmv_gbs(cm, torch, dev, stream):
     return out
 
 
+# The reference's own published benchmarks (ms per call, RTX 2070, from
+# benchmarks/CSRMV - 2D-Poisson Matrix.json and benchmarks/Conjugate Gradient -
+# 2D-Poisson Matrix.json; see docs/03_Benchmarks.dox)
+REF_CSRMV_MS = {10: (0.0178, 0.0136), 100: (0.0160, 0.0151), 1000: (0.1635, 0.1444), 10000: (17.69, 19.62)}
+REF_CG_MS = {10: 6.67, 20: 11.47, 50: 28.58, 100: 48.60, 200: 74.14, 500: 201.58, 1000: 599.84}
+
+
+def _boundary_rhs(g: int) -> np.ndarray:
+    """Right-hand side of the reference's CG benchmark
+    (benchmarks/conjugate_gradient/Implementation_cuMat.cu): zero inside,
+    rand()/RAND_MAX on the boundary cells after srand(42), in the order
+    x-major then y, cell index y + x * g. The C library's own rand() is called."""
+    import ctypes
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(42)
+    rand_max = 2147483647.0
+    b = np.zeros(g * g, np.float32)
+    for x in range(g):
+        for y in range(g):
+            if x == 0 or y == 0 or x == g - 1 or y == g - 1:
+                b[y + x * g] = np.float32(libc.rand()) / np.float32(rand_max)
+    return b
+
+
+def reference_suite(cm, torch, dev, stream, hbm_peak):
+    """The reference's own benchmark shapes, timed here like the reference times
+    them: CSR / ELLPACK SpMV on the 2D Poisson matrix (grids 10..10000), repeated
+    calls on one matrix and vector, ms per call; CG on the 2D Poisson matrix
+    (grids 10..1000, default Jacobi preconditioner, tolerance 1e-4), solver
+    construction + solve, ms per call (wall clock around a device sync)."""
+    from cumat_b200 import problems as P
+
+    def ev_ms(fn, reps, warm=3):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    out = {"source": "reference ms per call on an RTX 2070 (benchmarks/*.json); ours on this B200",
+           "spmv": [], "cg": []}
+    for g in (10, 100, 1000, 10000):
+        pr = P.poisson2d(g, 1)
+        n, nnz = pr.n, pr.nnz
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(n, n, pr.row_ptr, pr.col)).setData(pr.val)
+        idx, ev = P.csr_to_ell(n, pr.row_ptr, pr.col, pr.val)
+        E = cm.SparseMatrix(cm.SparsityPattern.ell(n, n, idx)).setData(ev)
+        del idx, ev
+        x = torch.from_numpy(pr.b).to(dev)
+        y = torch.empty_like(x)
+        reps = 2000 if n < 10 ** 6 else (200 if n < 10 ** 7 else 20)
+        tc = ev_ms(lambda: A.product(x, out=y), reps)
+        te = ev_ms(lambda: E.product(x, out=y), reps)
+        csr_b = nnz * 8 + (n + 1) * 4 + 2 * n * 4
+        ell_b = n * 5 * 8 + 2 * n * 4
+        rc, re = REF_CSRMV_MS[g]
+        out["spmv"].append({"grid": g, "rows": n, "csr_ms": round(tc, 5), "ell_ms": round(te, 5),
+                            "csr_gbs": round(csr_b / tc / 1e6, 1), "ell_gbs": round(ell_b / te / 1e6, 1),
+                            "csr_frac": round(csr_b / tc / 1e6 / hbm_peak, 3),
+                            "ell_frac": round(ell_b / te / 1e6 / hbm_peak, 3),
+                            "ref_csr_ms": rc, "ref_ell_ms": re,
+                            "speedup_csr": round(rc / tc, 1), "speedup_ell": round(re / te, 1)})
+        del A, E, x, y, pr
+        torch.cuda.empty_cache()
+    for g in sorted(REF_CG_MS):
+        pr = P.poisson2d(g, 0)
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+        b = torch.from_numpy(_boundary_rhs(g)).to(dev)
+        x = torch.empty_like(b)
+        its = []
+
+        def run():
+            cg = cm.ConjugateGradient(A).setTolerance(1e-4)
+            cg.solve(b, out=x)
+            its.append(cg.iterations())
+        run()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            run()
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+        ms = statistics.mean(times)
+        out["cg"].append({"grid": g, "ms": round(ms, 4), "iterations": int(its[-1]), "ref_ms": REF_CG_MS[g],
+                          "speedup": round(REF_CG_MS[g] / ms, 1)})
+    return out
+
+
+def traffic_per_alg_byte():
+    """DRAM bytes per algorithmic byte of the headline kernel, from the committed
+    ncu summary of its small-case capture (None when the summary is absent)."""
+    p = ROOT / "profiles" / "k_mixed_fast_fv2d512.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_alg_byte:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 def cpu_baseline(bt, budget_s=15.0):
     """Eigen FP64 Jacobi-CG to 1e-10 (the reference's bundled CPU path) on the
     first m systems of the batch (sides are drawn i.i.d., so a prefix is a
@@ -288,6 +398,7 @@ def run_ours(args):
     # roofline of the dominant (only) kernel: the persistent refined launch
     alg = refined_bytes(bt, st["iterations"].astype(np.float64), st["outer"].astype(np.float64))
     achieved = alg / (ms / 1e3) / 1e9
+    traffic_ratio = traffic_per_alg_byte()
 
     # plain FP64 batched CG on the same batch (FP64 values and vectors)
     A64 = cm.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
@@ -317,6 +428,8 @@ def run_ours(args):
         extra["spmv_poisson1024"] = spmv_gbs(cm, torch, dev, stream)
         for k in ("csr", "ell"):
             extra["spmv_poisson1024"][k]["frac"] = round(extra["spmv_poisson1024"][k]["gbs"] / hbm_peak, 3)
+    if rank == 0 and world == 1 and not args.no_suite:
+        extra["reference_suite"] = reference_suite(cm, torch, dev, stream, hbm_peak)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(bt, args.cpu_budget)
@@ -327,14 +440,19 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded finite-volume systems)",
             "config": {"workload": "4096 uneven 2D FV diffusion systems (sides 16..128, kappa=exp(N(0,0.25))), "
-                                   "Jacobi-CG FP32 inner to 1e-4 + FP64 refinement to 1e-10",
+                                   "Jacobi-scaled FP32 CG with FP64 residual replacement to 1e-10",
                        "systems_per_gpu": N_SYS, "rows_per_gpu": int(bt.n), "nnz_per_gpu": int(bt.nnz),
                        "parallelism": f"batch sharding x{world}, no collective",
                        "l2": "inputs larger than L2 (FP32 CSR batch %.2f GB)" % ((bt.nnz * 8 + bt.n * 4) / 1e9)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved / hbm_peak, 3), "traffic": None,
-                         "kernel": "k_persistent_refined", "peak_source": peak_src,
-                         "alg_bytes_per_launch": alg},
+                         "frac": round(achieved / hbm_peak, 3),
+                         "traffic": round(alg * traffic_ratio) if traffic_ratio else None,
+                         "traffic_note": "dram bytes per launch, ncu capture of the first 512 systems scaled by "
+                                         "algorithmic bytes (profiles/k_mixed_fast_fv2d512.md)",
+                         "kernel": "k_mixed_fast", "peak_source": peak_src,
+                         "alg_bytes_per_launch": alg,
+                         "note": "achieved = streaming-model bytes / time; vectors stay on chip and matrices in L2, "
+                                 "so frac > 1 means the kernel avoids the modelled DRAM passes (it is issue-bound)"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(N_SYS * world / (ms_e2e / 1e3), 1), "unit": UNIT,
                     "h2d_bytes_per_step": int(bt.n * 8), "d2h_bytes_per_step": int(bt.n * 8)},
@@ -403,10 +521,11 @@ def run_reference(args):
 
 def run_profile_small():
     """The small case for ncu captures (a few hundred MB on the device): three
-    SpMV calls per format on the 1024^2 Poisson matrix, then one mixed and one
-    FP64 batched solve of the first 512 systems of the batch. Prints the
-    algorithmic bytes of the mixed launch so that its DRAM traffic can be
-    compared per unit with the full batch."""
+    SpMV calls per format on the 1024^2 Poisson matrix, one grid-path Jacobi-CG
+    solve of that matrix capped at 50 iterations (the cooperative one-launch
+    kernel), then one mixed and one FP64 batched solve of the first 512 systems
+    of the batch. Prints the algorithmic bytes of the mixed launch so that its
+    DRAM traffic can be compared per unit with the full batch."""
     import torch
 
     import cumat_b200 as cm
@@ -422,6 +541,8 @@ def run_profile_small():
     for _ in range(3):
         A.product(x, out=y)
         E.product(x, out=y)
+    cgg = cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(50).set_path(2)
+    cgg.solve(x, out=y)
     bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED)
     k = int(bt.row_off[512])
     kz = int(bt.row_ptr[k])
@@ -457,6 +578,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-spmv", action="store_true", help="skip the SpMV GB/s sub-benchmark")
+    ap.add_argument("--no-suite", action="store_true",
+                    help="skip the reference's own benchmark shapes (SpMV grids 10..10000, CG grids 10..1000)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile-small", action="store_true",
                     help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "

@@ -33,6 +33,7 @@
 #include "cg_dev.cuh"
 #include "cg_smem.cuh"
 #include "common.cuh"
+#include "cg_grid.cuh"
 #include "objects.h"
 
 namespace cmcg {
@@ -47,104 +48,6 @@ using namespace cmcg;
 
 namespace {
 
-constexpr int kTile = 256;          // rows per tile of the grid path (= threads per CTA)
-constexpr int kGridCtasPerSm = 4;   // grid path CTAs per SM (segment plan size)
-constexpr int kPersistThreads = 256;
-
-// ---------------------------------------------------------------------------
-// Kernel arguments
-// ---------------------------------------------------------------------------
-
-template <typename MT>
-struct MatArgs {
-    const int32_t* rp;
-    const int32_t* ci;
-    const int32_t* ell;
-    int32_t width, rows_pad;
-    const MT* vals;
-    int64_t vstride;
-    int32_t mb;
-    // sliced ELLPACK copy (CSR patterns)
-    const int32_t* sell_col;
-    const MT* sell_vals;
-    int64_t sell_vstride;
-    const int64_t* slice_off;
-    const int32_t* slice_w;
-    const int32_t* sys_slice0;
-};
-
-template <typename MT, int FMT>
-__device__ __forceinline__ InstMatrix<MT, FMT> inst_matrix(const MatArgs<MT>& m, int b) {
-    InstMatrix<MT, FMT> A;
-    const MT* v = m.vals + (m.mb == 1 ? 0 : static_cast<int64_t>(b) * m.vstride);
-    A.csr = CsrView<MT>{m.rp, m.ci, v};
-    A.ell = EllView<MT>{m.ell, v, m.width, m.rows_pad};
-    if (FMT == CMCG_CSR)
-        A.rm = RowMat<MT>{m.sell_col, m.sell_vals + (m.mb == 1 ? 0 : static_cast<int64_t>(b) * m.sell_vstride),
-                          m.slice_off, m.slice_w, m.sys_slice0, 0, 0};
-    else
-        A.rm = RowMat<MT>{m.ell, v, nullptr, nullptr, nullptr, m.rows_pad, m.width};
-    return A;
-}
-
-// Per-instance state (instance = batch * n_sys + system).
-struct InstState {
-    double* bb;      // |b|^2
-    double* rr;      // |r|^2 (latest)
-    double* rz;      // r.z
-    double* alpha;
-    double* beta;
-    int32_t* it;     // iterations (reference semantics)
-    int32_t* status;
-    int32_t* outer;  // refinement steps
-    double* err;     // sqrt(rr / bb) written by the finaliser
-    unsigned* tk1;
-    unsigned* tk2;
-    double* rmax;    // mixed solver: scaled |r|^2 at the last residual replacement
-    double* goal;    //   scaled |r|^2 that would meet the FP64 target
-    int32_t* flag;   //   1: replace the residual in this iteration
-};
-
-template <typename VT, typename MT>
-struct SolveArgs {
-    MatArgs<MT> m;
-    int32_t rows, n_sys, ob;
-    const int32_t* row_off;
-    const int32_t* order;          // persistent: systems, largest first
-    int32_t* next;                 // persistent: work counter
-    // grid path tiles
-    int32_t n_tiles;
-    const int32_t* tile_row0;
-    int32_t n_seg;
-    const int32_t* seg_t0;       // segment = tiles [seg_t0, seg_t1) of one CTA in one system
-    const int32_t* seg_t1;
-    const int32_t* seg_sys;
-    const int32_t* cta_seg0;     // segments of CTA c: [cta_seg0[c], cta_seg0[c+1])
-    const int32_t* sys_seg0;     // segments of system s: [sys_seg0[s], sys_seg0[s+1])
-    VT* part1;
-    VT* part2;
-    int32_t* active;
-    int32_t* loops;
-    int32_t loop_cap;
-    cudaGraphConditionalHandle cond;
-    // vectors, [batch][rows]
-    const VT* dinv;
-    int32_t dinv_b;
-    const VT* b;
-    int32_t b_b;
-    const VT* guess;
-    int32_t g_b;
-    VT* x;
-    VT* r;
-    VT* p;
-    VT* q;
-    double tol;
-    int64_t max_iter;              // < 0: 2 * rows of the system
-    int32_t abs_zero_test;         // reference early-out |b|^2 < tol^2 (0 for refinement inner solves)
-    InstState st;
-};
-
-__device__ __forceinline__ int64_t sys_max_iter(int64_t mi, int n) { return mi < 0 ? 2 * static_cast<int64_t>(n) : mi; }
 
 // ---------------------------------------------------------------------------
 // One system, one CTA (shared by the persistent plain and refined kernels)
@@ -1200,65 +1103,6 @@ __global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __r
 // Grid path kernels
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ int32_t ld_status(const int32_t* s) { return *reinterpret_cast<const volatile int32_t*>(s); }
-
-// Publishes this tile's NV partial sums and, if it is the last tile of its
-// system instance, returns true with the instance totals (fixed order) in tot.
-template <typename VT, int NV>
-__device__ bool tile_ticket(const VT (&v)[NV], VT* const (&part)[NV], int64_t pbase, int t_begin, int t_count,
-                            int64_t pidx, unsigned* tk, int inst, VT (&tot)[NV], VT* red, bool* last_s) {
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) part[j][pidx] = v[j];
-        __threadfence();
-        const unsigned t = atomicAdd(tk + inst, 1u);
-        *last_s = (t == static_cast<unsigned>(t_count - 1));
-    }
-    __syncthreads();
-    const bool last = *last_s;
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-#pragma unroll
-    for (int j = 0; j < NV; ++j) tot[j] = VT(0);
-    for (int i = threadIdx.x; i < t_count; i += blockDim.x) {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) tot[j] += __ldcg(part[j] + pbase + t_begin + i);
-    }
-    block_sum<VT, NV>(tot, red);
-    if (threadIdx.x == 0) tk[inst] = 0u;
-    return true;
-}
-
-// The grid path's work plan: the tiles are split into gridDim.x contiguous
-// ranges, one per CTA; a "segment" is the part of one CTA's range that lies in
-// one system. Each CTA keeps its running sums in registers over a segment's
-// tiles and publishes one partial per segment; the last segment of a system
-// instance to finish (ticket) adds that system's partials in segment order.
-// A system's segments have consecutive ids, so the closing sum reads at most
-// gridDim.x values.
-struct SegInfo {
-    int s, inst, t0, t1, sr0, send, pidx, pbase, count;
-};
-
-template <typename VT, typename MT>
-__device__ __forceinline__ SegInfo seg_info(const SolveArgs<VT, MT>& a, int b, int seg) {
-    SegInfo g;
-    g.s = a.seg_sys[seg];
-    g.inst = b * a.n_sys + g.s;
-    g.t0 = a.seg_t0[seg];
-    g.t1 = a.seg_t1[seg];
-    g.sr0 = a.row_off[g.s];
-    g.send = a.row_off[g.s + 1];
-    g.pidx = b * a.n_seg + seg;
-    g.pbase = b * a.n_seg + a.sys_seg0[g.s];
-    g.count = a.sys_seg0[g.s + 1] - a.sys_seg0[g.s];
-    return g;
-}
-
-#define CMCG_FOR_SEGMENTS(a)                                                     \
-    for (int b_ = 0; b_ < (a).ob; ++b_)                                          \
-        for (int seg_ = (a).cta_seg0[blockIdx.x]; seg_ < (a).cta_seg0[blockIdx.x + 1]; ++seg_)
 
 // init A: x = guess or 0, r = b - A x, |b|^2, |r|^2 -> status
 template <typename VT, typename MT, int FMT>
@@ -1274,26 +1118,23 @@ __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
         VT acc[2] = {VT(0), VT(0)};
         const auto A = inst_matrix<MT, FMT>(a.m, b_);
         const VT* gv = a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr;
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
-            if (gv) {
-                cta_rows<VT>(A, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<VT>{gv}, [&](int row, VT v) {
-                    const VT bi = bv[row];
-                    const VT ri = bi - v;
-                    r[row] = ri;
-                    x[row] = gv[row];
-                    acc[0] += bi * bi;
-                    acc[1] += ri * ri;
-                });
-            } else {
-                const int i = r0 + threadIdx.x;
-                if (i < r1) {
-                    const VT bi = bv[i];
-                    r[i] = bi;
-                    x[i] = VT(0);
-                    acc[0] += bi * bi;
-                    acc[1] += bi * bi;
-                }
+        if (gv) {
+            cta_rows_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{gv}, [&](int row, VT v) {
+                const VT bi = bv[row];
+                const VT ri = bi - v;
+                r[row] = ri;
+                x[row] = gv[row];
+                acc[0] += bi * bi;
+                acc[1] += ri * ri;
+            });
+        } else {
+#pragma unroll 4
+            for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+                const VT bi = bv[i];
+                r[i] = bi;
+                x[i] = VT(0);
+                acc[0] += bi * bi;
+                acc[1] += bi * bi;
             }
         }
         block_sum<VT, 2>(acc, red);
@@ -1326,23 +1167,19 @@ __global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
         const int32_t st = ld_status(a.st.status + g.inst);
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         if (st == CMCG_SOLVE_ZERO_RHS) {
-            for (int t = g.t0; t < g.t1; ++t) {
-                const int i = a.tile_row0[t] + threadIdx.x;
-                if (i < min(a.tile_row0[t] + kTile, g.send)) a.x[vo + i] = VT(0);
-            }
+#pragma unroll 4
+            for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) a.x[vo + i] = VT(0);
             continue;
         }
         if (st != ST_RUNNING) continue;
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
         VT acc[1] = {VT(0)};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) {
-                const VT ri = a.r[vo + i];
-                const VT zi = dinv ? dinv[i] * ri : ri;
-                a.p[vo + i] = zi;
-                acc[0] += ri * zi;
-            }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+            const VT ri = a.r[vo + i];
+            const VT zi = dinv ? dinv[i] * ri : ri;
+            a.p[vo + i] = zi;
+            acc[0] += ri * zi;
         }
         block_sum<VT, 1>(acc, red);
         VT tot[1];
@@ -1375,13 +1212,10 @@ __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
         VT* q = a.q + vo;
         const auto A = inst_matrix<MT, FMT>(a.m, b_);
         VT acc[1] = {VT(0)};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
-            cta_rows<VT>(A, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<VT>{p}, [&](int row, VT v) {
-                q[row] = v;
-                acc[0] += p[row] * v;
-            });
-        }
+        cta_rows_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, [&](int row, VT v) {
+            q[row] = v;
+            acc[0] += p[row] * v;
+        });
         block_sum<VT, 1>(acc, red);
         VT tot[1];
         VT* const parts[1] = {a.part1};
@@ -1414,16 +1248,14 @@ __global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
         const VT alpha = static_cast<VT>(a.st.alpha[g.inst]);
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
         VT acc[2] = {VT(0), VT(0)};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) {
-                a.x[vo + i] += alpha * a.p[vo + i];
-                const VT ri = a.r[vo + i] - alpha * a.q[vo + i];
-                a.r[vo + i] = ri;
-                const VT zi = dinv ? dinv[i] * ri : ri;
-                acc[0] += ri * ri;
-                acc[1] += ri * zi;
-            }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+            a.x[vo + i] += alpha * a.p[vo + i];
+            const VT ri = a.r[vo + i] - alpha * a.q[vo + i];
+            a.r[vo + i] = ri;
+            const VT zi = dinv ? dinv[i] * ri : ri;
+            acc[0] += ri * ri;
+            acc[1] += ri * zi;
         }
         block_sum<VT, 2>(acc, red);
         VT tot[2];
@@ -1464,13 +1296,11 @@ __global__ void __launch_bounds__(kTile) k_grid_pupdate(SolveArgs<VT, MT> a) {
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const VT beta = static_cast<VT>(a.st.beta[g.inst]);
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) {
-                const VT ri = a.r[vo + i];
-                const VT zi = dinv ? dinv[i] * ri : ri;
-                a.p[vo + i] = zi + beta * a.p[vo + i];
-            }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+            const VT ri = a.r[vo + i];
+            const VT zi = dinv ? dinv[i] * ri : ri;
+            a.p[vo + i] = zi + beta * a.p[vo + i];
         }
     }
 }
@@ -1514,18 +1344,16 @@ __global__ void __launch_bounds__(kTile) k_gmix_init(GMixArgs<MI, MO> m) {
         const double* bv = m.b64 + (a.b_b == 1 ? 0 : vo);
         const double* sv = m.s + (a.m.mb == 1 ? 0 : vo);
         double acc[2] = {0.0, 0.0};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) {
-                const double bi = bv[i];
-                const float rh = static_cast<float>(sv[i] * bi);
-                m.x64[vo + i] = 0.0;
-                m.xh[vo + i] = 0.0f;
-                a.r[vo + i] = rh;
-                a.p[vo + i] = rh;
-                acc[0] += bi * bi;
-                acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
-            }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+            const double bi = bv[i];
+            const float rh = static_cast<float>(sv[i] * bi);
+            m.x64[vo + i] = 0.0;
+            m.xh[vo + i] = 0.0f;
+            a.r[vo + i] = rh;
+            a.p[vo + i] = rh;
+            acc[0] += bi * bi;
+            acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
         }
         block_sum<double, 2>(acc, red);
         double tot[2];
@@ -1575,13 +1403,10 @@ __global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
         float* q = a.q + vo;
         const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
         float acc[1] = {0.0f};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
-            cta_rows<float>(A, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<float>{p}, [&](int row, float v) {
-                q[row] = v;
-                acc[0] += p[row] * v;
-            });
-        }
+        cta_rows_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, [&](int row, float v) {
+            q[row] = v;
+            acc[0] += p[row] * v;
+        });
         block_sum<float, 1>(acc, red);
         float tot[1];
         float* const parts[1] = {a.part1};
@@ -1614,14 +1439,12 @@ __global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const float alpha = static_cast<float>(a.st.alpha[g.inst]);
         float acc[1] = {0.0f};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) {
-                m.xh[vo + i] += alpha * a.p[vo + i];
-                const float ri = a.r[vo + i] - alpha * a.q[vo + i];
-                a.r[vo + i] = ri;
-                acc[0] += ri * ri;
-            }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+            m.xh[vo + i] += alpha * a.p[vo + i];
+            const float ri = a.r[vo + i] - alpha * a.q[vo + i];
+            a.r[vo + i] = ri;
+            acc[0] += ri * ri;
         }
         block_sum<float, 1>(acc, red);
         float tot[1];
@@ -1660,12 +1483,10 @@ __global__ void __launch_bounds__(kTile) k_gmix_fold(GMixArgs<MI, MO> m) {
         if (TAIL ? !gmix_tail_status(st) : (st != ST_RUNNING || !ld_status(a.st.flag + g.inst))) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const double* sv = m.s + (a.m.mb == 1 ? 0 : vo);
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) {
-                m.x64[vo + i] += sv[i] * static_cast<double>(m.xh[vo + i]);
-                m.xh[vo + i] = 0.0f;
-            }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
+            m.x64[vo + i] += sv[i] * static_cast<double>(m.xh[vo + i]);
+            m.xh[vo + i] = 0.0f;
         }
     }
 }
@@ -1687,16 +1508,13 @@ __global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
         const double* xv = m.x64 + vo;
         const auto Ao = inst_matrix<MO, CMCG_CSR>(m.mo, b_);
         double acc[2] = {0.0, 0.0};
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int r0 = a.tile_row0[t], r1 = min(r0 + kTile, g.send);
-            cta_rows<double>(Ao, g.s, g.sr0, r0 - g.sr0, r1 - r0, GlobalX<double>{xv}, [&](int row, double v) {
-                const double r64 = bv[row] - v;
-                const float rh = static_cast<float>(sv[row] * r64);
-                if (!TAIL) a.r[vo + row] = rh;
-                acc[0] += r64 * r64;
-                acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
-            });
-        }
+        cta_rows_seg<double>(Ao, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<double>{xv}, [&](int row, double v) {
+            const double r64 = bv[row] - v;
+            const float rh = static_cast<float>(sv[row] * r64);
+            if (!TAIL) a.r[vo + row] = rh;
+            acc[0] += r64 * r64;
+            acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
+        });
         block_sum<double, 2>(acc, red);
         double tot[2];
         double* const parts[2] = {m.p1, m.p2};
@@ -1741,10 +1559,8 @@ __global__ void __launch_bounds__(kTile) k_gmix_pupdate(GMixArgs<MI, MO> m) {
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const float beta = static_cast<float>(a.st.beta[g.inst]);
-        for (int t = g.t0; t < g.t1; ++t) {
-            const int i = a.tile_row0[t] + threadIdx.x;
-            if (i < min(a.tile_row0[t] + kTile, g.send)) a.p[vo + i] = a.r[vo + i] + beta * a.p[vo + i];
-        }
+#pragma unroll 4
+        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) a.p[vo + i] = a.r[vo + i] + beta * a.p[vo + i];
     }
 }
 
@@ -1818,6 +1634,7 @@ struct cmcg_solver_s {
     bool use_smem = true;     // shared-memory-resident kernels where the systems fit
     bool inner_solve = false; // set while the solver runs the inner solves of a refinement
     bool fast_kernels = true; // compact-layout kernels where available (CUMAT_CG_FAST=0 disables)
+    bool coop = true;         // cooperative one-launch grid solve where it applies (CUMAT_CG_COOP=0 disables)
     int64_t systems_version = -1;  // pattern systems the plan was built for
     // plan
     int32_t n_sys = 0, max_sys_rows = 0, n_tiles = 0;
@@ -1830,6 +1647,13 @@ struct cmcg_solver_s {
     int32_t* d_seg_sys = nullptr;
     int32_t* d_cta_seg0 = nullptr;
     int32_t* d_sys_seg0 = nullptr;
+    // the same for the cooperative launch (one CTA per SM)
+    int32_t coop_ctas = 0, coop_n_seg = 0, coop_max_segs = 0;
+    int32_t* d_cseg_t0 = nullptr;
+    int32_t* d_cseg_t1 = nullptr;
+    int32_t* d_cseg_sys = nullptr;
+    int32_t* d_ccta_seg0 = nullptr;
+    int32_t* d_csys_seg0 = nullptr;
     // Jacobi inverse diagonal per vector type (F32, F64), [matrix batches][rows]
     void* dinv[2] = {nullptr, nullptr};
     // workspace
@@ -1892,35 +1716,51 @@ cmcg_status build_plan(cmcg_solver s) {
     s->n_tiles = static_cast<int32_t>(t_row0.size());
     s->systems_version = p->systems_version;
     // grid path: contiguous tile ranges per CTA, cut into segments at system
-    // boundaries (segment ids of one system are consecutive)
-    const int32_t G = std::max<int32_t>(1, std::min<int32_t>(s->n_tiles, p->ctx->sm_count * kGridCtasPerSm));
-    std::vector<int32_t> seg_t0, seg_t1, seg_sys, cta_seg0(G + 1), sys_seg0(n_sys + 1, -1);
-    for (int32_t c = 0; c < G; ++c) {
-        cta_seg0[c] = static_cast<int32_t>(seg_t0.size());
-        const int32_t a = static_cast<int32_t>(static_cast<int64_t>(c) * s->n_tiles / G);
-        const int32_t e = static_cast<int32_t>(static_cast<int64_t>(c + 1) * s->n_tiles / G);
-        for (int32_t t = a; t < e;) {
-            const int32_t sys = t_sys[t];
-            int32_t u = t;
-            while (u < e && t_sys[u] == sys) ++u;
-            if (sys_seg0[sys] < 0) sys_seg0[sys] = static_cast<int32_t>(seg_t0.size());
-            seg_t0.push_back(t);
-            seg_t1.push_back(u);
-            seg_sys.push_back(sys);
-            t = u;
+    // boundaries (segment ids of one system are consecutive); one plan for the
+    // graph kernels, one for the cooperative launch
+    struct SegPlan {
+        std::vector<int32_t> t0, t1, sys, cta0, sys0;
+    };
+    auto make_plan = [&](int32_t G) {
+        SegPlan P;
+        P.cta0.assign(G + 1, 0);
+        P.sys0.assign(n_sys + 1, -1);
+        for (int32_t c = 0; c < G; ++c) {
+            P.cta0[c] = static_cast<int32_t>(P.t0.size());
+            const int32_t a = static_cast<int32_t>(static_cast<int64_t>(c) * s->n_tiles / G);
+            const int32_t e = static_cast<int32_t>(static_cast<int64_t>(c + 1) * s->n_tiles / G);
+            for (int32_t t = a; t < e;) {
+                const int32_t sys = t_sys[t];
+                int32_t u = t;
+                while (u < e && t_sys[u] == sys) ++u;
+                if (P.sys0[sys] < 0) P.sys0[sys] = static_cast<int32_t>(P.t0.size());
+                P.t0.push_back(t);
+                P.t1.push_back(u);
+                P.sys.push_back(sys);
+                t = u;
+            }
         }
-    }
-    cta_seg0[G] = static_cast<int32_t>(seg_t0.size());
-    sys_seg0[n_sys] = static_cast<int32_t>(seg_t0.size());
-    for (int32_t i = n_sys - 1; i >= 0; --i)
-        if (sys_seg0[i] < 0) sys_seg0[i] = sys_seg0[i + 1];   // (every system has at least one tile)
+        P.cta0[G] = static_cast<int32_t>(P.t0.size());
+        P.sys0[n_sys] = static_cast<int32_t>(P.t0.size());
+        for (int32_t i = n_sys - 1; i >= 0; --i)
+            if (P.sys0[i] < 0) P.sys0[i] = P.sys0[i + 1];   // (every system has at least one tile)
+        return P;
+    };
+    const int32_t G = std::max<int32_t>(1, std::min<int32_t>(s->n_tiles, p->ctx->sm_count * kGridCtasPerSm));
+    const int32_t Gc = std::max<int32_t>(1, std::min<int32_t>(s->n_tiles, p->ctx->sm_count));
+    const SegPlan pg = make_plan(G), pc = make_plan(Gc);
     s->grid_ctas = G;
-    s->n_seg = static_cast<int32_t>(seg_t0.size());
+    s->n_seg = static_cast<int32_t>(pg.t0.size());
+    s->coop_ctas = Gc;
+    s->coop_n_seg = static_cast<int32_t>(pc.t0.size());
+    s->coop_max_segs = 0;
+    for (int32_t c = 0; c < Gc; ++c) s->coop_max_segs = std::max(s->coop_max_segs, pc.cta0[c + 1] - pc.cta0[c]);
     cudaStream_t st = p->ctx->stream;
     int32_t** bufs[] = {&s->d_order, &s->d_tile_row0, &s->d_seg_t0, &s->d_seg_t1, &s->d_seg_sys, &s->d_cta_seg0,
-                        &s->d_sys_seg0};
-    const std::vector<int32_t>* src[] = {&order, &t_row0, &seg_t0, &seg_t1, &seg_sys, &cta_seg0, &sys_seg0};
-    for (int k = 0; k < 7; ++k) {
+                        &s->d_sys_seg0, &s->d_cseg_t0, &s->d_cseg_t1, &s->d_cseg_sys, &s->d_ccta_seg0, &s->d_csys_seg0};
+    const std::vector<int32_t>* src[] = {&order, &t_row0, &pg.t0, &pg.t1, &pg.sys, &pg.cta0, &pg.sys0,
+                                         &pc.t0, &pc.t1, &pc.sys, &pc.cta0, &pc.sys0};
+    for (int k = 0; k < 12; ++k) {
         dev_free(*bufs[k]);
         *bufs[k] = nullptr;
         CMCG_TRY(dev_alloc(reinterpret_cast<void**>(bufs[k]), std::max<size_t>(src[k]->size(), 1) * 4));
@@ -2240,6 +2080,42 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     return CMCG_OK;
 }
 
+// One cooperative launch for the whole grid-path solve, when the instances are
+// few (the closing sums run in one CTA per barrier) and the segment plan's
+// CTAs can all be resident. *done = false leaves the solve to the graph path.
+template <typename VT, typename MT, int FMT>
+cmcg_status run_coop(cmcg_solver s, SolveArgs<VT, MT>& a, VT* p_alt, bool* done) {
+    *done = false;
+    cmcg_ctx ctx = s->A->pat->ctx;
+    const int n_inst = a.n_sys * a.ob;
+    if (!s->coop || n_inst > kCoopMaxInst || s->coop_ctas < 1 || s->coop_max_segs > kCoopMaxSegs) return CMCG_OK;
+    int coop_attr = 0, occ = 0;
+    CMCG_CUDA(cudaDeviceGetAttribute(&coop_attr, cudaDevAttrCooperativeLaunch, ctx->device));
+    CMCG_TRY((coop_cg_occupancy<VT, MT, FMT>(&occ)));
+    if (!coop_attr || occ * ctx->sm_count < s->coop_ctas) return CMCG_OK;
+    // the cooperative launch has its own segment plan (one CTA per SM)
+    SolveArgs<VT, MT> c = a;
+    c.n_seg = s->coop_n_seg;
+    c.seg_t0 = s->d_cseg_t0;
+    c.seg_t1 = s->d_cseg_t1;
+    c.seg_sys = s->d_cseg_sys;
+    c.cta_seg0 = s->d_ccta_seg0;
+    c.sys_seg0 = s->d_csys_seg0;
+    const int64_t items = static_cast<int64_t>(c.n_seg) * c.ob;
+    CMCG_TRY(ensure_buffer(&s->part_ws, &s->part_ws_bytes, 2 * sizeof(VT) * static_cast<size_t>(items) + 64));
+    c.part1 = static_cast<VT*>(s->part_ws);
+    c.part2 = c.part1 + items;
+    const int64_t cap = s->max_iter >= 0 ? s->max_iter : 2 * static_cast<int64_t>(s->max_sys_rows);
+    c.loop_cap = static_cast<int32_t>(std::min<int64_t>(cap + 2, INT32_MAX - 1));
+    // counters: next, active, loops, -, grid barrier (count, generation)
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 8 * sizeof(int32_t), ctx->stream));
+    // counters[4..7]: the grid barrier's two 64-bit words
+    CMCG_TRY((coop_cg_launch<VT, MT, FMT>(c, s->counters + 4, ctx->d_err, n_inst, p_alt, s->coop_ctas, ctx->stream)));
+    count_launch();
+    *done = true;
+    return CMCG_OK;
+}
+
 cmcg_status ensure_vec_ws(cmcg_solver s, size_t bytes) {
     if (s->vec_ws_bytes >= bytes && s->vec_ws) return CMCG_OK;
     CMCG_TRY(ensure_buffer(&s->vec_ws, &s->vec_ws_bytes, bytes));
@@ -2273,12 +2149,14 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
     } else {
         // the graph iterates on internal copies of x so that its arguments do not
         // depend on the caller's buffers
-        CMCG_TRY(ensure_vec_ws(s, 4 * vbytes + 256));
+        CMCG_TRY(ensure_vec_ws(s, 5 * vbytes + 256));
         VT* w = static_cast<VT*>(s->vec_ws);
         const size_t nv = p->rows * static_cast<size_t>(ob);
         a.r = w; a.p = w + nv; a.q = w + 2 * nv; a.x = w + 3 * nv;
         a.b = b; a.b_b = b_b; a.guess = guess; a.g_b = ob;
-        CMCG_TRY((run_grid<VT, MT, FMT>(s, a)));
+        bool done = false;
+        CMCG_TRY((run_coop<VT, MT, FMT>(s, a, w + 4 * nv, &done)));
+        if (!done) CMCG_TRY((run_grid<VT, MT, FMT>(s, a)));
         const int fb = (n_inst + 255) / 256;
         k_finalize<<<fb, 256, 0, ctx->stream>>>(s->st, n_inst);
         count_launch();
@@ -2635,6 +2513,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     // default tolerance: epsilon of the scalar type (IterativeSolverBase.h:131)
     s->tol = (A->dtype == CMCG_F64) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
     if (const char* e = std::getenv("CUMAT_CG_FAST")) s->fast_kernels = std::atoi(e) != 0;
+    if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);
     if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);
     if (st == CMCG_OK && cudaMemsetAsync(s->counters, 0, 64, A->pat->ctx->stream) != cudaSuccess) st = fail(CMCG_ERR_CUDA, "memset");
@@ -2659,7 +2538,9 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
     if (s->graph_mix) cudaGraphDestroy(s->graph_mix);
     for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_seg_t0),
                     static_cast<void*>(s->d_seg_t1), static_cast<void*>(s->d_seg_sys), static_cast<void*>(s->d_cta_seg0),
-                    static_cast<void*>(s->d_sys_seg0), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
+                    static_cast<void*>(s->d_sys_seg0), static_cast<void*>(s->d_cseg_t0), static_cast<void*>(s->d_cseg_t1),
+                    static_cast<void*>(s->d_cseg_sys), static_cast<void*>(s->d_ccta_seg0),
+                    static_cast<void*>(s->d_csys_seg0), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
                     s->st_ws, static_cast<void*>(s->counters), s->mix_vals, static_cast<void*>(s->mix_s)})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);

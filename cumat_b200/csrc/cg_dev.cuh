@@ -101,6 +101,89 @@ __device__ __forceinline__ void cta_rows(const InstMatrix<MT, FMT>& A, int s, in
     for (int i = i0 + threadIdx.x; i < i0 + n; i += blockDim.x) f(r0 + i, row_product<VT>(A.rm, s, r0, i, xf));
 }
 
+constexpr int kRowsInFlight = 4;   // rows per thread whose loads are interleaved
+
+// (A x) for K rows i[k] (local, ok[k] = row exists) of system s at once: the
+// slice descriptors, then two entries of every row, are loaded before any of
+// them is used, so a thread has K times the independent loads of
+// row_product in flight. Per row the entries are added in the same order as
+// row_product.
+template <typename VT, int K, typename MT, typename XF>
+__device__ __forceinline__ void row_products(const RowMat<MT>& A, int s, int r0, const int (&i)[K], const bool (&ok)[K],
+                                             const XF& xf, VT (&out)[K]) {
+    int64_t base[K];
+    int w[K];
+    int stride;
+    if (A.slice_off) {
+        const int sl0 = __ldg(A.sys_slice0 + s);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int sl = sl0 + (i[k] >> 5);
+            base[k] = ok[k] ? __ldg(A.slice_off + sl) + (i[k] & 31) : 0;
+            w[k] = ok[k] ? __ldg(A.slice_w + sl) : 0;
+        }
+        stride = 32;
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            base[k] = r0 + i[k];
+            w[k] = ok[k] ? A.ell_w : 0;
+        }
+        stride = A.ell_stride;
+    }
+    int wmax = w[0];
+#pragma unroll
+    for (int k = 1; k < K; ++k) wmax = max(wmax, w[k]);
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = VT(0);
+    for (int j0 = 0; j0 < wmax; j0 += 2) {
+        int c[K][2];
+        MT v[K][2];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj) {
+                const bool in = j0 + jj < w[k];
+                const int64_t o = base[k] + static_cast<int64_t>(j0 + jj) * stride;
+                c[k][jj] = in ? __ldg(A.col + o) : -1;
+                v[k][jj] = in ? A.val[o] : MT{};
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+                if (c[k][jj] >= 0) out[k] += mval<VT>(v[k][jj]) * xf(c[k][jj]);
+        }
+    }
+}
+
+// cta_rows with kRowsInFlight rows per thread in flight: thread t takes rows
+// i0 + t + k * blockDim.x, k = 0, 1, ... in groups of kRowsInFlight (i0 a
+// multiple of 32); f(global row, value) is called in increasing row order per
+// thread, as in cta_rows.
+template <typename VT, typename MT, int FMT, typename XF, typename F>
+__device__ __forceinline__ void cta_rows_seg(const InstMatrix<MT, FMT>& A, int s, int r0, int i0, int n, const XF& xf,
+                                             F&& f) {
+    // FP64 vectors or values: two rows (register budget of 1024-thread CTAs)
+    constexpr int K = sizeof(VT) + sizeof(MT) > 8 ? 2 : kRowsInFlight;
+    const int T = blockDim.x, end = i0 + n;
+    for (int ib = i0 + threadIdx.x; ib < end; ib += K * T) {
+        int ii[K];
+        bool ok[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            ii[k] = ib + k * T;
+            ok[k] = ii[k] < end;
+        }
+        VT v[K];
+        row_products<VT, K>(A.rm, s, r0, ii, ok, xf, v);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (ok[k]) f(r0 + ii[k], v[k]);
+    }
+}
+
 // Applies the product to the rows [r0, r0 + n) of one system with the whole
 // CTA: warp w takes the 32-row blocks w, w + W, ... so thread t always owns
 // rows r0 + t + k * blockDim.x. f(row, value) is called on the owning lane.

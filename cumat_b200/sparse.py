@@ -74,6 +74,13 @@ class Context:
     def synchronize(self) -> None:
         N.call("cmcg_ctx_synchronize", self.handle)
 
+    def device_errors(self) -> int:
+        """Synchronises and returns (and clears) the device error bits: 1 = a
+        bulk-copy wait ran out, 2 = a grid barrier wait ran out."""
+        f = C.c_int32(0)
+        N.call("cmcg_ctx_device_errors", self.handle, C.byref(f))
+        return int(f.value)
+
     @property
     def torch_device(self) -> torch.device:
         return torch.device("cuda", self.device)

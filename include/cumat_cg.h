@@ -111,9 +111,10 @@ cmcg_status cmcg_device_free(cmcg_ctx ctx, void* p);
 cmcg_status cmcg_memcpy(cmcg_ctx ctx, void* dst, const void* src, int64_t bytes, int32_t kind);
 cmcg_status cmcg_memset_zero(cmcg_ctx ctx, void* dst, int64_t bytes);
 cmcg_status cmcg_ctx_stream(cmcg_ctx ctx, void** stream);
-/* Synchronises and returns (then clears) the context's device error bits: a
- * bounded wait inside a kernel that ran out sets bit 0 (no reference
- * counterpart; the reference has no device-side waits). */
+/* Synchronises and returns (then clears) the context's device error bits:
+ * bit 0 = a bulk-copy (mbarrier) wait ran out, bit 1 = a grid-barrier wait of
+ * the cooperative solver ran out. Every device-side wait is bounded (no
+ * reference counterpart; the reference has no device-side waits). */
 cmcg_status cmcg_ctx_device_errors(cmcg_ctx ctx, int32_t* flags);
 
 /* ---- sparsity patterns --------------------------------------------------- */

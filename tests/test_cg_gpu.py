@@ -400,6 +400,58 @@ def test_refined_grid_path_single_system(cuda):
     assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-8
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_cooperative_grid_solve_matches_graph_path(cuda, monkeypatch, dtype):
+    # the one-launch cooperative grid solve (one CTA per SM) and the CUDA-graph
+    # grid solve (four CTAs per SM) differ only in how the partial sums are
+    # grouped
+    m = cm()
+    pr = P.poisson2d(160, 3)
+    A = _matrix(pr, dtype=dtype)
+    b = torch.from_numpy(pr.b.astype(np.float64 if dtype == torch.float64 else np.float32)).to(cuda)
+    tol = 1e-10 if dtype == torch.float64 else 1e-6
+    cg = m.ConjugateGradient(A).setTolerance(tol).set_path(2)
+    cg.solve(b)
+    before = m.launch_count()
+    x1 = cg.solve(b).cpu().numpy()
+    assert m.launch_count() - before == 2      # the cooperative solve + the finaliser
+    s1 = cg.system_stats()
+    monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    cg0 = m.ConjugateGradient(A).setTolerance(tol).set_path(2)
+    x0 = cg0.solve(b).cpu().numpy()
+    s0 = cg0.system_stats()
+    assert s1["status"][0] == 0 and abs(int(s1["iterations"][0]) - int(s0["iterations"][0])) <= 1
+    rtol = 1e-9 if dtype == torch.float64 else 1e-4
+    assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < rtol
+    # deterministic: the same launch twice gives the same bits
+    assert np.array_equal(cg.solve(b).cpu().numpy(), x1)
+    _, it_o, _ = O.cg_csr(pr.n, pr.row_ptr, pr.col, pr.val.astype(np.float64) if dtype == torch.float64 else pr.val,
+                          pr.b.astype(np.float64) if dtype == torch.float64 else pr.b, tol, -1, 1)
+    assert abs(int(s1["iterations"][0]) - int(it_o[0])) <= 2
+    assert m.Context.current().device_errors() == 0
+
+
+def test_cooperative_grid_solve_batched_instances(cuda):
+    # 3 value batches x 2 systems = 6 instances in one cooperative launch
+    m = cm()
+    bt = P.fv2d_batch(2, 150, 170, 0.5, 17)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    vals = np.concatenate([bt.val, bt.val * 2.0, bt.val * 0.5]).astype(np.float32)
+    A = m.SparseMatrix(p, dtype=torch.float32, batches=3).setData(vals)
+    b = torch.from_numpy(np.tile(bt.b, 3)).to(cuda)
+    cg = m.ConjugateGradient(A).setTolerance(1e-6).set_path(2)
+    x = cg.solve(b).cpu().numpy().reshape(3, -1)
+    st = cg.system_stats()
+    assert st["status"].shape == (6,) and np.all(st["status"] == 0)
+    _, it_o, _ = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, bt.b, 1e-6)
+    # Jacobi CG is invariant to scaling the matrix: the same counts per batch
+    for k in range(3):
+        assert np.all(np.abs(st["iterations"][2 * k:2 * k + 2] - it_o) <= 2)
+    assert np.allclose(x[1], x[0] / 2, rtol=1e-3, atol=1e-5 * np.abs(x[0]).max())
+    assert np.allclose(x[2], x[0] * 2, rtol=1e-3, atol=1e-5 * np.abs(x[0]).max())
+
+
 def test_grid_reliable_updates_packed_vs_oracle(cuda):
     # the grid path's reliable-update solver on packed systems: same method as
     # the persistent kernel, whole-GPU reductions per system
