@@ -157,7 +157,7 @@ def whole_job_rate(units_per_rank: int, world: int, ms_max: float) -> float:
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes (per unit, stated in DESIGN.md)
+# algorithmic bytes (per unit)
 # ---------------------------------------------------------------------------
 
 def refined_bytes(bt, inner_iters, outer_steps, inner_value_bytes=4):
@@ -243,6 +243,13 @@ def spmv_gbs(cm, torch, dev, stream):
 # 2D-Poisson Matrix.json; see docs/03_Benchmarks.dox)
 REF_CSRMV_MS = {10: (0.0178, 0.0136), 100: (0.0160, 0.0151), 1000: (0.1635, 0.1444), 10000: (17.69, 19.62)}
 REF_CG_MS = {10: 6.67, 20: 11.47, 50: 28.58, 100: 48.60, 200: 74.14, 500: 201.58, 1000: 599.84}
+# benchmarks/Linear Combination - Constant Size.json / Constant Count.json and
+# benchmarks/Dotproduct.json ("CuMat" rows; the dot includes reading the result)
+REF_LINCOMB_SIZE_MS = [0.03682, 0.04331, 0.05314, 0.06548, 0.0775, 0.09306, 0.09788, 0.10953, 0.12119, 0.13133]
+REF_LINCOMB_COUNT_MS = {100: 0.01513, 1000: 0.01483, 10000: 0.01967, 100000: 0.01702, 1000000: 0.04742,
+                        10000000: 0.33869, 50000000: 2.00751}
+REF_DOT_MS = {10: 0.11192, 100: 0.14819, 1000: 0.16076, 10000: 0.16291, 100000: 0.14098, 1000000: 0.16244,
+              10000000: 0.39226, 100000000: 2.37392}
 
 
 def _boundary_rhs(g: int) -> np.ndarray:
@@ -330,6 +337,41 @@ def reference_suite(cm, torch, dev, stream, hbm_peak):
         ms = statistics.mean(times)
         out["cg"].append({"grid": g, "ms": round(ms, 4), "iterations": int(its[-1]), "ref_ms": REF_CG_MS[g],
                           "speedup": round(REF_CG_MS[g] / ms, 1)})
+    # linear combinations of FP32 vectors U[0, 1) (the reference's benchmark expression)
+    out["lincomb"] = []
+    gen = torch.Generator(device=dev).manual_seed(7)
+
+    def lincomb_case(n, k, ref):
+        vs = [torch.rand(n, device=dev, generator=gen) for _ in range(k)]
+        fs = torch.rand(k, generator=torch.Generator().manual_seed(k)).tolist()
+        o = torch.empty(n, device=dev)
+        t = ev_ms(lambda: cm.linear_combination(fs, vs, out=o), 200 if n <= 10 ** 7 else 50)
+        byt = (k + 1) * n * 4
+        out["lincomb"].append({"n": n, "terms": k, "ms": round(t, 5), "gbs": round(byt / t / 1e6, 1),
+                               "frac": round(byt / t / 1e6 / hbm_peak, 3), "ref_ms": ref, "speedup": round(ref / t, 1)})
+    for k in range(1, 11):
+        lincomb_case(10 ** 6, k, REF_LINCOMB_SIZE_MS[k - 1])
+    for n, ref in REF_LINCOMB_COUNT_MS.items():
+        lincomb_case(n, 2, ref)
+    # dot product including the device-to-host read of the result, like the reference's timing
+    out["dot"] = []
+    for n, ref in REF_DOT_MS.items():
+        x = torch.rand(n, device=dev, generator=gen)
+        y = torch.rand(n, device=dev, generator=gen)
+        h = torch.empty(()).pin_memory()
+
+        def dot_read():
+            h.copy_(cm.dot(x, y), non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+        for _ in range(5):
+            dot_read()
+        reps = 200 if n <= 10 ** 7 else 50
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            dot_read()
+        t = (time.perf_counter() - t0) * 1e3 / reps
+        out["dot"].append({"n": n, "ms": round(t, 5), "gbs": round(2 * n * 4 / t / 1e6, 1), "ref_ms": ref,
+                           "speedup": round(ref / t, 1)})
     return out
 
 

@@ -6,10 +6,12 @@ Importing fails if the library has not been built (no CPU fallback).
 """
 from . import _native
 from ._native import CuMatError, launch_count
-from .sparse import (CSR, ELLPACK, Context, SparseMatrix, SparsityPattern, dot, norm, sddmm, squaredNorm)
+from .sparse import (CSR, ELLPACK, Context, SparseMatrix, SparsityPattern, dot, linear_combination, norm, sddmm,
+                     squaredNorm)
 from .solvers import ConjugateGradient, DiagonalPreconditioner, IdentityPreconditioner
 
 __all__ = [
-    "CSR", "ELLPACK", "Context", "SparseMatrix", "SparsityPattern", "dot", "norm", "squaredNorm", "sddmm",
+    "CSR", "ELLPACK", "Context", "SparseMatrix", "SparsityPattern", "dot", "linear_combination", "norm", "squaredNorm",
+    "sddmm",
     "ConjugateGradient", "DiagonalPreconditioner", "IdentityPreconditioner", "CuMatError", "launch_count",
 ]

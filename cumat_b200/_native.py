@@ -57,6 +57,7 @@ SIGNATURES = {
     "cmcg_dot": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp, _i32, _vp]),
     "cmcg_squared_norm": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp]),
     "cmcg_dot_noalloc": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp, _i32, _vp]),
+    "cmcg_lincomb": (_i32, [_vp, _i32, _i64, _i32, _vp, _vp, _vp, _vp, _i32, _i32]),
     "cmcg_sddmm": (_i32, [_vp, _i32, _f64, _vp, _i32, _vp, _i32, _vp, _i32]),
     "cmcg_cg_create": (_i32, [_vp, _i32, C.POINTER(_vp)]),
     "cmcg_cg_destroy": (_i32, [_vp]),

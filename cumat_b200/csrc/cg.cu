@@ -678,6 +678,58 @@ __device__ __forceinline__ VT fast_row(const uint16_t* __restrict__ col, const M
     return acc;
 }
 
+// Two rows of equal width W (the lane's rows in two slices): the 4 W index
+// and value loads of both rows issue before the first product, so the two
+// rows cost one memory latency instead of two; each row sums in entry order.
+template <int W, typename VT, typename MT, typename XF>
+__device__ __forceinline__ void row_w2(const uint16_t* __restrict__ c0, const MT* __restrict__ v0,
+                                       const uint16_t* __restrict__ c1, const MT* __restrict__ v1, const XF& xf, VT& q0,
+                                       VT& q1) {
+    int ci0[W], ci1[W];
+    MT vi0[W], vi1[W];
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+        ci0[j] = __ldg(c0 + 32 * j);
+        vi0[j] = v0[32 * j];
+        ci1[j] = __ldg(c1 + 32 * j);
+        vi1[j] = v1[32 * j];
+    }
+    VT a0 = VT(0), a1 = VT(0);
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+        a0 += mval<VT>(vi0[j]) * xf(ci0[j]);
+        a1 += mval<VT>(vi1[j]) * xf(ci1[j]);
+    }
+    q0 = a0;
+    q1 = a1;
+}
+
+// fast_row for the lane's rows in two slices (e1.w == 0: no second row).
+template <typename VT, typename MT, typename XF>
+__device__ __forceinline__ void fast_rows2(const uint16_t* __restrict__ col, const MT* __restrict__ val, SliceEnt e0,
+                                           SliceEnt e1, int lane, const XF& xf, VT& q0, VT& q1) {
+    if (e0.w == e1.w) {   // warp-uniform
+        const uint16_t* c0 = col + e0.off + lane;
+        const MT* v0 = val + e0.off + lane;
+        const uint16_t* c1 = col + e1.off + lane;
+        const MT* v1 = val + e1.off + lane;
+        switch (e0.w) {
+            case 0: q0 = q1 = VT(0); return;
+            case 3: row_w2<3>(c0, v0, c1, v1, xf, q0, q1); return;
+            case 4: row_w2<4>(c0, v0, c1, v1, xf, q0, q1); return;
+            case 5: row_w2<5>(c0, v0, c1, v1, xf, q0, q1); return;
+            default: break;
+        }
+        // wider rows only with 4-byte values (register budget of 1024-thread CTAs)
+        if constexpr (sizeof(MT) <= 4) {
+            if (e0.w == 6) { row_w2<6>(c0, v0, c1, v1, xf, q0, q1); return; }
+            if (e0.w == 7) { row_w2<7>(c0, v0, c1, v1, xf, q0, q1); return; }
+        }
+    }
+    q0 = fast_row<VT>(col, val, e0, lane, xf);
+    q1 = fast_row<VT>(col, val, e1, lane, xf);
+}
+
 struct CompactArgs {
     const uint16_t* col16;
     const int32_t* off32;
@@ -788,14 +840,20 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
             while (status == ST_RUNNING) {
                 if (it >= maxit) { status = CMCG_SOLVE_MAX_ITER; break; }
                 VT pq[1] = {VT(0)};
+                // two row slots at a time (slices past the system have width 0)
 #pragma unroll
-                for (int k = 0; k < kSmemNK; ++k) {
+                for (int k = 0; k < kSmemNK; k += 2) {
                     if (k * kSmemThreads >= n) break;
-                    const int i = tid + k * kSmemThreads;
-                    if (i < n) {
-                        const VT qi = fast_row<VT>(c.col16, vals, tab[warp][k], lane, LocalX<VT>{P});
-                        if constexpr (kQReg) q[k] = qi; else Qg[i] = qi;
-                        pq[0] += P[i] * qi;
+                    const int i0 = tid + k * kSmemThreads, i1 = i0 + kSmemThreads;
+                    VT q0, q1;
+                    fast_rows2<VT>(c.col16, vals, tab[warp][k], tab[warp][k + 1], lane, LocalX<VT>{P}, q0, q1);
+                    if (i0 < n) {
+                        if constexpr (kQReg) q[k] = q0; else Qg[i0] = q0;
+                        pq[0] += P[i0] * q0;
+                    }
+                    if (i1 < n) {
+                        if constexpr (kQReg) q[k + 1] = q1; else Qg[i1] = q1;
+                        pq[0] += P[i1] * q1;
                     }
                 }
                 block_sum<VT, 1>(pq, red);
@@ -945,15 +1003,17 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         while (status == ST_RUNNING) {
             if (it >= maxit || updates >= a.max_updates) { status = CMCG_SOLVE_MAX_ITER; break; }
             float pq[1] = {0.0f};
+            // two row slots at a time (slices past the system have width 0)
 #pragma unroll
-            for (int k = 0; k < kSmemNK; ++k) {
+            for (int k = 0; k < kSmemNK; k += 2) {
                 if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
-                q[k] = 0.0f;
-                if (i < n) {
-                    q[k] = fast_row<float>(a.c.col16, vin, tab[warp][k], lane, LocalX<float>{P});
-                    pq[0] += P[i] * q[k];
-                }
+                const int i0 = tid + k * kSmemThreads, i1 = i0 + kSmemThreads;
+                float q0, q1;
+                fast_rows2<float>(a.c.col16, vin, tab[warp][k], tab[warp][k + 1], lane, LocalX<float>{P}, q0, q1);
+                q[k] = i0 < n ? q0 : 0.0f;
+                q[k + 1] = i1 < n ? q1 : 0.0f;
+                if (i0 < n) pq[0] += P[i0] * q[k];
+                if (i1 < n) pq[0] += P[i1] * q[k + 1];
             }
             block_sum<float, 1>(pq, red);
             const float alpha = rz / pq[0];

@@ -293,6 +293,29 @@ def norm(x: torch.Tensor) -> torch.Tensor:
     return torch.sqrt(squaredNorm(x))
 
 
+def linear_combination(coeffs, vectors, out: Optional[torch.Tensor] = None, mode: int = N.ASSIGN) -> torch.Tensor:
+    """sum_t coeffs[t] * vectors[t] in one fused pass (up to 16 terms): the
+    cwise expression ``v0 * f0 + v1 * f1 + ...`` of the reference. Vectors are
+    (n,) or (b, n); one-batch vectors broadcast. mode ADD / SUB accumulates
+    into ``out``."""
+    vectors = [v.contiguous() for v in vectors]
+    if len(vectors) != len(coeffs) or not 1 <= len(vectors) <= 16:
+        raise ValueError("linear_combination: 1 to 16 (coefficient, vector) pairs")
+    ctx = Context.current()
+    n = vectors[0].shape[-1]
+    vb = [1 if v.dim() == 1 else v.shape[0] for v in vectors]
+    ob = max(vb)
+    batched = any(v.dim() == 2 for v in vectors)
+    if out is None:
+        out = torch.empty((ob, n) if batched else (n,), dtype=vectors[0].dtype, device=vectors[0].device)
+    cs = (C.c_double * len(coeffs))(*[float(c) for c in coeffs])
+    ptrs = (C.c_void_p * len(vectors))(*[v.data_ptr() for v in vectors])
+    bs = (C.c_int32 * len(vectors))(*vb)
+    N.call("cmcg_lincomb", ctx.handle, _TORCH_DT[vectors[0].dtype], n, len(vectors), cs, ptrs, bs, _vp(out), ob,
+           int(mode))
+    return out
+
+
 def sddmm(A: SparseMatrix, u: torch.Tensor, v: torch.Tensor, alpha: float = 1.0) -> torch.Tensor:
     """alpha * u v^T sampled on A's pattern, in A's value layout ([batch][nnz])."""
     ub = 1 if u.dim() == 1 else u.shape[0]

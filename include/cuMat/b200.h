@@ -283,6 +283,32 @@ public:
     }
 };
 
+// sum_t factors[t] * vectors[t] in one fused pass (up to 16 terms): the value
+// of the reference's cwise expression `v0 * f0 + v1 * f1 + ...`
+// (benchmarks/linear_combination/Implementation_cuMat.cu:52-66). Vectors with
+// one batch broadcast against batched ones.
+template <typename S, int R, int C, int B, int F>
+Matrix<S, R, C, B, F> linearCombination(const std::vector<Matrix<S, R, C, B, F>>& vectors, const std::vector<double>& factors) {
+    static_assert(b200::DType<S>::id >= 0, "linearCombination: float or double storage");
+    if (vectors.empty() || vectors.size() != factors.size() || vectors.size() > 16)
+        throw std::invalid_argument("linearCombination: 1 to 16 (vector, factor) pairs");
+    Index ob = 1;
+    std::vector<const void*> ptrs;
+    std::vector<int32_t> vb;
+    for (const auto& v : vectors) {
+        if (v.rows() * v.cols() != vectors[0].rows() * vectors[0].cols())
+            throw std::invalid_argument("linearCombination: size mismatch");
+        ob = v.batches() > ob ? v.batches() : ob;
+        ptrs.push_back(v.data());
+        vb.push_back(static_cast<int32_t>(v.batches()));
+    }
+    Matrix<S, R, C, B, F> out(vectors[0].rows(), vectors[0].cols(), ob);
+    b200::check(cmcg_lincomb(out.context(), b200::DType<S>::id, vectors[0].rows() * vectors[0].cols(),
+                             static_cast<int32_t>(vectors.size()), factors.data(), ptrs.data(), vb.data(), out.data(),
+                             static_cast<int32_t>(ob), CMCG_ASSIGN));
+    return out;
+}
+
 // typedefs of the reference (cuMat/src/Matrix.h:1396-1440), the ones this path uses
 #define CUMAT_B200_TYPEDEFS(T, s)                                         \
     typedef Matrix<T, 1, 1, 1, ColumnMajor> Scalar##s;                    \

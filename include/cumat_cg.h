@@ -195,6 +195,17 @@ cmcg_status cmcg_squared_norm(cmcg_ctx ctx, int32_t dtype, int64_t n, const void
 cmcg_status cmcg_dot_noalloc(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t x_batches, const void* y,
                              int32_t y_batches, void* out);
 
+/* out (mode)= sum_t coeffs[t] * v_t over n_terms <= 16 vectors, for every
+ * batch, in one streaming pass (reference: the cwise evaluation of
+ * `v0 * f0 + v1 * f1 + ...`, cuMat/src/CwiseOp.h:66-85, timed by
+ * benchmarks/linear_combination/Implementation_cuMat.cu:52-66). vectors: host
+ * array of n_terms device pointers, vector t holding v_batches[t] batches of n
+ * elements (1 broadcasts, else out_batches); coeffs: host array; out: device
+ * [out_batches][n]; dtype F32 or F64. Terms are added in order. */
+cmcg_status cmcg_lincomb(cmcg_ctx ctx, int32_t dtype, int64_t n, int32_t n_terms, const double* coeffs,
+                         const void* const* vectors, const int32_t* v_batches, void* out, int32_t out_batches,
+                         int32_t mode);
+
 /* out[k] = alpha * u[row(k)] * v[col(k)] for every stored entry k of batch b
  * (u: [u_batches][rows], v: [v_batches][cols], out: [out_batches][nnz] in the
  * matrix layout). The sparse outer product evaluated on a pattern (reference

@@ -212,6 +212,22 @@ int main() {
         REQUIRE(close_rel(host(m.squaredNorm()), {46, 130}, 0));
         REQUIRE(close_rel(host(m.norm()), {6.782329983125268139, 11.401754250991379791}, 1e-15));
     });
+    run("linear combination", [] {
+        // the reference's linear-combination benchmark expression with 3 terms
+        std::mt19937 rng(11);
+        const int n = 1001;   // not a multiple of 4: the element-wise path
+        std::vector<VectorXf> vs;
+        std::vector<std::vector<float>> hv;
+        for (int t = 0; t < 3; ++t) {
+            hv.push_back(uniform<float>(n, rng));
+            vs.push_back(VectorXf::fromHost(hv.back(), n));
+        }
+        const std::vector<double> f = {0.5, -2.0, 3.25};
+        VectorXf out = linearCombination(vs, f);
+        std::vector<double> want(n);
+        for (int i = 0; i < n; ++i) want[i] = 0.5 * hv[0][i] - 2.0 * hv[1][i] + 3.25 * hv[2][i];
+        REQUIRE(close_rel(host(out), want, 1e-6));
+    });
     for (int size : {5, 10, 50, 100}) {
         const std::string n = "Conjugate Gradient - Early Out Rhs, size " + std::to_string(size);
         run(n.c_str(), [size] {

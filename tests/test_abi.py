@@ -59,6 +59,8 @@ def test_validation_without_device(native):
     assert L.cmcg_spmv(None, 0, None, 1, None, 0) == 1
     assert L.cmcg_pattern_create_csr(None, 4, 4, 0, None, None, 0, None) == 1
     assert L.cmcg_cg_create(None, 1, None) == 1
+    assert L.cmcg_lincomb(None, 0, 8, 1, None, None, None, None, 1, 0) == 1
+    assert L.cmcg_device_alloc(None, 16, None) == 1
     with pytest.raises(native.CuMatError):
         native.check(L.cmcg_matrix_create(None, 0, 1, None))
 

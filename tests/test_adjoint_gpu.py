@@ -48,7 +48,7 @@ def test_adjoint_vs_dense_and_finite_differences(cuda):
             for k in range(rp[r], rp[r + 1]):
                 assert abs(gA[k0 + k] - (-lam[r] * xt[ci[k]])) <= 1e-9 * np.abs(lam).max() * np.abs(xt).max()
         # central finite differences of L in FP64 (h = 1e-6) on 8 random b and A
-        # entries, judged relative to the gradient's scale in this system
+        # entries, measured relative to the gradient's scale in this system
         L = lambda xx: 0.5 * np.sum((xx - xs[r0:r1]) ** 2)  # noqa: E731
         h = 1e-6
         gscale = max(np.abs(lam).max(), np.abs(gA[k0:bt.row_ptr[r1]]).max())
@@ -135,7 +135,7 @@ def test_adjoint_config5_shape_vs_sparse_fd(cuda):
         bs = bt.b[r0:r1].astype(np.float64)
         L = lambda xx: 0.5 * np.sum((xx - xs[r0:r1]) ** 2)  # noqa: E731
         # |L| ~ 1e5 and kappa ~ 1e4 here, so FP64 central differences carry
-        # noise of ~1e-5 absolute; the agreement is judged relative to the
+        # noise of ~1e-5 absolute; the agreement is measured relative to the
         # gradient's scale (its largest entry in this system)
         k0, k1 = bt.row_ptr[r0], bt.row_ptr[r1]
         gscale = max(np.abs(gb[r0:r1]).max(), np.abs(gA[k0:k1]).max())
