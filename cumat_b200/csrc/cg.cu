@@ -1179,7 +1179,7 @@ __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
         const auto A = inst_matrix<MT, FMT>(a.m, b_);
         const VT* gv = a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr;
         if (gv) {
-            cta_rows_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{gv}, [&](int row, VT v) {
+            cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{gv}, [&](int row, VT v) {
                 const VT bi = bv[row];
                 const VT ri = bi - v;
                 r[row] = ri;
@@ -1272,7 +1272,7 @@ __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
         VT* q = a.q + vo;
         const auto A = inst_matrix<MT, FMT>(a.m, b_);
         VT acc[1] = {VT(0)};
-        cta_rows_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, [&](int row, VT v) {
+        cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, [&](int row, VT v) {
             q[row] = v;
             acc[0] += p[row] * v;
         });
@@ -1308,15 +1308,40 @@ __global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
         const VT alpha = static_cast<VT>(a.st.alpha[g.inst]);
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
         VT acc[2] = {VT(0), VT(0)};
-#pragma unroll 4
-        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
-            a.x[vo + i] += alpha * a.p[vo + i];
-            const VT ri = a.r[vo + i] - alpha * a.q[vo + i];
-            a.r[vo + i] = ri;
-            const VT zi = dinv ? dinv[i] * ri : ri;
-            acc[0] += ri * ri;
-            acc[1] += ri * zi;
-        }
+        VT* x = a.x + vo;
+        const VT* p = a.p + vo;
+        VT* r = a.r + vo;
+        const VT* q = a.q + vo;
+        const void* const ptrs[5] = {x + g.r0, p + g.r0, r + g.r0, q + g.r0, dinv ? dinv + g.r0 : nullptr};
+        seg_rows_vec<5>(
+            g.r0, g.r1, ptrs,
+            [&](int i) {
+                V4<VT> X, P, R, Q, D;
+                X.load(x + i);
+                P.load(p + i);
+                R.load(r + i);
+                Q.load(q + i);
+                if (dinv) D.load(dinv + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    X.v[k] += alpha * P.v[k];
+                    const VT ri = R.v[k] - alpha * Q.v[k];
+                    R.v[k] = ri;
+                    const VT zi = dinv ? D.v[k] * ri : ri;
+                    acc[0] += ri * ri;
+                    acc[1] += ri * zi;
+                }
+                X.store(x + i);
+                R.store(r + i);
+            },
+            [&](int i) {
+                x[i] += alpha * p[i];
+                const VT ri = r[i] - alpha * q[i];
+                r[i] = ri;
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                acc[0] += ri * ri;
+                acc[1] += ri * zi;
+            });
         block_sum<VT, 2>(acc, red);
         VT tot[2];
         VT* const parts[2] = {a.part1, a.part2};
@@ -1356,12 +1381,25 @@ __global__ void __launch_bounds__(kTile) k_grid_pupdate(SolveArgs<VT, MT> a) {
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const VT beta = static_cast<VT>(a.st.beta[g.inst]);
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
-#pragma unroll 4
-        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
-            const VT ri = a.r[vo + i];
-            const VT zi = dinv ? dinv[i] * ri : ri;
-            a.p[vo + i] = zi + beta * a.p[vo + i];
-        }
+        const VT* r = a.r + vo;
+        VT* p = a.p + vo;
+        const void* const ptrs[3] = {r + g.r0, p + g.r0, dinv ? dinv + g.r0 : nullptr};
+        seg_rows_vec<3>(
+            g.r0, g.r1, ptrs,
+            [&](int i) {
+                V4<VT> R, P, D;
+                R.load(r + i);
+                P.load(p + i);
+                if (dinv) D.load(dinv + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) P.v[k] = (dinv ? D.v[k] * R.v[k] : R.v[k]) + beta * P.v[k];
+                P.store(p + i);
+            },
+            [&](int i) {
+                const VT ri = r[i];
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                p[i] = zi + beta * p[i];
+            });
     }
 }
 
@@ -1463,7 +1501,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
         float* q = a.q + vo;
         const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
         float acc[1] = {0.0f};
-        cta_rows_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, [&](int row, float v) {
+        cta_rows4_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, [&](int row, float v) {
             q[row] = v;
             acc[0] += p[row] * v;
         });
@@ -1499,13 +1537,34 @@ __global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const float alpha = static_cast<float>(a.st.alpha[g.inst]);
         float acc[1] = {0.0f};
-#pragma unroll 4
-        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
-            m.xh[vo + i] += alpha * a.p[vo + i];
-            const float ri = a.r[vo + i] - alpha * a.q[vo + i];
-            a.r[vo + i] = ri;
-            acc[0] += ri * ri;
-        }
+        float* xh = m.xh + vo;
+        const float* p = a.p + vo;
+        float* r = a.r + vo;
+        const float* q = a.q + vo;
+        const void* const ptrs[4] = {xh + g.r0, p + g.r0, r + g.r0, q + g.r0};
+        seg_rows_vec<4>(
+            g.r0, g.r1, ptrs,
+            [&](int i) {
+                V4<float> X, P, R, Q;
+                X.load(xh + i);
+                P.load(p + i);
+                R.load(r + i);
+                Q.load(q + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    X.v[k] += alpha * P.v[k];
+                    R.v[k] -= alpha * Q.v[k];
+                    acc[0] += R.v[k] * R.v[k];
+                }
+                X.store(xh + i);
+                R.store(r + i);
+            },
+            [&](int i) {
+                xh[i] += alpha * p[i];
+                const float ri = r[i] - alpha * q[i];
+                r[i] = ri;
+                acc[0] += ri * ri;
+            });
         block_sum<float, 1>(acc, red);
         float tot[1];
         float* const parts[1] = {a.part2};
@@ -1568,7 +1627,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
         const double* xv = m.x64 + vo;
         const auto Ao = inst_matrix<MO, CMCG_CSR>(m.mo, b_);
         double acc[2] = {0.0, 0.0};
-        cta_rows_seg<double>(Ao, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<double>{xv}, [&](int row, double v) {
+        cta_rows4_seg<double>(Ao, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<double>{xv}, [&](int row, double v) {
             const double r64 = bv[row] - v;
             const float rh = static_cast<float>(sv[row] * r64);
             if (!TAIL) a.r[vo + row] = rh;
@@ -1619,8 +1678,20 @@ __global__ void __launch_bounds__(kTile) k_gmix_pupdate(GMixArgs<MI, MO> m) {
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const float beta = static_cast<float>(a.st.beta[g.inst]);
-#pragma unroll 4
-        for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) a.p[vo + i] = a.r[vo + i] + beta * a.p[vo + i];
+        const float* r = a.r + vo;
+        float* p = a.p + vo;
+        const void* const ptrs[2] = {r + g.r0, p + g.r0};
+        seg_rows_vec<2>(
+            g.r0, g.r1, ptrs,
+            [&](int i) {
+                V4<float> R, P;
+                R.load(r + i);
+                P.load(p + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) P.v[k] = R.v[k] + beta * P.v[k];
+                P.store(p + i);
+            },
+            [&](int i) { p[i] = r[i] + beta * p[i]; });
     }
 }
 
@@ -2149,6 +2220,9 @@ cmcg_status run_coop(cmcg_solver s, SolveArgs<VT, MT>& a, VT* p_alt, bool* done)
     cmcg_ctx ctx = s->A->pat->ctx;
     const int n_inst = a.n_sys * a.ob;
     if (!s->coop || n_inst > kCoopMaxInst || s->coop_ctas < 1 || s->coop_max_segs > kCoopMaxSegs) return CMCG_OK;
+    // systems large enough to hide the graph's per-kernel launches run faster
+    // on the graph kernels (more threads per SM in flight)
+    if (s->max_sys_rows > kCoopMaxRows) return CMCG_OK;
     int coop_attr = 0, occ = 0;
     CMCG_CUDA(cudaDeviceGetAttribute(&coop_attr, cudaDevAttrCooperativeLaunch, ctx->device));
     CMCG_TRY((coop_cg_occupancy<VT, MT, FMT>(&occ)));

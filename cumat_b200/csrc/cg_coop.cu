@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
         const VT* gv = a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr;
         if (gv) {
             const auto A = inst_matrix<MT, FMT>(a.m, b_);
-            cta_rows_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{gv}, [&](int row, VT v) {
+            cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{gv}, [&](int row, VT v) {
                 const VT bi = bv[row];
                 const VT ri = bi - v;
                 r[row] = ri;
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
                 VT* pc = pcur + vo;
                 VT* q = a.q + vo;
                 const auto A = inst_matrix<MT, FMT>(a.m, b_);
-                cta_rows_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, PNextX<VT>{rv, dinv, pp, beta},
+                cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, PNextX<VT>{rv, dinv, pp, beta},
                                  [&](int row, VT v) {
                                      const VT pk = p_next(dinv ? __ldg(dinv + row) : VT(1), rv[row], pp[row], beta);
                                      pc[row] = pk;

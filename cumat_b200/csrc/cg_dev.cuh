@@ -184,6 +184,65 @@ __device__ __forceinline__ void cta_rows_seg(const InstMatrix<MT, FMT>& A, int s
     }
 }
 
+// (A x) for the four consecutive rows i .. i+3 (local, i a multiple of 4) of
+// one slice of the sliced layout: per entry slot one 16-byte index load and
+// one 4-value load cover the four rows (a warp's eight lanes per slice read
+// whole 128-byte lines), and the slots of a step are all loaded before the
+// first gather. Rows sum their entries in entry order.
+template <typename VT, typename MT, typename XF>
+__device__ __forceinline__ void sell_rows4(const RowMat<MT>& A, int s, int i, const XF& xf, VT (&out)[4]) {
+    // slots per step: fewer for 8-byte values (register budget)
+    constexpr int S = sizeof(MT) == 8 ? 2 : 4;
+    const int sl = __ldg(A.sys_slice0 + s) + (i >> 5);
+    const int64_t base = __ldg(A.slice_off + sl) + (i & 31);
+    const int w = __ldg(A.slice_w + sl);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) out[q] = VT(0);
+    for (int j0 = 0; j0 < w; j0 += S) {
+        int4 c[S];
+        Vals4<MT> v[S];
+#pragma unroll
+        for (int jj = 0; jj < S; ++jj) {
+            if (j0 + jj < w) {
+                const int64_t o = base + static_cast<int64_t>(j0 + jj) * 32;
+                c[jj] = __ldg(reinterpret_cast<const int4*>(A.col + o));
+                v[jj].load(A.val + o);
+            }
+        }
+#pragma unroll
+        for (int jj = 0; jj < S; ++jj) {
+            if (j0 + jj < w) {
+                out[0] += mval<VT>(v[jj].v[0]) * xf(c[jj].x);
+                out[1] += mval<VT>(v[jj].v[1]) * xf(c[jj].y);
+                out[2] += mval<VT>(v[jj].v[2]) * xf(c[jj].z);
+                out[3] += mval<VT>(v[jj].v[3]) * xf(c[jj].w);
+            }
+        }
+    }
+}
+
+// Thread-per-4-rows product over the local rows [i0, i0 + n) of system s (i0 a
+// multiple of 32; the range ends at a multiple of 4 or at the system's end):
+// thread t takes rows i0 + 4 t .. + 3, then i0 + 4 (t + blockDim.x) ...;
+// f(global row, value) per row in increasing order per thread. The sliced
+// layout (CSR patterns) only; ELLPACK patterns take cta_rows_seg.
+template <typename VT, typename MT, int FMT, typename XF, typename F>
+__device__ __forceinline__ void cta_rows4_seg(const InstMatrix<MT, FMT>& A, int s, int r0, int i0, int n, const XF& xf,
+                                              F&& f) {
+    if (!A.rm.slice_off) {
+        cta_rows_seg<VT>(A, s, r0, i0, n, xf, f);
+        return;
+    }
+    const int end = i0 + n;
+    for (int ib = i0 + 4 * threadIdx.x; ib < end; ib += 4 * blockDim.x) {
+        VT v[4];
+        sell_rows4<VT>(A.rm, s, ib, xf, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (ib + q < end) f(r0 + ib + q, v[q]);
+    }
+}
+
 // Applies the product to the rows [r0, r0 + n) of one system with the whole
 // CTA: warp w takes the 32-row blocks w, w + W, ... so thread t always owns
 // rows r0 + t + k * blockDim.x. f(row, value) is called on the owning lane.

@@ -174,6 +174,50 @@ __device__ __forceinline__ SegInfo seg_info(const SolveArgs<VT, MT>& a, int b, i
     return g;
 }
 
+// Four consecutive vector elements moved with 16-byte accesses (float4, or
+// two double2).
+template <typename VT> struct V4;
+template <> struct V4<float> {
+    float v[4];
+    __device__ __forceinline__ void load(const float* p) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+    __device__ __forceinline__ void store(float* p) const { *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]); }
+};
+template <> struct V4<double> {
+    double v[4];
+    __device__ __forceinline__ void load(const double* p) {
+        const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    __device__ __forceinline__ void store(double* p) const {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+};
+
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Row loop of a segment [r0, r1) for the vector passes: when every pointer in
+// `ptrs` is 16-byte aligned at r0, thread t takes the 4-row chunks
+// r0 + 4 (t + k T) through body4(i), the rest (or everything) goes row by row
+// through body1(i).
+template <int NP, typename F4, typename F1>
+__device__ __forceinline__ void seg_rows_vec(int r0, int r1, const void* const (&ptrs)[NP], F4&& body4, F1&& body1) {
+    bool vec = true;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) vec = vec && (ptrs[j] == nullptr || aligned16(ptrs[j]));
+    int tail = r0;
+    if (vec) {
+        const int n4 = (r1 - r0) >> 2;
+#pragma unroll 2
+        for (int c = threadIdx.x; c < n4; c += blockDim.x) body4(r0 + 4 * c);
+        tail = r0 + 4 * n4;
+    }
+    for (int i = tail + threadIdx.x; i < r1; i += blockDim.x) body1(i);
+}
+
 #define CMCG_FOR_SEGMENTS(a)                                                     \
     for (int b_ = 0; b_ < (a).ob; ++b_)                                          \
         for (int seg_ = (a).cta_seg0[blockIdx.x]; seg_ < (a).cta_seg0[blockIdx.x + 1]; ++seg_)
@@ -186,6 +230,7 @@ __device__ __forceinline__ SegInfo seg_info(const SolveArgs<VT, MT>& a, int b, i
 constexpr int kCoopMaxInst = 16;
 constexpr int kCoopThreads = 1024;
 constexpr int kCoopMaxSegs = 32;   // segments one CTA may own (cached in shared memory)
+constexpr int kCoopMaxRows = 1 << 19;   // largest system for which the cooperative launch is chosen
 
 template <typename VT, typename MT, int FMT>
 cmcg_status coop_cg_occupancy(int* ctas_per_sm);

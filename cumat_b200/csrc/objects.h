@@ -77,6 +77,9 @@ struct cmcg_pattern_s {
     int32_t* d_spmv_tiles = nullptr;
     // sliced ELLPACK copy for the CG kernels (CSR only, built on first use)
     SellPlan sell;
+    // stand-alone product kernel picked by timing on first use, per
+    // [value dtype][vector dtype] (-1: not tuned yet)
+    int8_t spmv_choice[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
     int64_t systems_version = 0;      // incremented by cmcg_pattern_set_systems
     int refs = 1;
 };

@@ -10,11 +10,13 @@
 //  cmcg_sddmm         replaces the sparse outer product on a pattern
 //                     (SparseProductEvaluation.h:16-37 + SparseEvaluation.h:15-34)
 //
-// Design: CSR rows are processed in 32-row blocks per warp with 16-byte loads
-// of the block's contiguous entries (warp_csr_rows); ELLPACK is thread per row
-// over the column-major slabs. Reductions are warp shuffles, one partial per
-// CTA and a single deterministic combine by the last CTA of each batch (ticket
-// counter, no spinning).
+// Design: CSR is thread per row with the row's index and value loads issued
+// before its gathers (bulk-staged tiles and warp row blocks are variants);
+// ELLPACK is four rows per thread with 16-byte loads of the column-major slabs.
+// The first product of a pattern picks among the variants that add in the same
+// order by timing them (launch_spmv). Reductions are warp shuffles, one
+// partial per CTA and a single deterministic combine by the last CTA of each
+// batch (ticket counter, no spinning).
 
 #include <algorithm>
 #include <cstdlib>
@@ -33,13 +35,14 @@ namespace {
 constexpr int kSpmvThreads = 256;
 
 // Stand-alone product kernels: 0 = row-unrolled CSR / four-rows-per-thread
-// ELLPACK (default), 1 = warp row-block CSR / thread-per-row ELLPACK,
-// 2 = bulk-staged CSR / four-rows-per-thread ELLPACK. Chosen once per process
-// from CUMAT_SPMV_VARIANT (a tuning and comparison knob).
+// ELLPACK, 1 = warp row-block CSR / thread-per-row ELLPACK, 2 = bulk-staged
+// CSR / four-rows-per-thread ELLPACK. CUMAT_SPMV_VARIANT forces one for the
+// whole process (a comparison knob); unset, each pattern picks by timing on
+// its first product (see launch_spmv).
 int spmv_variant() {
     static const int v = [] {
         const char* e = std::getenv("CUMAT_SPMV_VARIANT");
-        return e ? std::atoi(e) : 0;
+        return e ? std::atoi(e) : -1;
     }();
     return v;
 }
@@ -140,8 +143,8 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_rows(const int32_t* _
 // flight per CTA. Threads then take rows (thread per row), read their entries
 // from shared memory, gather x through the read-only path and write y. A tile
 // that is one row longer than kTileNnz is summed by the whole CTA from global
-// memory. (Kept as a selectable variant: with two stages the copies stall
-// behind the gathers, so the row-unrolled kernel below is the default.)
+// memory. (A variant the autotuner may pick: with two stages the copies often
+// stall behind the gathers, and the row-unrolled kernel above wins.)
 
 constexpr int kTileRows = 512;
 constexpr int kTileNnz = 2048;
@@ -408,7 +411,7 @@ void launch_ell4(cmcg_matrix A, int blocks, const MT* vals, const VT* xv, int32_
 }
 
 template <typename MT, typename VT>
-cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode) {
+cmcg_status launch_spmv_variant(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode, int variant) {
     cmcg_pattern p = A->pat;
     cmcg_ctx ctx = p->ctx;
     const int32_t ob = std::max(A->batches, xb);
@@ -416,7 +419,6 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     const VT* xv = static_cast<const VT*>(x);
     VT* yv = static_cast<VT*>(y);
     const int max_blocks = ctx->sm_count * 8;
-    const int variant = spmv_variant();
     if (p->format == CMCG_CSR && variant == 2) {
         if (mode == CMCG_ASSIGN) return launch_csr_tma<MT, VT, CMCG_ASSIGN>(A, xv, xb, yv, ob);
         if (mode == CMCG_ADD) return launch_csr_tma<MT, VT, CMCG_ADD>(A, xv, xb, yv, ob);
@@ -618,6 +620,59 @@ cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub,
 }  // namespace
 
 // Internal entry used by the solver (device pointers, no validation).
+// Autotuner of the stand-alone product: among the kernels that add every
+// row's products in the same order (CSR: row-unrolled, bulk-staged; ELLPACK:
+// four rows per thread, thread per row), so that the choice never changes a
+// result, it times each candidate on the caller's operands (one warm-up and
+// three timed launches, CUDA events on the context stream) the first time a
+// pattern is multiplied with a given value / vector type, and keeps the
+// fastest in the pattern. Tuning needs an assigning product (the candidates
+// write y) and a stream that is not being captured; otherwise the default
+// kernel runs untuned.
+template <typename MT, typename VT>
+cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode) {
+    const int forced = spmv_variant();
+    if (forced >= 0) return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, forced);
+    cmcg_pattern p = A->pat;
+    int8_t& choice = p->spmv_choice[DT<MT>::id][DT<VT>::id];
+    if (choice >= 0) return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, choice);
+    cudaStream_t st = p->ctx->stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (mode != CMCG_ASSIGN || cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+        return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, 0);
+    const int cands[2] = {0, p->format == CMCG_CSR ? 2 : 1};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CMCG_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(CMCG_ERR_CUDA, "spmv autotune: event creation failed");
+    }
+    float best = 0.0f;
+    int pick = cands[0];
+    cmcg_status rc = CMCG_OK;
+    for (int c : cands) {
+        if ((rc = launch_spmv_variant<MT, VT>(A, x, xb, y, mode, c)) != CMCG_OK) break;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3 && rc == CMCG_OK; ++r) rc = launch_spmv_variant<MT, VT>(A, x, xb, y, mode, c);
+        cudaEventRecord(e1, st);
+        float ms = 0.0f;
+        if (rc != CMCG_OK || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            if (rc == CMCG_OK) rc = fail(CMCG_ERR_CUDA, "spmv autotune: timing failed");
+            break;
+        }
+        if (c == cands[0] || ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != CMCG_OK) return rc;
+    choice = static_cast<int8_t>(pick);
+    // the last candidate's output is in y; rerun the pick if it was another one
+    return pick == cands[1] ? CMCG_OK : launch_spmv_variant<MT, VT>(A, x, xb, y, mode, pick);
+}
+
 cmcg_status spmv_dispatch(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t xb, void* y, int32_t mode) {
     if (vec_dtype == CMCG_F32) {
         switch (A->dtype) {

@@ -30,10 +30,11 @@ def test_kat_csr_product(cuda):
     k = KAT["spmv_csr"]
     A = cm.SparseMatrix(_csr_pattern(k)).setData(np.array(k["values"], np.float32))
     x = torch.tensor(k["x"], dtype=torch.float32, device=cuda)
+    y0 = (A * x).cpu().tolist()                     # first product: kernel picked by timing
     before = cm.launch_count()
     y = A * x
-    assert cm.launch_count() - before == 1          # one kernel per product
-    assert y.cpu().tolist() == k["y"]
+    assert cm.launch_count() - before == 1          # one kernel per product afterwards
+    assert y.cpu().tolist() == k["y"] == y0
     k2 = KAT["spmv_csr_scaled_matrix"]
     A2 = cm.SparseMatrix(_csr_pattern(k)).setData(np.array(k["values"], np.float32) * k2["scale"])
     assert (A2 * x).cpu().tolist() == k2["y"]
@@ -194,3 +195,23 @@ def test_invalid_patterns_raise(cuda):
     p = cm.SparsityPattern.csr(4, 4, [0, 1, 2, 3, 4], [0, 2, 1, 3])
     with pytest.raises(cm.CuMatError):
         p.set_systems([0, 2, 4])                                # (1, 2) couples two systems
+
+
+@pytest.mark.parametrize("fmt", ["csr", "ell"])
+def test_autotuned_product_is_deterministic(cuda, fmt):
+    # the first product times the candidate kernels; they add every row in the
+    # same order, so the tuned product gives the same bits as the first one
+    cm = _cm()
+    pr = P.poisson2d(300, 4)
+    vals = (pr.val * P.uniform(5, pr.nnz, 0.5, 1.5)).astype(np.float32)
+    if fmt == "csr":
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(vals)
+    else:
+        idx, ev = P.csr_to_ell(pr.n, pr.row_ptr, pr.col, vals)
+        A = cm.SparseMatrix(cm.SparsityPattern.ell(pr.n, pr.n, idx)).setData(ev)
+    x = torch.from_numpy(pr.b).to(cuda)
+    y1 = (A * x).cpu().numpy()
+    y2 = (A * x).cpu().numpy()
+    assert np.array_equal(y1, y2)
+    yo = O.spmv_csr(pr.n, pr.n, pr.row_ptr, pr.col, vals, pr.b)[0]
+    assert np.allclose(y1, yo, rtol=1e-6, atol=1e-6 * np.abs(yo).max())
