@@ -912,6 +912,28 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
     }
 }
 
+// q[k] = (S A S p)[tid + k T] for the first NK row slots from the diagonal
+// layout (vp[d]: value of diagonal d at this thread's first row, po[d]: p index
+// of that row plus the diagonal's offset; later slots are immediate offsets),
+// entries added in ascending offset order; pq += p[i] q[i] in slot order.
+template <int NK, int ND, typename MI>
+__device__ __forceinline__ void dia_rows(const MI* const (&vp)[ND], const int (&po)[ND], const float* P, int n, int tid,
+                                         float (&q)[kSmemNK], float& pq) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        const int i = tid + k * kSmemThreads;
+        float acc = 0.0f;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const float v = i < n ? mval<float>(vp[d][k * kSmemThreads]) : 0.0f;
+            const float pv = i < n ? P[po[d] + k * kSmemThreads] : 0.0f;
+            acc = fmaf(v, pv, acc);   // the fused multiply-add of the sliced-layout rows
+        }
+        q[k] = i < n ? acc : 0.0f;
+        if (i < n) pq += P[i] * acc;
+    }
+}
+
 template <typename MI, typename MO>
 struct MixArgs {
     int32_t rows, n_sys, ob, mb;
@@ -932,6 +954,12 @@ struct MixArgs {
     int32_t max_updates;
     float delta;
     InstState st;
+    // diagonal layout of the scaled inner values (kernels built with ND > 0)
+    const MI* vdia;         // [mb][vdia_stride]
+    int64_t vdia_stride;
+    const int64_t* dia_base;   // n_sys
+    const int32_t* dia_off;    // n_sys * kDiaMax
+    int32_t margin;            // largest |offset|: zero halo around p in shared memory
 };
 
 // Mixed precision with reliable updates on the compact layout. The inner FP32
@@ -940,16 +968,23 @@ struct MixArgs {
 // FP64 parts use the unscaled values: x += S xh at every fold and the inner
 // residual is S (b - A x). Residual replacement as in k_reliable_smem, the
 // trigger compared in the scaled norm.
-template <typename MI, typename MO>
+// ND > 0: the inner product reads the scaled values in the diagonal layout
+// (ND diagonals per system): row i sums v_d[i] * p[i + offset_d] over the
+// diagonals in ascending offset order (the row's CSR order; absent entries are
+// zeros), with no column index loads, and p carries a zero halo of `margin`
+// entries on both sides in shared memory. The FP64 residual keeps the compact
+// sliced layout.
+template <typename MI, typename MO, int ND>
 __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
     extern __shared__ __align__(16) float smf[];
     __shared__ SliceEnt tab[32][kSmemNK];
     __shared__ float red[2 * (kSmemThreads / 32)];
     __shared__ double red64[2 * (kSmemThreads / 32)];
     __shared__ int slot;
-    float* P = smf;
-    float* R = smf + nmax;
-    float* XH = smf + 2 * nmax;
+    const int M = ND > 0 ? a.margin : 0;
+    float* P = smf + M;
+    float* R = smf + nmax + 2 * M;
+    float* XH = R + nmax;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n_inst = a.n_sys * a.ob;
     const float d2 = a.delta * a.delta;
@@ -966,6 +1001,22 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         const double* sv = a.s + (a.mb == 1 ? 0 : vo) + r0;
         const double* bv = a.b + (a.b_b == 1 ? 0 : vo) + r0;
         double* x = a.x + vo + r0;
+        // diagonal layout: per diagonal the value pointer and the p index of
+        // this thread's first row (later row slots are immediate offsets)
+        const MI* vp[ND > 0 ? ND : 1] = {};
+        int po[ND > 0 ? ND : 1] = {};
+        if constexpr (ND > 0) {
+            const MI* vd = a.vdia + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vdia_stride) + __ldg(a.dia_base + s) + tid;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                vp[d] = vd + static_cast<int64_t>(d) * n;
+                po[d] = tid + __ldg(a.dia_off + s * kDiaMax + d);
+            }
+            for (int t = tid; t < M; t += kSmemThreads) {
+                P[-1 - t] = 0.0f;
+                P[n + t] = 0.0f;
+            }
+        }
         __syncthreads();   // slice table ready
         float q[kSmemNK];
         double acc[1] = {0.0};
@@ -1003,17 +1054,31 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         while (status == ST_RUNNING) {
             if (it >= maxit || updates >= a.max_updates) { status = CMCG_SOLVE_MAX_ITER; break; }
             float pq[1] = {0.0f};
-            // two row slots at a time (slices past the system have width 0)
+            if constexpr (ND > 0) {
+                // straight-line code over the system's row slots (no branch
+                // between slots, so later slots' loads can issue early)
+                switch ((n + kSmemThreads - 1) / kSmemThreads) {   // row slots of the system (uniform)
+#define CMCG_DIA_ROWS(K) \
+    case K: dia_rows<K>(vp, po, P, n, tid, q, pq[0]); break;
+                    CMCG_DIA_ROWS(1) CMCG_DIA_ROWS(2) CMCG_DIA_ROWS(3) CMCG_DIA_ROWS(4) CMCG_DIA_ROWS(5)
+                    CMCG_DIA_ROWS(6) CMCG_DIA_ROWS(7) CMCG_DIA_ROWS(8) CMCG_DIA_ROWS(9) CMCG_DIA_ROWS(10)
+                    CMCG_DIA_ROWS(11) CMCG_DIA_ROWS(12) CMCG_DIA_ROWS(13) CMCG_DIA_ROWS(14) CMCG_DIA_ROWS(15)
+                    default: dia_rows<16>(vp, po, P, n, tid, q, pq[0]);
+#undef CMCG_DIA_ROWS
+                }
+            } else {
+                // two row slots at a time (slices past the system have width 0)
 #pragma unroll
-            for (int k = 0; k < kSmemNK; k += 2) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i0 = tid + k * kSmemThreads, i1 = i0 + kSmemThreads;
-                float q0, q1;
-                fast_rows2<float>(a.c.col16, vin, tab[warp][k], tab[warp][k + 1], lane, LocalX<float>{P}, q0, q1);
-                q[k] = i0 < n ? q0 : 0.0f;
-                q[k + 1] = i1 < n ? q1 : 0.0f;
-                if (i0 < n) pq[0] += P[i0] * q[k];
-                if (i1 < n) pq[0] += P[i1] * q[k + 1];
+                for (int k = 0; k < kSmemNK; k += 2) {
+                    if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
+                    const int i0 = tid + k * kSmemThreads, i1 = i0 + kSmemThreads;
+                    float q0 = 0.0f, q1 = 0.0f;
+                    fast_rows2<float>(a.c.col16, vin, tab[warp][k], tab[warp][k + 1], lane, LocalX<float>{P}, q0, q1);
+                    q[k] = i0 < n ? q0 : 0.0f;
+                    q[k + 1] = i1 < n ? q1 : 0.0f;
+                    if (i0 < n) pq[0] += P[i0] * q[k];
+                    if (i1 < n) pq[0] += P[i1] * q[k + 1];
+                }
             }
             block_sum<float, 1>(pq, red);
             const float alpha = rz / pq[0];
@@ -1131,6 +1196,23 @@ __global__ void k_jacobi_scale(const int32_t* __restrict__ rp, const int32_t* __
             for (int k = rp[r]; k < rp[r + 1]; ++k)
                 if (ci[k] == r) { d = mval<double>(vals[b * vstride + k]); break; }
         out[it] = d > 0.0 ? 1.0 / sqrt(d) : 1.0;
+    }
+}
+
+// Scaled values in the diagonal layout: dst[b][pos[k]] = a_k * s_row * s_col for
+// every CSR entry k (thread per row); slots without an entry stay zero.
+template <typename MT>
+__global__ void k_scale_dia(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const MT* __restrict__ vals,
+                            int64_t vstride, const int32_t* __restrict__ pos, const double* __restrict__ sc, int32_t rows,
+                            int32_t mb, MT* __restrict__ dst, int64_t dstride) {
+    const int64_t items = static_cast<int64_t>(rows) * mb;
+    for (int64_t it = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(it / rows);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * rows);
+        const double* sb = sc + static_cast<int64_t>(b) * rows;
+        for (int k = rp[r]; k < rp[r + 1]; ++k)
+            dst[b * dstride + pos[k]] = from_f64<MT>(mval<double>(vals[b * vstride + k]) * sb[r] * sb[ci[k]]);
     }
 }
 
@@ -1802,6 +1884,12 @@ struct cmcg_solver_s {
     double* mix_s = nullptr;
     int64_t mix_version = -1, mix_plan_id = -1;
     int32_t mix_dtype = -1;
+    // the same scaled values in the pattern's diagonal layout, when it has one
+    bool dia_kernels = true;  // CUMAT_CG_DIA=0 keeps the sliced layout
+    void* dia_vals = nullptr;
+    int64_t dia_stride = 0;
+    int64_t dia_version = -1, dia_plan_id = -1;
+    int32_t dia_dtype = -1;
     InstState st{};
     int32_t st_inst = 0;
     // graph cache of the grid path
@@ -2035,6 +2123,10 @@ cmcg_status allow_smem(K kern, size_t bytes) {
 
 inline int smem_rows(int32_t max_rows) { return (max_rows + 3) / 4 * 4; }
 
+// dynamic shared memory the diagonal-layout kernel may use (the opt-in
+// maximum per CTA minus the kernel's static arrays, with room to spare)
+constexpr size_t kDiaSmemLimit = 216 * 1024;
+
 // Compact sliced layout available for the fast shared-memory kernels?
 inline bool compact_ok(cmcg_solver s) {
     const cmcg_pattern p = s->A->pat;
@@ -2085,6 +2177,42 @@ cmcg_status ensure_mix(cmcg_solver s) {
     s->mix_version = A->version;
     s->mix_plan_id = S.plan_id;
     s->mix_dtype = A->dtype;
+    return CMCG_OK;
+}
+
+// Scaled inner values in the pattern's diagonal layout (after ensure_mix);
+// false when the pattern has no diagonal plan.
+cmcg_status ensure_dia_vals(cmcg_solver s, bool* ok) {
+    *ok = false;
+    cmcg_matrix A = s->A;
+    cmcg_pattern p = A->pat;
+    CMCG_TRY(ensure_dia(p));
+    const DiaPlan& D = p->dia;
+    if (!D.ok) return CMCG_OK;
+    if (!(s->dia_vals && s->dia_version == A->version && s->dia_plan_id == D.plan_id && s->dia_dtype == A->dtype)) {
+        cmcg_ctx ctx = p->ctx;
+        dev_free(s->dia_vals);
+        s->dia_vals = nullptr;
+        s->dia_stride = (D.n_slots + 7) / 8 * 8 + 8;
+        const size_t bytes = static_cast<size_t>(s->dia_stride) * A->batches * dtype_size(A->dtype);
+        CMCG_TRY(dev_alloc(&s->dia_vals, bytes));
+        CMCG_CUDA(cudaMemsetAsync(s->dia_vals, 0, bytes, ctx->stream));
+        const int blocks = ctx->sm_count * 8;
+#define CMCG_SCALE_DIA(MT)                                                                                              \
+    k_scale_dia<MT><<<blocks, 256, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, static_cast<const MT*>(A->d_vals), A->stride, \
+                                                     D.d_pos, s->mix_s, p->rows, A->batches, static_cast<MT*>(s->dia_vals), \
+                                                     s->dia_stride)
+        if (A->dtype == CMCG_F32) CMCG_SCALE_DIA(float);
+        else if (A->dtype == CMCG_BF16) CMCG_SCALE_DIA(__nv_bfloat16);
+        else CMCG_SCALE_DIA(double);
+#undef CMCG_SCALE_DIA
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        s->dia_version = A->version;
+        s->dia_plan_id = D.plan_id;
+        s->dia_dtype = A->dtype;
+    }
+    *ok = true;
     return CMCG_OK;
 }
 
@@ -2380,9 +2508,28 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         m.st = s->st;
         const int nmax = smem_rows(s->max_sys_rows);
         const size_t sm = smem_bytes(nmax);
-        CMCG_TRY(allow_smem(k_mixed_fast<MI, MO>, sm));
         const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
-        k_mixed_fast<MI, MO><<<grid, kSmemThreads, sm, ctx->stream>>>(m, nmax);
+        bool dia = false;
+        if (s->dia_kernels) CMCG_TRY(ensure_dia_vals(s, &dia));
+        // the zero halo of p must fit next to the vectors in shared memory
+        const size_t sm_dia = dia ? sm + 2 * sizeof(float) * static_cast<size_t>(p->dia.margin) : 0;
+        if (dia && sm_dia <= kDiaSmemLimit) {
+            m.vdia = static_cast<const MI*>(s->dia_vals);
+            m.vdia_stride = s->dia_stride;
+            m.dia_base = p->dia.d_sys_base;
+            m.dia_off = p->dia.d_sys_off;
+            m.margin = p->dia.margin;
+            if (p->dia.max_nd == 5) {
+                CMCG_TRY(allow_smem(k_mixed_fast<MI, MO, 5>, sm_dia));
+                k_mixed_fast<MI, MO, 5><<<grid, kSmemThreads, sm_dia, ctx->stream>>>(m, nmax);
+            } else {
+                CMCG_TRY(allow_smem(k_mixed_fast<MI, MO, 7>, sm_dia));
+                k_mixed_fast<MI, MO, 7><<<grid, kSmemThreads, sm_dia, ctx->stream>>>(m, nmax);
+            }
+        } else {
+            CMCG_TRY(allow_smem(k_mixed_fast<MI, MO, 0>, sm));
+            k_mixed_fast<MI, MO, 0><<<grid, kSmemThreads, sm, ctx->stream>>>(m, nmax);
+        }
         count_launch();
         CMCG_CHECK_LAUNCH();
         s->last_inst = n_inst;
@@ -2647,6 +2794,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     // default tolerance: epsilon of the scalar type (IterativeSolverBase.h:131)
     s->tol = (A->dtype == CMCG_F64) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
     if (const char* e = std::getenv("CUMAT_CG_FAST")) s->fast_kernels = std::atoi(e) != 0;
+    if (const char* e = std::getenv("CUMAT_CG_DIA")) s->dia_kernels = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);
     if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);
@@ -2675,7 +2823,8 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
                     static_cast<void*>(s->d_sys_seg0), static_cast<void*>(s->d_cseg_t0), static_cast<void*>(s->d_cseg_t1),
                     static_cast<void*>(s->d_cseg_sys), static_cast<void*>(s->d_ccta_seg0),
                     static_cast<void*>(s->d_csys_seg0), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
-                    s->st_ws, static_cast<void*>(s->counters), s->mix_vals, static_cast<void*>(s->mix_s)})
+                    s->st_ws, static_cast<void*>(s->counters), s->mix_vals, static_cast<void*>(s->mix_s),
+                    s->dia_vals})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);
     cmcg_matrix A = s->A;

@@ -50,6 +50,26 @@ struct SellPlan {
     int64_t plan_id = 0;              // changes when the systems change
 };
 
+// Diagonal (DIA) copy of a CSR pattern whose systems each have at most
+// kDiaMax distinct column offsets col - row (stencils on structured grids,
+// banded matrices): system s stores diagonal d (offset sys_off[s][d], sorted
+// ascending, padded with offset 0) of its local row i at slot
+// sys_base[s] + d * n_s + i; entries missing from a row hold value 0. Feeds
+// the mixed-precision persistent kernel, whose rows then need no column
+// indices.
+constexpr int kDiaMax = 8;
+struct DiaPlan {
+    bool built = false;
+    bool ok = false;            // every system has at most kDiaMax offsets
+    int32_t max_nd = 0;         // diagonals stored per system (5 or 7)
+    int32_t margin = 0;         // largest |offset|
+    int64_t n_slots = 0;
+    int32_t* d_pos = nullptr;       // per CSR entry: its slot
+    int64_t* d_sys_base = nullptr;  // n_sys
+    int32_t* d_sys_off = nullptr;   // n_sys * kDiaMax
+    int64_t plan_id = 0;            // changes when the systems change
+};
+
 // Sparsity pattern. CSR: row_ptr (rows+1) + col_idx (nnz), the reference's JA /
 // IA (cuMat/src/SparseMatrixBase.h:89-147). ELLPACK: column-major indices with
 // rows padded to a multiple of 4 ([width][rows_pad], -1 padding), the
@@ -77,6 +97,8 @@ struct cmcg_pattern_s {
     int32_t* d_spmv_tiles = nullptr;
     // sliced ELLPACK copy for the CG kernels (CSR only, built on first use)
     SellPlan sell;
+    // diagonal copy for the mixed-precision kernel (CSR only, built on first use)
+    DiaPlan dia;
     // stand-alone product kernel picked by timing on first use, per
     // [value dtype][vector dtype] (-1: not tuned yet)
     int8_t spmv_choice[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
@@ -116,4 +138,7 @@ cmcg_status convert(cmcg_ctx ctx, int src_dt, const void* src, int dst_dt, void*
 cmcg_status ensure_sell(cmcg_pattern p);
 cmcg_status ensure_sell_values(cmcg_matrix m);
 void free_sell(SellPlan& s);
+// builds the pattern's diagonal plan (CSR; dia.ok tells whether it applies)
+cmcg_status ensure_dia(cmcg_pattern p);
+void free_dia(DiaPlan& d);
 }  // namespace cmcg

@@ -84,6 +84,7 @@ void pattern_release(cmcg_pattern p) {
     dev_free(p->d_row_off);
     dev_free(p->d_spmv_tiles);
     free_sell(p->sell);
+    free_dia(p->dia);
     cmcg_ctx c = p->ctx;
     delete p;
     ctx_release(c);
@@ -420,6 +421,8 @@ cmcg_status cmcg_pattern_set_systems(cmcg_pattern p, int64_t n_sys, const int64_
     cudaStreamSynchronize(p->ctx->stream);
     free_sell(p->sell);
     p->sell.plan_id++;
+    free_dia(p->dia);
+    p->dia.plan_id++;
     p->systems_version++;
     std::vector<int32_t> h(row_off, row_off + n_sys + 1);
     dev_free(p->d_row_off);

@@ -9,6 +9,7 @@
 // gathered into it on the device whenever the matrix values change.
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -108,6 +109,87 @@ cmcg_status ensure_sell(cmcg_pattern p) {
             return st;
         }
     }
+    return CMCG_OK;
+}
+
+void free_dia(DiaPlan& d) {
+    dev_free(d.d_pos);
+    dev_free(d.d_sys_base);
+    dev_free(d.d_sys_off);
+    const int64_t id = d.plan_id;
+    d = DiaPlan();
+    d.plan_id = id;
+}
+
+cmcg_status ensure_dia(cmcg_pattern p) {
+    DiaPlan& D = p->dia;
+    if (p->format != CMCG_CSR || D.built) return CMCG_OK;
+    D.built = true;   // a failed or inapplicable plan is not retried until the systems change
+    const auto& rp = p->h_row_ptr;
+    const auto& ci = p->h_col;
+    const auto& ro = p->row_off;
+    const int64_t n_sys = static_cast<int64_t>(ro.size()) - 1;
+    std::vector<int32_t> off(static_cast<size_t>(n_sys) * kDiaMax, 0);
+    std::vector<int64_t> base(n_sys);
+    std::vector<int32_t> nd(n_sys);
+    int64_t slots = 0;
+    int32_t max_nd = 0, margin = 0;
+    for (int64_t s = 0; s < n_sys; ++s) {
+        std::vector<int32_t> o;
+        for (int64_t r = ro[s]; r < ro[s + 1]; ++r) {
+            for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
+                const int32_t d = static_cast<int32_t>(ci[k] - r);
+                if (std::find(o.begin(), o.end(), d) == o.end()) {
+                    if (static_cast<int>(o.size()) == kDiaMax) return CMCG_OK;   // not diagonal-shaped: D.ok stays false
+                    o.push_back(d);
+                }
+            }
+        }
+        std::sort(o.begin(), o.end());
+        for (size_t j = 0; j < o.size(); ++j) {
+            off[static_cast<size_t>(s) * kDiaMax + j] = o[j];
+            margin = std::max(margin, std::abs(o[j]));
+        }
+        nd[s] = static_cast<int32_t>(o.size());
+        max_nd = std::max(max_nd, nd[s]);
+    }
+    // every system stores the same number of diagonals (5 or 7, the widths the
+    // kernel is built for); unused ones hold zeros
+    const int32_t nd_alloc = max_nd <= 5 ? 5 : max_nd <= 7 ? 7 : 0;
+    if (nd_alloc == 0) return CMCG_OK;
+    for (int64_t s = 0; s < n_sys; ++s) {
+        base[s] = slots;
+        slots += static_cast<int64_t>(nd_alloc) * (ro[s + 1] - ro[s]);
+    }
+    if (slots >= INT32_MAX) return CMCG_OK;
+    std::vector<int32_t> pos(static_cast<size_t>(p->nnz));
+    for (int64_t s = 0; s < n_sys; ++s) {
+        const int64_t n = ro[s + 1] - ro[s];
+        const int32_t* o = off.data() + s * kDiaMax;
+        for (int64_t r = ro[s]; r < ro[s + 1]; ++r) {
+            for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
+                const int32_t d = static_cast<int32_t>(std::find(o, o + nd[s], static_cast<int32_t>(ci[k] - r)) - o);
+                pos[k] = static_cast<int32_t>(base[s] + d * n + (r - ro[s]));
+            }
+        }
+    }
+    auto up = [](void** dptr, const void* h, size_t bytes) -> cmcg_status {
+        CMCG_TRY(dev_alloc(dptr, std::max<size_t>(bytes, 16)));
+        if (bytes) CMCG_CUDA(cudaMemcpy(*dptr, h, bytes, cudaMemcpyHostToDevice));
+        return CMCG_OK;
+    };
+    cmcg_status st;
+    if ((st = up(reinterpret_cast<void**>(&D.d_pos), pos.data(), pos.size() * 4)) != CMCG_OK ||
+        (st = up(reinterpret_cast<void**>(&D.d_sys_base), base.data(), base.size() * 8)) != CMCG_OK ||
+        (st = up(reinterpret_cast<void**>(&D.d_sys_off), off.data(), off.size() * 4)) != CMCG_OK) {
+        free_dia(D);
+        D.built = true;
+        return st;
+    }
+    D.n_slots = slots;
+    D.max_nd = nd_alloc;
+    D.margin = margin;
+    D.ok = true;
     return CMCG_OK;
 }
 

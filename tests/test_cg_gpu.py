@@ -309,6 +309,38 @@ def test_reliable_updates_vs_oracle_and_truth(cuda):
             assert np.linalg.norm(x[r0:r1] - xt) / np.linalg.norm(xt) < 1e-8
 
 
+@pytest.mark.parametrize("inner", [torch.float32, torch.bfloat16])
+def test_diagonal_layout_matches_sliced_layout(cuda, monkeypatch, inner):
+    # FV stencils have 5 column offsets per system: the mixed kernel reads the
+    # scaled values in the diagonal layout; with CUMAT_CG_DIA=0 it reads the
+    # sliced layout. Both add every row's products in the same order.
+    m = cm()
+    bt = P.fv2d_batch(40, 16, 128, 0.5, 23)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A = m.SparseMatrix(p, dtype=inner).setData(bt.val)
+    A64 = m.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
+    b64 = torch.from_numpy(bt.b.astype(np.float64)).to(cuda)
+    cg = m.ConjugateGradient(A)
+    x1 = cg.solve_refined(b64, outer=A64, outer_tol=1e-10, max_outer=200).cpu().numpy()
+    s1 = cg.system_stats()
+    monkeypatch.setenv("CUMAT_CG_DIA", "0")
+    cg0 = m.ConjugateGradient(A)
+    x0 = cg0.solve_refined(b64, outer=A64, outer_tol=1e-10, max_outer=200).cpu().numpy()
+    s0 = cg0.system_stats()
+    assert np.array_equal(s1["status"], s0["status"]) and np.array_equal(s1["iterations"], s0["iterations"])
+    assert np.array_equal(s1["outer"], s0["outer"]) and np.array_equal(x1, x0, equal_nan=True)
+    if inner == torch.bfloat16:
+        # BF16 values (8-bit mantissa) are too coarse for systems whose
+        # condition number exceeds ~2^8: the statuses report it, identically
+        return
+    assert np.all(s1["status"] == 0) and np.all(s1["error"] < 1e-10)
+    r = b64.cpu().numpy() - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x1)[0]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(bt.b[r0:r1]) < 1e-10
+
+
 def test_generic_kernels_match_oracle(cuda, monkeypatch):
     # CUMAT_CG_FAST=0 (read when a solver is created) selects the generic
     # shared-memory kernels: explicit Jacobi PCG inside the reliable updates
