@@ -30,6 +30,7 @@
 
 #include <type_traits>
 
+#include "cg_compact.cuh"
 #include "cg_dev.cuh"
 #include "cg_smem.cuh"
 #include "common.cuh"
@@ -150,13 +151,6 @@ __device__ int32_t cta_pcg(const InstMatrix<MT, FMT>& A, int sys, int r0, int n,
     return status;
 }
 
-__device__ __forceinline__ int fetch_item(int32_t* next, int* slot) {
-    if (threadIdx.x == 0) *slot = atomicAdd(next, 1);
-    __syncthreads();
-    const int item = *slot;
-    __syncthreads();
-    return item;
-}
 
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kPersistThreads) k_persistent_cg(SolveArgs<VT, MT> a) {
@@ -600,142 +594,9 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_reliable_smem(RefineArgs<MI
 }
 
 // ---------------------------------------------------------------------------
-// Fast shared-memory kernels over the compact sliced layout (CSR patterns whose
-// systems have at most 65536 rows): 16-bit system-local column indices, the
-// slice offsets / widths a warp visits cached in shared memory once per system
-// (no dependent global loads per row), 32-bit offsets.
+// Fast shared-memory kernels over the compact sliced layout (cg_compact.cuh;
+// the mixed-precision one is in cg_mixed.cu)
 // ---------------------------------------------------------------------------
-
-struct SliceEnt {
-    int32_t off;
-    int32_t w;
-};
-
-// tab[w][k]: slice w + 32 k of the system (local rows 32 (w + 32 k) ...), the
-// slice holding the rows tid + k * 1024 of warp w.
-__device__ __forceinline__ void load_slice_table(SliceEnt (*tab)[kSmemNK], const int32_t* __restrict__ off32,
-                                                 const int32_t* __restrict__ sw, int sl0, int nsl) {
-    for (int t = threadIdx.x; t < 32 * kSmemNK; t += blockDim.x) {
-        const int w = t / kSmemNK, k = t - (t / kSmemNK) * kSmemNK, sl = w + 32 * k;
-        tab[w][k] = sl < nsl ? SliceEnt{__ldg(off32 + sl0 + sl), __ldg(sw + sl0 + sl)} : SliceEnt{0, 0};
-    }
-}
-
-template <typename T>
-struct LocalX {
-    const T* p;
-    __device__ __forceinline__ T operator()(int c) const { return p[c]; }
-};
-
-// W entries of a row, fully unrolled: every load is the row's base pointer
-// plus an immediate offset; all loads issue before the first product; the
-// products are summed in entry order.
-template <int W, typename VT, typename MT, typename XF>
-__device__ __forceinline__ VT row_w(const uint16_t* __restrict__ c, const MT* __restrict__ v, const XF& xf) {
-    int ci[W];
-    MT vi[W];
-#pragma unroll
-    for (int j = 0; j < W; ++j) {
-        ci[j] = __ldg(c + 32 * j);
-        vi[j] = v[32 * j];
-    }
-    VT acc = VT(0);
-#pragma unroll
-    for (int j = 0; j < W; ++j) acc += mval<VT>(vi[j]) * xf(ci[j]);
-    return acc;
-}
-
-// Entries of the lane's row in one compact slice, summed in entry order.
-template <typename VT, typename MT, typename XF>
-__device__ __forceinline__ VT fast_row(const uint16_t* __restrict__ col, const MT* __restrict__ val, SliceEnt e, int lane,
-                                       const XF& xf) {
-    const uint16_t* c = col + e.off + lane;
-    const MT* v = val + e.off + lane;
-    switch (e.w) {   // warp-uniform: one slice per warp
-        case 0: return VT(0);
-        case 1: return row_w<1, VT>(c, v, xf);
-        case 2: return row_w<2, VT>(c, v, xf);
-        case 3: return row_w<3, VT>(c, v, xf);
-        case 4: return row_w<4, VT>(c, v, xf);
-        case 5: return row_w<5, VT>(c, v, xf);
-        case 6: return row_w<6, VT>(c, v, xf);
-        case 7: return row_w<7, VT>(c, v, xf);
-        case 8: return row_w<8, VT>(c, v, xf);
-        default: break;
-    }
-    VT acc = VT(0);
-    int j = 0;
-    for (; j + 4 <= e.w; j += 4) {
-        const int c0 = __ldg(c + 32 * j), c1 = __ldg(c + 32 * (j + 1)), c2 = __ldg(c + 32 * (j + 2)),
-                  c3 = __ldg(c + 32 * (j + 3));
-        const MT v0 = v[32 * j], v1 = v[32 * (j + 1)], v2 = v[32 * (j + 2)], v3 = v[32 * (j + 3)];
-        acc += mval<VT>(v0) * xf(c0);
-        acc += mval<VT>(v1) * xf(c1);
-        acc += mval<VT>(v2) * xf(c2);
-        acc += mval<VT>(v3) * xf(c3);
-    }
-    for (; j < e.w; ++j) acc += mval<VT>(v[32 * j]) * xf(__ldg(c + 32 * j));
-    return acc;
-}
-
-// Two rows of equal width W (the lane's rows in two slices): the 4 W index
-// and value loads of both rows issue before the first product, so the two
-// rows cost one memory latency instead of two; each row sums in entry order.
-template <int W, typename VT, typename MT, typename XF>
-__device__ __forceinline__ void row_w2(const uint16_t* __restrict__ c0, const MT* __restrict__ v0,
-                                       const uint16_t* __restrict__ c1, const MT* __restrict__ v1, const XF& xf, VT& q0,
-                                       VT& q1) {
-    int ci0[W], ci1[W];
-    MT vi0[W], vi1[W];
-#pragma unroll
-    for (int j = 0; j < W; ++j) {
-        ci0[j] = __ldg(c0 + 32 * j);
-        vi0[j] = v0[32 * j];
-        ci1[j] = __ldg(c1 + 32 * j);
-        vi1[j] = v1[32 * j];
-    }
-    VT a0 = VT(0), a1 = VT(0);
-#pragma unroll
-    for (int j = 0; j < W; ++j) {
-        a0 += mval<VT>(vi0[j]) * xf(ci0[j]);
-        a1 += mval<VT>(vi1[j]) * xf(ci1[j]);
-    }
-    q0 = a0;
-    q1 = a1;
-}
-
-// fast_row for the lane's rows in two slices (e1.w == 0: no second row).
-template <typename VT, typename MT, typename XF>
-__device__ __forceinline__ void fast_rows2(const uint16_t* __restrict__ col, const MT* __restrict__ val, SliceEnt e0,
-                                           SliceEnt e1, int lane, const XF& xf, VT& q0, VT& q1) {
-    if (e0.w == e1.w) {   // warp-uniform
-        const uint16_t* c0 = col + e0.off + lane;
-        const MT* v0 = val + e0.off + lane;
-        const uint16_t* c1 = col + e1.off + lane;
-        const MT* v1 = val + e1.off + lane;
-        switch (e0.w) {
-            case 0: q0 = q1 = VT(0); return;
-            case 3: row_w2<3>(c0, v0, c1, v1, xf, q0, q1); return;
-            case 4: row_w2<4>(c0, v0, c1, v1, xf, q0, q1); return;
-            case 5: row_w2<5>(c0, v0, c1, v1, xf, q0, q1); return;
-            default: break;
-        }
-        // wider rows only with 4-byte values (register budget of 1024-thread CTAs)
-        if constexpr (sizeof(MT) <= 4) {
-            if (e0.w == 6) { row_w2<6>(c0, v0, c1, v1, xf, q0, q1); return; }
-            if (e0.w == 7) { row_w2<7>(c0, v0, c1, v1, xf, q0, q1); return; }
-        }
-    }
-    q0 = fast_row<VT>(col, val, e0, lane, xf);
-    q1 = fast_row<VT>(col, val, e1, lane, xf);
-}
-
-struct CompactArgs {
-    const uint16_t* col16;
-    const int32_t* off32;
-    const int32_t* sw;
-    const int32_t* sys_slice0;
-};
 
 // Plain PCG (the reference's algorithm and stopping rule) on the compact layout.
 // p always lives in shared memory (it is gathered); r and x live there too when
@@ -907,276 +768,6 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_cg_fast(SolveArgs<VT, MT> a
             a.st.bb[inst] = static_cast<double>(bb);
             a.st.outer[inst] = 0;
             a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(static_cast<double>(rr) / static_cast<double>(bb));
-        }
-        __syncthreads();
-    }
-}
-
-// q[k] = (S A S p)[tid + k T] for the first NK row slots from the diagonal
-// layout (vp[d]: value of diagonal d at this thread's first row, po[d]: p index
-// of that row plus the diagonal's offset; later slots are immediate offsets),
-// entries added in ascending offset order; pq += p[i] q[i] in slot order.
-template <int NK, int ND, typename MI>
-__device__ __forceinline__ void dia_rows(const MI* const (&vp)[ND], const int (&po)[ND], const float* P, int n, int tid,
-                                         float (&q)[kSmemNK], float& pq) {
-#pragma unroll
-    for (int k = 0; k < NK; ++k) {
-        const int i = tid + k * kSmemThreads;
-        float acc = 0.0f;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-            const float v = i < n ? mval<float>(vp[d][k * kSmemThreads]) : 0.0f;
-            const float pv = i < n ? P[po[d] + k * kSmemThreads] : 0.0f;
-            acc = fmaf(v, pv, acc);   // the fused multiply-add of the sliced-layout rows
-        }
-        q[k] = i < n ? acc : 0.0f;
-        if (i < n) pq += P[i] * acc;
-    }
-}
-
-template <typename MI, typename MO>
-struct MixArgs {
-    int32_t rows, n_sys, ob, mb;
-    const int32_t* row_off;
-    const int32_t* order;
-    int32_t* next;
-    CompactArgs c;
-    const MI* vin;          // Jacobi-scaled inner values, sliced layout
-    int64_t vin_stride;
-    const MO* vout;         // unscaled outer values, sliced layout
-    int64_t vout_stride;
-    const double* s;        // scale 1/sqrt(a_ii) (or 1), [mb][rows]
-    const double* b;
-    int32_t b_b;
-    double* x;
-    double outer_tol;
-    int64_t max_inner;
-    int32_t max_updates;
-    float delta;
-    InstState st;
-    // diagonal layout of the scaled inner values (kernels built with ND > 0)
-    const MI* vdia;         // [mb][vdia_stride]
-    int64_t vdia_stride;
-    const int64_t* dia_base;   // n_sys
-    const int32_t* dia_off;    // n_sys * kDiaMax
-    int32_t margin;            // largest |offset|: zero halo around p in shared memory
-};
-
-// Mixed precision with reliable updates on the compact layout. The inner FP32
-// CG runs on the symmetrically Jacobi-scaled system S A S (S = diag(s)), which
-// is Jacobi PCG in exact arithmetic but needs no diagonal inside the loop; the
-// FP64 parts use the unscaled values: x += S xh at every fold and the inner
-// residual is S (b - A x). Residual replacement as in k_reliable_smem, the
-// trigger compared in the scaled norm.
-// ND > 0: the inner product reads the scaled values in the diagonal layout
-// (ND diagonals per system): row i sums v_d[i] * p[i + offset_d] over the
-// diagonals in ascending offset order (the row's CSR order; absent entries are
-// zeros), with no column index loads, and p carries a zero halo of `margin`
-// entries on both sides in shared memory. The FP64 residual keeps the compact
-// sliced layout.
-template <typename MI, typename MO, int ND>
-__global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
-    extern __shared__ __align__(16) float smf[];
-    __shared__ SliceEnt tab[32][kSmemNK];
-    __shared__ float red[2 * (kSmemThreads / 32)];
-    __shared__ double red64[2 * (kSmemThreads / 32)];
-    __shared__ int slot;
-    const int M = ND > 0 ? a.margin : 0;
-    float* P = smf + M;
-    float* R = smf + nmax + 2 * M;
-    float* XH = R + nmax;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int n_inst = a.n_sys * a.ob;
-    const float d2 = a.delta * a.delta;
-    for (;;) {
-        const int item = fetch_item(a.next, &slot);
-        if (item >= n_inst) return;
-        const int s = a.order[item / a.ob], bi = item % a.ob, inst = bi * a.n_sys + s;
-        const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
-        const int sl0 = __ldg(a.c.sys_slice0 + s), nsl = __ldg(a.c.sys_slice0 + s + 1) - sl0;
-        load_slice_table(tab, a.c.off32, a.c.sw, sl0, nsl);
-        const int64_t vo = static_cast<int64_t>(bi) * a.rows;
-        const MI* vin = a.vin + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vin_stride);
-        const MO* vout = a.vout + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vout_stride);
-        const double* sv = a.s + (a.mb == 1 ? 0 : vo) + r0;
-        const double* bv = a.b + (a.b_b == 1 ? 0 : vo) + r0;
-        double* x = a.x + vo + r0;
-        // diagonal layout: per diagonal the value pointer and the p index of
-        // this thread's first row (later row slots are immediate offsets)
-        const MI* vp[ND > 0 ? ND : 1] = {};
-        int po[ND > 0 ? ND : 1] = {};
-        if constexpr (ND > 0) {
-            const MI* vd = a.vdia + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vdia_stride) + __ldg(a.dia_base + s) + tid;
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                vp[d] = vd + static_cast<int64_t>(d) * n;
-                po[d] = tid + __ldg(a.dia_off + s * kDiaMax + d);
-            }
-            for (int t = tid; t < M; t += kSmemThreads) {
-                P[-1 - t] = 0.0f;
-                P[n + t] = 0.0f;
-            }
-        }
-        __syncthreads();   // slice table ready
-        float q[kSmemNK];
-        double acc[1] = {0.0};
-        float rz1[1] = {0.0f};
-#pragma unroll
-        for (int k = 0; k < kSmemNK; ++k) {
-            if (k * kSmemThreads >= n) break;
-            const int i = tid + k * kSmemThreads;
-            if (i < n) {
-                const double b_i = bv[i];
-                x[i] = 0.0;
-                const float rh = static_cast<float>(__ldg(sv + i) * b_i);
-                R[i] = rh;
-                P[i] = rh;
-                XH[i] = 0.0f;
-                acc[0] += b_i * b_i;
-                rz1[0] += rh * rh;
-            }
-        }
-        block_sum<double, 1>(acc, red64);
-        block_sum<float, 1>(rz1, red);
-        const double bb = acc[0];
-        const double thr = a.outer_tol * a.outer_tol * bb;
-        double rr64 = bb;
-        float rz = rz1[0];
-        float rmax = rz;            // scaled |r|^2 at the last replacement
-        float goal = static_cast<float>(thr / rr64) * rmax;   // scaled |r|^2 that would meet the target
-        int32_t status = ST_RUNNING, it = 0, updates = 0;
-        if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
-        else if (!finite_(bb)) status = CMCG_SOLVE_NON_FINITE;
-        else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
-        else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
-        const int64_t maxit = sys_max_iter(a.max_inner, n);
-        bool folded = true;
-        while (status == ST_RUNNING) {
-            if (it >= maxit || updates >= a.max_updates) { status = CMCG_SOLVE_MAX_ITER; break; }
-            float pq[1] = {0.0f};
-            if constexpr (ND > 0) {
-                // straight-line code over the system's row slots (no branch
-                // between slots, so later slots' loads can issue early)
-                switch ((n + kSmemThreads - 1) / kSmemThreads) {   // row slots of the system (uniform)
-#define CMCG_DIA_ROWS(K) \
-    case K: dia_rows<K>(vp, po, P, n, tid, q, pq[0]); break;
-                    CMCG_DIA_ROWS(1) CMCG_DIA_ROWS(2) CMCG_DIA_ROWS(3) CMCG_DIA_ROWS(4) CMCG_DIA_ROWS(5)
-                    CMCG_DIA_ROWS(6) CMCG_DIA_ROWS(7) CMCG_DIA_ROWS(8) CMCG_DIA_ROWS(9) CMCG_DIA_ROWS(10)
-                    CMCG_DIA_ROWS(11) CMCG_DIA_ROWS(12) CMCG_DIA_ROWS(13) CMCG_DIA_ROWS(14) CMCG_DIA_ROWS(15)
-                    default: dia_rows<16>(vp, po, P, n, tid, q, pq[0]);
-#undef CMCG_DIA_ROWS
-                }
-            } else {
-                // two row slots at a time (slices past the system have width 0)
-#pragma unroll
-                for (int k = 0; k < kSmemNK; k += 2) {
-                    if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                    const int i0 = tid + k * kSmemThreads, i1 = i0 + kSmemThreads;
-                    float q0 = 0.0f, q1 = 0.0f;
-                    fast_rows2<float>(a.c.col16, vin, tab[warp][k], tab[warp][k + 1], lane, LocalX<float>{P}, q0, q1);
-                    q[k] = i0 < n ? q0 : 0.0f;
-                    q[k + 1] = i1 < n ? q1 : 0.0f;
-                    if (i0 < n) pq[0] += P[i0] * q[k];
-                    if (i1 < n) pq[0] += P[i1] * q[k + 1];
-                }
-            }
-            block_sum<float, 1>(pq, red);
-            const float alpha = rz / pq[0];
-            if (!finite_(pq[0]) || !finite_(alpha)) { status = CMCG_SOLVE_NON_FINITE; break; }
-            if (!(pq[0] > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
-            float s1[1] = {0.0f};
-#pragma unroll
-            for (int k = 0; k < kSmemNK; ++k) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
-                if (i < n) {
-                    XH[i] += alpha * P[i];
-                    const float ri = R[i] - alpha * q[k];
-                    R[i] = ri;
-                    s1[0] += ri * ri;
-                }
-            }
-            block_sum<float, 1>(s1, red);
-            ++it;
-            folded = false;
-            float rzn = s1[0];
-            if (!finite_(rzn)) { status = CMCG_SOLVE_NON_FINITE; break; }
-            // replace the residual when it dropped by delta, or when it suggests
-            // that the FP64 residual may have reached the target
-            if (rzn < d2 * rmax || rzn < goal) {
-#pragma unroll
-                for (int k = 0; k < kSmemNK; ++k) {
-                    if (k * kSmemThreads >= n) break;
-                    const int i = tid + k * kSmemThreads;
-                    if (i < n) {
-                        x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
-                        XH[i] = 0.0f;
-                    }
-                }
-                __syncthreads();
-                double t2[2] = {0.0, 0.0};
-#pragma unroll
-                for (int k = 0; k < kSmemNK; ++k) {
-                    if (k * kSmemThreads >= n) break;
-                    const int i = tid + k * kSmemThreads;
-                    if (i < n) {
-                        const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
-                        const float rh = static_cast<float>(__ldg(sv + i) * r64);
-                        R[i] = rh;
-                        t2[0] += r64 * r64;
-                        t2[1] += static_cast<double>(rh) * static_cast<double>(rh);
-                    }
-                }
-                block_sum<double, 2>(t2, red64);
-                ++updates;
-                folded = true;
-                rr64 = t2[0];
-                rzn = static_cast<float>(t2[1]);
-                rmax = rzn;
-                goal = static_cast<float>(thr / rr64) * rmax;
-                if (!finite_(rr64)) { status = CMCG_SOLVE_NON_FINITE; break; }
-                if (rr64 < thr) { status = CMCG_SOLVE_CONVERGED; break; }
-            }
-            if (!(rzn > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
-            const float beta = rzn / rz;
-            rz = rzn;
-#pragma unroll
-            for (int k = 0; k < kSmemNK; ++k) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
-                if (i < n) P[i] = R[i] + beta * P[i];
-            }
-            __syncthreads();
-        }
-        if (!folded) {
-            // fold the pending increments and report the true residual
-#pragma unroll
-            for (int k = 0; k < kSmemNK; ++k) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
-                if (i < n) x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
-            }
-            __syncthreads();
-            double t1[1] = {0.0};
-#pragma unroll
-            for (int k = 0; k < kSmemNK; ++k) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
-                if (i < n) {
-                    const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
-                    t1[0] += r64 * r64;
-                }
-            }
-            block_sum<double, 1>(t1, red64);
-            rr64 = t1[0];
-        }
-        if (tid == 0) {
-            a.st.it[inst] = it;
-            a.st.status[inst] = status;
-            a.st.rr[inst] = rr64;
-            a.st.bb[inst] = bb;
-            a.st.outer[inst] = updates;
-            a.st.err[inst] = (status == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(rr64 / bb);
         }
         __syncthreads();
     }
@@ -2512,23 +2103,18 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         bool dia = false;
         if (s->dia_kernels) CMCG_TRY(ensure_dia_vals(s, &dia));
         // the zero halo of p must fit next to the vectors in shared memory
-        const size_t sm_dia = dia ? sm + 2 * sizeof(float) * static_cast<size_t>(p->dia.margin) : 0;
+        // (vectors of whole 1024-row blocks in the diagonal layout)
+        const int nmax_dia = (s->max_sys_rows + kDiaBlockRows - 1) / kDiaBlockRows * kDiaBlockRows;
+        const size_t sm_dia = dia ? smem_bytes(nmax_dia) + 2 * sizeof(float) * static_cast<size_t>(p->dia.margin) : 0;
         if (dia && sm_dia <= kDiaSmemLimit) {
             m.vdia = static_cast<const MI*>(s->dia_vals);
             m.vdia_stride = s->dia_stride;
             m.dia_base = p->dia.d_sys_base;
             m.dia_off = p->dia.d_sys_off;
             m.margin = p->dia.margin;
-            if (p->dia.max_nd == 5) {
-                CMCG_TRY(allow_smem(k_mixed_fast<MI, MO, 5>, sm_dia));
-                k_mixed_fast<MI, MO, 5><<<grid, kSmemThreads, sm_dia, ctx->stream>>>(m, nmax);
-            } else {
-                CMCG_TRY(allow_smem(k_mixed_fast<MI, MO, 7>, sm_dia));
-                k_mixed_fast<MI, MO, 7><<<grid, kSmemThreads, sm_dia, ctx->stream>>>(m, nmax);
-            }
+            CMCG_TRY((launch_mixed_fast<MI, MO>(m, nmax_dia, sm_dia, p->dia.max_nd, grid, ctx->stream)));
         } else {
-            CMCG_TRY(allow_smem(k_mixed_fast<MI, MO, 0>, sm));
-            k_mixed_fast<MI, MO, 0><<<grid, kSmemThreads, sm, ctx->stream>>>(m, nmax);
+            CMCG_TRY((launch_mixed_fast<MI, MO>(m, nmax, sm, 0, grid, ctx->stream)));
         }
         count_launch();
         CMCG_CHECK_LAUNCH();

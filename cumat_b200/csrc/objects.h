@@ -52,12 +52,16 @@ struct SellPlan {
 
 // Diagonal (DIA) copy of a CSR pattern whose systems each have at most
 // kDiaMax distinct column offsets col - row (stencils on structured grids,
-// banded matrices): system s stores diagonal d (offset sys_off[s][d], sorted
-// ascending, padded with offset 0) of its local row i at slot
-// sys_base[s] + d * n_s + i; entries missing from a row hold value 0. Feeds
-// the mixed-precision persistent kernel, whose rows then need no column
-// indices.
+// banded matrices), in blocks of kDiaBlockRows rows: system s stores diagonal
+// d (offset sys_off[s][d], sorted ascending, padded with offset 0) of its
+// local row i = kDiaBlockRows k + j at slot
+// sys_base[s] + kDiaBlockRows (k nd + d) + j (nd = max_nd); entries missing
+// from a row, and the rows of the last block past the system's end, hold
+// value 0. Feeds the mixed-precision persistent kernel, whose thread j then
+// reads every value of its rows from one pointer with immediate offsets and
+// needs no column indices.
 constexpr int kDiaMax = 8;
+constexpr int kDiaBlockRows = 1024;
 struct DiaPlan {
     bool built = false;
     bool ok = false;            // every system has at most kDiaMax offsets

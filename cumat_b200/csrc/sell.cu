@@ -157,19 +157,20 @@ cmcg_status ensure_dia(cmcg_pattern p) {
     // kernel is built for); unused ones hold zeros
     const int32_t nd_alloc = max_nd <= 5 ? 5 : max_nd <= 7 ? 7 : 0;
     if (nd_alloc == 0) return CMCG_OK;
+    constexpr int64_t B = kDiaBlockRows;
     for (int64_t s = 0; s < n_sys; ++s) {
         base[s] = slots;
-        slots += static_cast<int64_t>(nd_alloc) * (ro[s + 1] - ro[s]);
+        slots += static_cast<int64_t>(nd_alloc) * ((ro[s + 1] - ro[s] + B - 1) / B) * B;
     }
     if (slots >= INT32_MAX) return CMCG_OK;
     std::vector<int32_t> pos(static_cast<size_t>(p->nnz));
     for (int64_t s = 0; s < n_sys; ++s) {
-        const int64_t n = ro[s + 1] - ro[s];
         const int32_t* o = off.data() + s * kDiaMax;
         for (int64_t r = ro[s]; r < ro[s + 1]; ++r) {
+            const int64_t i = r - ro[s];
             for (int32_t k = rp[r]; k < rp[r + 1]; ++k) {
                 const int32_t d = static_cast<int32_t>(std::find(o, o + nd[s], static_cast<int32_t>(ci[k] - r)) - o);
-                pos[k] = static_cast<int32_t>(base[s] + d * n + (r - ro[s]));
+                pos[k] = static_cast<int32_t>(base[s] + B * ((i / B) * nd_alloc + d) + i % B);
             }
         }
     }
