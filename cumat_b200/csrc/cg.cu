@@ -807,6 +807,25 @@ __global__ void k_scale_dia(const int32_t* __restrict__ rp, const int32_t* __res
     }
 }
 
+// flag[b][s] = 1 when diagonal nd / 2 of system s is offset 0 and its values on
+// the system's rows are all exactly 1 (Jacobi scaling of a positive diagonal
+// gives 1 after rounding), else 0; one CTA per (batch, system).
+template <typename MT>
+__global__ void k_dia_unit(const MT* __restrict__ vals, int64_t vstride, const int64_t* __restrict__ base,
+                           const int32_t* __restrict__ off, const int32_t* __restrict__ row_off, int32_t n_sys,
+                           int32_t mb, int32_t nd, int32_t* __restrict__ flag) {
+    for (int64_t item = blockIdx.x; item < static_cast<int64_t>(n_sys) * mb; item += gridDim.x) {
+        const int b = static_cast<int>(item / n_sys), s = static_cast<int>(item - static_cast<int64_t>(b) * n_sys);
+        const int n = row_off[s + 1] - row_off[s];
+        const MT* v = vals + b * vstride + base[s];
+        int ok = off[s * kDiaMax + nd / 2] == 0;
+        for (int i = threadIdx.x; ok && i < n; i += blockDim.x)
+            ok = mval<double>(v[kDiaBlockRows * ((i / kDiaBlockRows) * nd + nd / 2) + i % kDiaBlockRows]) == 1.0;
+        ok = __syncthreads_and(ok);
+        if (threadIdx.x == 0) flag[item] = ok;
+    }
+}
+
 // out[b][slot] = a * s_row * s_col for every slot of the sliced layout (warp per slice)
 template <typename MS, typename MD>
 __global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __restrict__ off64,
@@ -1477,7 +1496,8 @@ struct cmcg_solver_s {
     int32_t mix_dtype = -1;
     // the same scaled values in the pattern's diagonal layout, when it has one
     bool dia_kernels = true;  // CUMAT_CG_DIA=0 keeps the sliced layout
-    void* dia_vals = nullptr;
+    void* dia_vals = nullptr;      // diagonal-layout values, then the unit-diagonal flags
+    int32_t* dia_unit = nullptr;   // inside dia_vals
     int64_t dia_stride = 0;
     int64_t dia_version = -1, dia_plan_id = -1;
     int32_t dia_dtype = -1;
@@ -1785,9 +1805,12 @@ cmcg_status ensure_dia_vals(cmcg_solver s, bool* ok) {
         dev_free(s->dia_vals);
         s->dia_vals = nullptr;
         s->dia_stride = (D.n_slots + 7) / 8 * 8 + 8;
-        const size_t bytes = static_cast<size_t>(s->dia_stride) * A->batches * dtype_size(A->dtype);
+        // values, then the per-(batch, system) unit-diagonal flags
+        const size_t vbytes = (static_cast<size_t>(s->dia_stride) * A->batches * dtype_size(A->dtype) + 255) / 256 * 256;
+        const size_t bytes = vbytes + static_cast<size_t>(s->n_sys) * A->batches * sizeof(int32_t);
         CMCG_TRY(dev_alloc(&s->dia_vals, bytes));
         CMCG_CUDA(cudaMemsetAsync(s->dia_vals, 0, bytes, ctx->stream));
+        s->dia_unit = reinterpret_cast<int32_t*>(static_cast<char*>(s->dia_vals) + vbytes);
         const int blocks = ctx->sm_count * 8;
 #define CMCG_SCALE_DIA(MT)                                                                                              \
     k_scale_dia<MT><<<blocks, 256, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, static_cast<const MT*>(A->d_vals), A->stride, \
@@ -1797,6 +1820,17 @@ cmcg_status ensure_dia_vals(cmcg_solver s, bool* ok) {
         else if (A->dtype == CMCG_BF16) CMCG_SCALE_DIA(__nv_bfloat16);
         else CMCG_SCALE_DIA(double);
 #undef CMCG_SCALE_DIA
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        const int ublocks = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(s->n_sys) * A->batches, 65535));
+#define CMCG_DIA_UNIT(MT)                                                                                          \
+    k_dia_unit<MT><<<ublocks, 256, 0, ctx->stream>>>(static_cast<const MT*>(s->dia_vals), s->dia_stride,          \
+                                                     D.d_sys_base, D.d_sys_off, p->d_row_off, s->n_sys, A->batches, \
+                                                     D.max_nd, s->dia_unit)
+        if (A->dtype == CMCG_F32) CMCG_DIA_UNIT(float);
+        else if (A->dtype == CMCG_BF16) CMCG_DIA_UNIT(__nv_bfloat16);
+        else CMCG_DIA_UNIT(double);
+#undef CMCG_DIA_UNIT
         count_launch();
         CMCG_CHECK_LAUNCH();
         s->dia_version = A->version;
@@ -2112,6 +2146,7 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
             m.dia_base = p->dia.d_sys_base;
             m.dia_off = p->dia.d_sys_off;
             m.margin = p->dia.margin;
+            m.dia_unit = s->dia_unit;
             CMCG_TRY((launch_mixed_fast<MI, MO>(m, nmax_dia, sm_dia, p->dia.max_nd, grid, ctx->stream)));
         } else {
             CMCG_TRY((launch_mixed_fast<MI, MO>(m, nmax, sm, 0, grid, ctx->stream)));

@@ -181,6 +181,7 @@ struct MixArgs {
     const int64_t* dia_base;   // n_sys
     const int32_t* dia_off;    // n_sys * kDiaMax
     int32_t margin;            // largest |offset|: zero halo around p in shared memory
+    const int32_t* dia_unit;   // [mb][n_sys]: 1 = middle diagonal is offset 0 with all values 1
 };
 
 // Launches k_mixed_fast (cg_mixed.cu) with `smem` bytes of dynamic shared

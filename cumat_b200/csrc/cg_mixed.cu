@@ -20,42 +20,57 @@ static_assert(kDiaBlockRows == kSmemThreads, "diagonal blocks hold one row per t
 // q[k] = (S A S p)[tid + 1024 k] for the NK row slots, entries added in
 // ascending offset order (the row's CSR order) with fused multiply-adds;
 // pq += p_i q_i in slot order. po[d]: p index of the thread's first row plus
-// the offset of diagonal d.
-template <int NK, int ND, typename MI>
+// the offset of diagonal d. UNIT: the middle diagonal is offset 0 with every
+// value exactly 1 (Jacobi scaling of a positive diagonal), so its values are
+// not loaded; fmaf(1, p, acc) rounds as the loaded form did.
+template <int NK, int ND, bool UNIT, typename MI>
 __device__ __forceinline__ void dia_spmv(const MI* __restrict__ vt, const int (&po)[ND], const float* P, int tid,
                                          float (&q)[kSmemNK], float& pq) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
         float acc = 0.0f;
 #pragma unroll
-        for (int d = 0; d < ND; ++d)
-            acc = fmaf(mval<float>(vt[(k * ND + d) * kSmemThreads]), P[po[d] + k * kSmemThreads], acc);
+        for (int d = 0; d < ND; ++d) {
+            const float v = (UNIT && d == ND / 2) ? 1.0f : mval<float>(vt[(k * ND + d) * kSmemThreads]);
+            acc = fmaf(v, P[po[d] + k * kSmemThreads], acc);
+        }
         q[k] = acc;
         pq += P[tid + k * kSmemThreads] * acc;
     }
 }
 
-// xh += alpha p, r -= alpha q over the NK slots; s1 += r_i^2 in slot order
+// r -= alpha q over the NK slots; s1 += r_i^2 in slot order
 template <int NK>
-__device__ __forceinline__ void dia_update(const float* P, float* R, float* XH, int tid, float alpha,
-                                           const float (&q)[kSmemNK], float& s1) {
+__device__ __forceinline__ void dia_update(float* R, int tid, float alpha, const float (&q)[kSmemNK], float& s1) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
         const int i = tid + k * kSmemThreads;
-        XH[i] += alpha * P[i];
         const float ri = R[i] - alpha * q[k];
         R[i] = ri;
         s1 += ri * ri;
     }
 }
 
-// p = r + beta p over the NK slots
-template <int NK>
-__device__ __forceinline__ void dia_pupdate(float* P, const float* R, int tid, float beta) {
+// xh += alpha p (the iteration's x increment, unless a fold took it already)
+// and p = r + beta p over the NK slots, one read of p for both
+template <int NK, bool XINC>
+__device__ __forceinline__ void dia_pupdate(float* P, const float* R, float* XH, int tid, float alpha, float beta) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
         const int i = tid + k * kSmemThreads;
-        P[i] = R[i] + beta * P[i];
+        const float pi = P[i];
+        if (XINC) XH[i] += alpha * pi;
+        P[i] = R[i] + beta * pi;
+    }
+}
+
+// xh += alpha p over the NK slots (the pending increment before a fold)
+template <int NK>
+__device__ __forceinline__ void dia_xinc(const float* P, float* XH, int tid, float alpha) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        const int i = tid + k * kSmemThreads;
+        XH[i] += alpha * P[i];
     }
 }
 
@@ -127,7 +142,9 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         const int nk = (n + kSmemThreads - 1) / kSmemThreads;
         const MI* vt = nullptr;
         int po[ND > 0 ? ND : 1] = {};
+        bool unit = false;
         if constexpr (ND > 0) {
+            unit = __ldg(a.dia_unit + (a.mb == 1 ? 0 : bi) * a.n_sys + s) != 0;
             vt = a.vdia + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vdia_stride) + __ldg(a.dia_base + s) + tid;
 #pragma unroll
             for (int d = 0; d < ND; ++d) po[d] = tid + __ldg(a.dia_off + s * kDiaMax + d);
@@ -173,11 +190,18 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
         const int64_t maxit = sys_max_iter(a.max_inner, n);
         bool folded = true;
+        // diagonal layout: alpha of the x increment not yet added to xh
+        bool pend = false;
+        float alpha_pend = 0.0f;
         while (status == ST_RUNNING) {
             if (it >= maxit || updates >= a.max_updates) { status = CMCG_SOLVE_MAX_ITER; break; }
             float pq[1] = {0.0f};
             if constexpr (ND > 0) {
-                CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND>(vt, po, P, tid, q, pq[0])))
+                if (unit) {
+                    CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND, true>(vt, po, P, tid, q, pq[0])))
+                } else {
+                    CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND, false>(vt, po, P, tid, q, pq[0])))
+                }
             } else {
                 // two row slots at a time (slices past the system have width 0)
 #pragma unroll
@@ -198,7 +222,10 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             if (!(pq[0] > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
             float s1[1] = {0.0f};
             if constexpr (ND > 0) {
-                CMCG_DIA_SLOTS(nk, (dia_update<NK>(P, R, XH, tid, alpha, q, s1[0])))
+                // the x increment alpha p is added by the p update (or before a fold)
+                CMCG_DIA_SLOTS(nk, (dia_update<NK>(R, tid, alpha, q, s1[0])))
+                alpha_pend = alpha;
+                pend = true;
             } else {
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
@@ -220,6 +247,10 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             // replace the residual when it dropped by delta, or when it suggests
             // that the FP64 residual may have reached the target
             if (rzn < d2 * rmax || rzn < goal) {
+                if (ND > 0 && pend) {
+                    CMCG_DIA_SLOTS(nk, (dia_xinc<NK>(P, XH, tid, alpha_pend)))
+                    pend = false;
+                }
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
                     if (k * kSmemThreads >= n) break;
@@ -257,7 +288,12 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             const float beta = rzn / rz;
             rz = rzn;
             if constexpr (ND > 0) {
-                CMCG_DIA_SLOTS(nk, (dia_pupdate<NK>(P, R, tid, beta)))
+                if (pend) {
+                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, true>(P, R, XH, tid, alpha_pend, beta)))
+                } else {
+                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, false>(P, R, XH, tid, alpha_pend, beta)))
+                }
+                pend = false;
             } else {
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
@@ -270,6 +306,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         }
         if (!folded) {
             // fold the pending increments and report the true residual
+            if (ND > 0 && pend) CMCG_DIA_SLOTS(nk, (dia_xinc<NK>(P, XH, tid, alpha_pend)))
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
                 if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system

@@ -341,6 +341,58 @@ def test_diagonal_layout_matches_sliced_layout(cuda, monkeypatch, inner):
         assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(bt.b[r0:r1]) < 1e-10
 
 
+def _tridiag(n, rng):
+    """1D finite-volume diffusion with a reaction term 0.05 (Dirichlet ends):
+    offsets -1, 0, 1, condition number ~100."""
+    k = np.exp(rng.normal(0.0, 0.5, n + 1))
+    rp, col, val = [0], [], []
+    for i in range(n):
+        if i > 0:
+            col.append(i - 1); val.append(-k[i])
+        col.append(i); val.append(k[i] + k[i + 1] + 0.05)
+        if i < n - 1:
+            col.append(i + 1); val.append(-k[i + 1])
+        rp.append(len(col))
+    return np.array(rp, np.int32), np.array(col, np.int32), np.array(val, np.float32)
+
+
+def test_diagonal_layout_mixed_offset_sets(cuda, monkeypatch):
+    # 2D systems (5 offsets, Jacobi-scaled middle diagonal of ones: its values
+    # are not loaded) packed with 1D systems (3 offsets stored in 5 diagonal
+    # slots, so the middle slot is not the offset-0 diagonal and every value is
+    # loaded): both kinds agree bit for bit with the sliced layout
+    m = cm()
+    rng = np.random.default_rng(31)
+    bt = P.fv2d_batch(6, 16, 80, 0.5, 37)
+    rps, cols, vals, offs = [bt.row_ptr], [bt.col], [bt.val], list(bt.row_off)
+    n, nnz = bt.n, int(bt.row_ptr[-1])
+    for m1 in (700, 1500, 2500):
+        rp, c, v = _tridiag(m1, rng)
+        rps.append(rp[1:] + nnz); cols.append(c + n); vals.append(v)
+        n += m1; nnz += int(rp[-1]); offs.append(n)
+    row_ptr, col, val = np.concatenate(rps), np.concatenate(cols), np.concatenate(vals)
+    row_off = np.array(offs, np.int64)
+    b = rng.uniform(-1.0, 1.0, n)
+    p = m.SparsityPattern.csr(n, n, row_ptr, col)
+    p.set_systems(row_off)
+    A = m.SparseMatrix(p, dtype=torch.float32).setData(val)
+    A64 = m.SparseMatrix(p, dtype=torch.float64).setData(val.astype(np.float64))
+    b64 = torch.from_numpy(b).to(cuda)
+    cg = m.ConjugateGradient(A)
+    x1 = cg.solve_refined(b64, outer=A64, outer_tol=1e-10, max_outer=200).cpu().numpy()
+    s1 = cg.system_stats()
+    monkeypatch.setenv("CUMAT_CG_DIA", "0")
+    cg0 = m.ConjugateGradient(A)
+    x0 = cg0.solve_refined(b64, outer=A64, outer_tol=1e-10, max_outer=200).cpu().numpy()
+    s0 = cg0.system_stats()
+    assert np.array_equal(s1["iterations"], s0["iterations"]) and np.array_equal(x1, x0)
+    assert np.all(s1["status"] == 0) and np.all(s1["error"] < 1e-10)
+    r = b - O.spmv_csr_f32_in_f64(n, n, row_ptr, col, val, x1)[0]
+    for s in range(len(offs) - 1):
+        r0, r1 = offs[s], offs[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b[r0:r1]) < 1e-10
+
+
 def test_generic_kernels_match_oracle(cuda, monkeypatch):
     # CUMAT_CG_FAST=0 (read when a solver is created) selects the generic
     # shared-memory kernels: explicit Jacobi PCG inside the reliable updates
