@@ -31,36 +31,43 @@ __device__ __forceinline__ void dia_spmv(const MI* __restrict__ vt, const int (&
         float acc = 0.0f;
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
-            const float v = (UNIT && d == ND / 2) ? 1.0f : mval<float>(vt[(k * ND + d) * kSmemThreads]);
-            acc = fmaf(v, P[po[d] + k * kSmemThreads], acc);
+            if (UNIT && d == ND / 2)   // offset 0: the row's own p, read once for both uses
+                acc = fmaf(1.0f, P[tid + k * kSmemThreads], acc);
+            else
+                acc = fmaf(mval<float>(vt[(k * ND + d) * kSmemThreads]), P[po[d] + k * kSmemThreads], acc);
         }
         q[k] = acc;
         pq += P[tid + k * kSmemThreads] * acc;
     }
 }
 
-// r -= alpha q over the NK slots; s1 += r_i^2 in slot order
+// r -= alpha q over the NK slots; s1 += r_i^2 in slot order. q[k] then holds
+// the new r_i (q is not needed again), for the p update.
 template <int NK>
-__device__ __forceinline__ void dia_update(float* R, int tid, float alpha, const float (&q)[kSmemNK], float& s1) {
+__device__ __forceinline__ void dia_update(float* R, int tid, float alpha, float (&q)[kSmemNK], float& s1) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
         const int i = tid + k * kSmemThreads;
         const float ri = R[i] - alpha * q[k];
         R[i] = ri;
         s1 += ri * ri;
+        q[k] = ri;
     }
 }
 
-// xh += alpha p (the iteration's x increment, unless a fold took it already)
-// and p = r + beta p over the NK slots, one read of p for both
-template <int NK, bool XINC>
-__device__ __forceinline__ void dia_pupdate(float* P, const float* R, float* XH, int tid, float alpha, float beta) {
+// p = r + beta p over the NK slots, and with STEP (an iteration without a
+// residual replacement) xh += alpha p, the iteration's x increment, from the
+// same read of p, with r from the registers dia_update left it in; after a
+// replacement the fold took the increment and r comes from shared memory.
+template <int NK, bool STEP>
+__device__ __forceinline__ void dia_pupdate(float* P, const float* R, float* XH, int tid, float alpha, float beta,
+                                            const float (&rr)[kSmemNK]) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
         const int i = tid + k * kSmemThreads;
         const float pi = P[i];
-        if (XINC) XH[i] += alpha * pi;
-        P[i] = R[i] + beta * pi;
+        if (STEP) XH[i] += alpha * pi;
+        P[i] = (STEP ? rr[k] : R[i]) + beta * pi;
     }
 }
 
@@ -288,10 +295,11 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             const float beta = rzn / rz;
             rz = rzn;
             if constexpr (ND > 0) {
+                // pend: no replacement this iteration (the fold clears it)
                 if (pend) {
-                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, true>(P, R, XH, tid, alpha_pend, beta)))
+                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, true>(P, R, XH, tid, alpha_pend, beta, q)))
                 } else {
-                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, false>(P, R, XH, tid, alpha_pend, beta)))
+                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, false>(P, R, XH, tid, alpha_pend, beta, q)))
                 }
                 pend = false;
             } else {
