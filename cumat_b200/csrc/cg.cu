@@ -1453,7 +1453,7 @@ struct cmcg_solver_s {
     int64_t max_iter = -1;
     int32_t path = CMCG_PATH_AUTO;
     int32_t refine_method = CMCG_REFINE_RELIABLE;
-    double refine_delta = 0.1;
+    double refine_delta = 0.0;   // 0: by the inner value type (refine_delta_for)
     bool use_smem = true;     // shared-memory-resident kernels where the systems fit
     bool inner_solve = false; // set while the solver runs the inner solves of a refinement
     bool fast_kernels = true; // compact-layout kernels where available (CUMAT_CG_FAST=0 disables)
@@ -1733,6 +1733,15 @@ cmcg_status allow_smem(K kern, size_t bytes) {
 }
 
 inline int smem_rows(int32_t max_rows) { return (max_rows + 3) / 4 * 4; }
+
+// Residual-replacement threshold of the reliable updates: the one set, else
+// 0.01 for FP32 inner values (the FP32 recurrence stays within ~eps_f32 / 0.01
+// of the true residual between replacements) and 0.1 for BF16 inner values
+// (an operator perturbed by ~2^-9 needs the FP64 residual more often).
+inline float refine_delta_for(cmcg_solver s) {
+    if (s->refine_delta > 0.0) return static_cast<float>(s->refine_delta);
+    return s->A->dtype == CMCG_BF16 ? 0.1f : 0.01f;
+}
 
 // dynamic shared memory the diagonal-layout kernel may use (the opt-in
 // maximum per CTA minus the kernel's static arrays, with room to spare)
@@ -2129,7 +2138,7 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         m.outer_tol = outer_tol;
         m.max_inner = s->max_iter;
         m.max_updates = max_outer;
-        m.delta = static_cast<float>(s->refine_delta);
+        m.delta = refine_delta_for(s);
         m.st = s->st;
         const int nmax = smem_rows(s->max_sys_rows);
         const size_t sm = smem_bytes(nmax);
@@ -2162,7 +2171,7 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         const size_t sm = smem_bytes(nmax);
         CMCG_TRY(allow_smem(k_reliable_smem<MI, MO, FMT>, sm));
         const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
-        k_reliable_smem<MI, MO, FMT><<<grid, kSmemThreads, sm, ctx->stream>>>(a, nmax, static_cast<float>(s->refine_delta));
+        k_reliable_smem<MI, MO, FMT><<<grid, kSmemThreads, sm, ctx->stream>>>(a, nmax, refine_delta_for(s));
         count_launch();
         CMCG_CHECK_LAUNCH();
         s->last_inst = n_inst;
@@ -2330,7 +2339,7 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     m.p2 = p1 + items;
     m.outer_tol = outer_tol;
     m.max_updates = max_outer;
-    m.delta = static_cast<float>(s->refine_delta);
+    m.delta = refine_delta_for(s);
     const int grid = s->grid_ctas;
 
     CMCG_CUDA(cudaMemcpyAsync(b64, b, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -2488,7 +2497,7 @@ cmcg_status cmcg_cg_set_path(cmcg_solver s, int32_t path) {
 cmcg_status cmcg_cg_set_refinement(cmcg_solver s, int32_t method, double delta) {
     CMCG_REQUIRE(s, "cmcg_cg_set_refinement: NULL solver");
     CMCG_REQUIRE(method == CMCG_REFINE_RELIABLE || method == CMCG_REFINE_RESTART, "cmcg_cg_set_refinement: bad method");
-    CMCG_REQUIRE(delta > 0.0 && delta < 1.0, "cmcg_cg_set_refinement: delta must be in (0, 1)");
+    CMCG_REQUIRE(delta >= 0.0 && delta < 1.0, "cmcg_cg_set_refinement: delta must be 0 (automatic) or in (0, 1)");
     s->refine_method = method;
     s->refine_delta = delta;
     return CMCG_OK;

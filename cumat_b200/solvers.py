@@ -53,8 +53,9 @@ class ConjugateGradient:
         N.call("cmcg_cg_set_path", self.handle, int(path))
         return self
 
-    def set_refinement(self, method: int = N.REFINE_RELIABLE, delta: float = 0.1) -> "ConjugateGradient":
-        """Mixed-precision method of solve_refined: reliable updates (default) or restarts."""
+    def set_refinement(self, method: int = N.REFINE_RELIABLE, delta: float = 0.0) -> "ConjugateGradient":
+        """Mixed-precision method of solve_refined: reliable updates (default) or restarts;
+        delta 0 picks the replacement threshold by the inner value type (0.01 FP32, 0.1 BF16)."""
         N.call("cmcg_cg_set_refinement", self.handle, int(method), float(delta))
         return self
 

@@ -232,9 +232,12 @@ cmcg_status cmcg_cg_set_max_iterations(cmcg_solver s, int64_t max_iter);
 cmcg_status cmcg_cg_get_settings(cmcg_solver s, double* tol, int64_t* max_iter);
 /* Execution path (default AUTO). */
 cmcg_status cmcg_cg_set_path(cmcg_solver s, int32_t path);
-/* Mixed-precision method of cmcg_cg_solve_refined (default RELIABLE, delta 0.1:
- * the FP32 recursive residual is replaced by the FP64 one whenever it has
- * dropped by delta since the last replacement). No reference counterpart. */
+/* Mixed-precision method of cmcg_cg_solve_refined (default RELIABLE): the
+ * FP32 recursive residual is replaced by the FP64 one whenever its norm has
+ * dropped by delta since the last replacement. delta 0 (the default) picks
+ * 0.01 for FP32 inner values (the recurrence then stays within about
+ * eps_f32 / delta of the true residual) and 0.1 for BF16 inner values.
+ * No reference counterpart. */
 cmcg_status cmcg_cg_set_refinement(cmcg_solver s, int32_t method, double delta);
 /* Solves A x = b for every (batch, system) with vec_dtype F32 or F64 vectors
  * (reference solve / solveWithGuess, SolverBase.h:33-37, IterativeSolverBase.h:118-124;

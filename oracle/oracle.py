@@ -213,7 +213,7 @@ def refined_packed(row_off, rp, ci, val32, rhs64, inner_tol, outer_tol, max_inne
     return x, outer, inner, err
 
 
-def reliable_packed(row_off, rp, ci, val32, rhs64, tol, delta=0.1, max_iter=-1, max_updates=1000, precond=1,
+def reliable_packed(row_off, rp, ci, val32, rhs64, tol, delta=0.01, max_iter=-1, max_updates=1000, precond=1,
                     bf16_inner=False, scaled=True):
     """FP32 CG with FP64 reliable updates, per system; scaled=True is the
     Jacobi-scaled form of the CUDA fast path, scaled=False explicit Jacobi PCG.
