@@ -1454,6 +1454,12 @@ struct cmcg_solver_s {
     int32_t path = CMCG_PATH_AUTO;
     int32_t refine_method = CMCG_REFINE_RELIABLE;
     double refine_delta = 0.0;   // 0: by the inner value type (refine_delta_for)
+    // mixed kernel: systems at order positions >= mix_split on 512-thread CTAs
+    // (CUMAT_CG_SMALL=0 keeps every system on 1024-thread CTAs)
+    int32_t mix_split = 0;
+    bool mix_small = true;
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool use_smem = true;     // shared-memory-resident kernels where the systems fit
     bool inner_solve = false; // set while the solver runs the inner solves of a refinement
     bool fast_kernels = true; // compact-layout kernels where available (CUMAT_CG_FAST=0 disables)
@@ -1543,6 +1549,10 @@ cmcg_status build_plan(cmcg_solver s) {
     t_begin[n_sys] = static_cast<int32_t>(t_row0.size());
     s->n_sys = n_sys;
     s->max_sys_rows = maxr;
+    // last position of the size order with a system above kMixSmallRows rows
+    s->mix_split = 0;
+    for (int32_t i = 0; i < n_sys; ++i)
+        if (ro[order[i] + 1] - ro[order[i]] > kMixSmallRows) s->mix_split = i + 1;
     s->n_tiles = static_cast<int32_t>(t_row0.size());
     s->systems_version = p->systems_version;
     // grid path: contiguous tile ranges per CTA, cut into segments at system
@@ -1733,6 +1743,22 @@ cmcg_status allow_smem(K kern, size_t bytes) {
 }
 
 inline int smem_rows(int32_t max_rows) { return (max_rows + 3) / 4 * 4; }
+
+// dynamic shared memory of a 512-thread mixed-kernel CTA such that two fit on
+// an SM next to their static arrays
+constexpr size_t kMixSmallSmemLimit = 104 * 1024;
+
+// Stream of the highest priority and fork / join events for running the two
+// CTA sizes of the mixed kernel side by side (created on first use).
+cmcg_status ensure_aux_stream(cmcg_solver s) {
+    if (s->aux_stream) return CMCG_OK;
+    int least = 0, greatest = 0;
+    CMCG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CMCG_CUDA(cudaStreamCreateWithPriority(&s->aux_stream, cudaStreamNonBlocking, greatest));
+    CMCG_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+    CMCG_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    return CMCG_OK;
+}
 
 // Residual-replacement threshold of the reliable updates: the one set, else
 // 0.01 for FP32 inner values (the FP32 recurrence stays within ~eps_f32 / 0.01
@@ -2142,25 +2168,63 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         m.st = s->st;
         const int nmax = smem_rows(s->max_sys_rows);
         const size_t sm = smem_bytes(nmax);
-        const int grid = std::max(1, std::min(n_inst, ctx->sm_count));
         bool dia = false;
         if (s->dia_kernels) CMCG_TRY(ensure_dia_vals(s, &dia));
         // the zero halo of p must fit next to the vectors in shared memory
         // (vectors of whole 1024-row blocks in the diagonal layout)
         const int nmax_dia = (s->max_sys_rows + kDiaBlockRows - 1) / kDiaBlockRows * kDiaBlockRows;
         const size_t sm_dia = dia ? smem_bytes(nmax_dia) + 2 * sizeof(float) * static_cast<size_t>(p->dia.margin) : 0;
-        if (dia && sm_dia <= kDiaSmemLimit) {
+        const bool use_dia = dia && sm_dia <= kDiaSmemLimit;
+        const size_t halo = use_dia ? 2 * sizeof(float) * static_cast<size_t>(p->dia.margin) : 0;
+        int nd = 0;
+        if (use_dia) {
             m.vdia = static_cast<const MI*>(s->dia_vals);
             m.vdia_stride = s->dia_stride;
             m.dia_base = p->dia.d_sys_base;
             m.dia_off = p->dia.d_sys_off;
             m.margin = p->dia.margin;
             m.dia_unit = s->dia_unit;
-            CMCG_TRY((launch_mixed_fast<MI, MO>(m, nmax_dia, sm_dia, p->dia.max_nd, grid, ctx->stream)));
-        } else {
-            CMCG_TRY((launch_mixed_fast<MI, MO>(m, nmax, sm, 0, grid, ctx->stream)));
+            nd = p->dia.max_nd;
         }
-        count_launch();
+        // Systems past position mix_split of the size order have at most
+        // kMixSmallRows rows: they run on 512-thread CTAs, two per SM, so that
+        // two systems share an SM's latencies; they go to the SMs that the
+        // 1024-thread CTAs of the larger systems leave (those launch first, on
+        // a higher-priority stream, and take every SM while work is left).
+        const int nmax_big = use_dia ? nmax_dia : nmax;
+        const size_t sm_big = use_dia ? sm_dia : sm;
+        const int small_rows = std::min<int>(s->max_sys_rows, kMixSmallRows);
+        const int nmax_small = use_dia ? (small_rows + kDiaBlockRows - 1) / kDiaBlockRows * kDiaBlockRows
+                                       : smem_rows(small_rows);
+        const size_t sm_small = smem_bytes(nmax_small) + halo;
+        int32_t split = n_inst;
+        if (s->mix_small && sm_small <= kMixSmallSmemLimit) split = std::min<int32_t>(n_inst, s->mix_split * ob);
+        MixArgs<MI, MO> mb = m;
+        m.item_begin = 0;
+        m.item_end = split;
+        m.next = s->counters;
+        mb.item_begin = split;
+        mb.item_end = n_inst;
+        mb.next = s->counters + 1;
+        const int grid_big = std::max(1, std::min(split, ctx->sm_count));
+        const int grid_small = std::max(1, std::min(n_inst - split, 2 * ctx->sm_count));
+        if (split == n_inst) {
+            CMCG_TRY((launch_mixed_fast<MI, MO>(m, kSmemThreads, nmax_big, sm_big, nd, grid_big, ctx->stream)));
+            count_launch();
+        } else if (split == 0) {
+            CMCG_TRY((launch_mixed_fast<MI, MO>(mb, 512, nmax_small, sm_small, nd, grid_small, ctx->stream)));
+            count_launch();
+        } else {
+            CMCG_TRY(ensure_aux_stream(s));
+            CMCG_CUDA(cudaEventRecord(s->ev_fork, ctx->stream));
+            CMCG_CUDA(cudaStreamWaitEvent(s->aux_stream, s->ev_fork, 0));
+            CMCG_TRY((launch_mixed_fast<MI, MO>(m, kSmemThreads, nmax_big, sm_big, nd, grid_big, s->aux_stream)));
+            CMCG_CHECK_LAUNCH();
+            CMCG_TRY((launch_mixed_fast<MI, MO>(mb, 512, nmax_small, sm_small, nd, grid_small, ctx->stream)));
+            CMCG_CUDA(cudaEventRecord(s->ev_join, s->aux_stream));
+            CMCG_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join, 0));
+            count_launch(2);
+        }
         CMCG_CHECK_LAUNCH();
         s->last_inst = n_inst;
         s->last_refined = true;
@@ -2425,6 +2489,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     s->tol = (A->dtype == CMCG_F64) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
     if (const char* e = std::getenv("CUMAT_CG_FAST")) s->fast_kernels = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_DIA")) s->dia_kernels = std::atoi(e) != 0;
+    if (const char* e = std::getenv("CUMAT_CG_SMALL")) s->mix_small = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);
     if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);
@@ -2446,6 +2511,9 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
     cudaStreamSynchronize(s->A->pat->ctx->stream);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->aux_stream) cudaStreamDestroy(s->aux_stream);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
     if (s->gexec_mix) cudaGraphExecDestroy(s->gexec_mix);
     if (s->graph_mix) cudaGraphDestroy(s->graph_mix);
     for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_seg_t0),

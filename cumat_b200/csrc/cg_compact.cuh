@@ -31,10 +31,12 @@ struct SliceEnt {
 
 // tab[w][k]: slice w + 32 k of the system (local rows 32 (w + 32 k) ...), the
 // slice holding the rows tid + k * 1024 of warp w.
+// (T threads per CTA: warp w's rows in slot k are those of slice w + (T / 32) k)
+template <int T = kSmemThreads>
 __device__ __forceinline__ void load_slice_table(SliceEnt (*tab)[kSmemNK], const int32_t* __restrict__ off32,
                                                  const int32_t* __restrict__ sw, int sl0, int nsl) {
-    for (int t = threadIdx.x; t < 32 * kSmemNK; t += blockDim.x) {
-        const int w = t / kSmemNK, k = t - (t / kSmemNK) * kSmemNK, sl = w + 32 * k;
+    for (int t = threadIdx.x; t < (T / 32) * kSmemNK; t += blockDim.x) {
+        const int w = t / kSmemNK, k = t - (t / kSmemNK) * kSmemNK, sl = w + (T / 32) * k;
         tab[w][k] = sl < nsl ? SliceEnt{__ldg(off32 + sl0 + sl), __ldg(sw + sl0 + sl)} : SliceEnt{0, 0};
     }
 }
@@ -160,7 +162,8 @@ struct MixArgs {
     int32_t rows, n_sys, ob, mb;
     const int32_t* row_off;
     const int32_t* order;
-    int32_t* next;
+    int32_t* next;                 // work counter of this launch
+    int32_t item_begin, item_end;  // its work items: (position in order) * ob + batch
     CompactArgs c;
     const MI* vin;          // Jacobi-scaled inner values, sliced layout
     int64_t vin_stride;
@@ -184,9 +187,14 @@ struct MixArgs {
     const int32_t* dia_unit;   // [mb][n_sys]: 1 = middle diagonal is offset 0 with all values 1
 };
 
-// Launches k_mixed_fast (cg_mixed.cu) with `smem` bytes of dynamic shared
-// memory: nd = 0 sliced layout, nd = 5 or 7 diagonal layout.
+// Systems of at most this many rows may run on 512-thread CTAs, two per SM.
+constexpr int kMixSmallRows = kSmemNK * 512;
+
+// Launches k_mixed_fast (cg_mixed.cu) with `threads` (1024 or 512) threads per
+// CTA and `smem` bytes of dynamic shared memory: nd = 0 sliced layout, nd = 5
+// or 7 diagonal layout.
 template <typename MI, typename MO>
-cmcg_status launch_mixed_fast(const MixArgs<MI, MO>& m, int nmax, size_t smem, int nd, int grid, cudaStream_t stream);
+cmcg_status launch_mixed_fast(const MixArgs<MI, MO>& m, int threads, int nmax, size_t smem, int nd, int grid,
+                              cudaStream_t stream);
 
 }  // namespace cmcg

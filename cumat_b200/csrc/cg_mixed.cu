@@ -15,7 +15,15 @@ namespace {
 // immediate offset. Rows past the system's end hold zero values; their p, r
 // and xh are zeroed when the system starts and stay zero, so each phase runs
 // all NK = ceil(n / 1024) slots with no row test.
-static_assert(kDiaBlockRows == kSmemThreads, "diagonal blocks hold one row per thread");
+static_assert(kDiaBlockRows == kSmemThreads, "diagonal blocks hold one row per thread of a 1024-thread CTA");
+
+// Index of the value of diagonal d for row slot k of a T-thread CTA (thread
+// t's row t + T k), relative to the thread's first row: slot k lies in block
+// (k T) / 1024 at offset (k T) % 1024, a compile-time constant per (k, d).
+template <int T, int ND>
+__device__ __forceinline__ constexpr int dia_vidx(int k, int d) {
+    return ((k * T) / kDiaBlockRows * ND + d) * kDiaBlockRows + (k * T) % kDiaBlockRows;
+}
 
 // q[k] = (S A S p)[tid + 1024 k] for the NK row slots, entries added in
 // ascending offset order (the row's CSR order) with fused multiply-adds;
@@ -23,7 +31,7 @@ static_assert(kDiaBlockRows == kSmemThreads, "diagonal blocks hold one row per t
 // the offset of diagonal d. UNIT: the middle diagonal is offset 0 with every
 // value exactly 1 (Jacobi scaling of a positive diagonal), so its values are
 // not loaded; fmaf(1, p, acc) rounds as the loaded form did.
-template <int NK, int ND, bool UNIT, typename MI>
+template <int NK, int ND, bool UNIT, int T, typename MI>
 __device__ __forceinline__ void dia_spmv(const MI* __restrict__ vt, const int (&po)[ND], const float* P, int tid,
                                          float (&q)[kSmemNK], float& pq) {
 #pragma unroll
@@ -32,22 +40,22 @@ __device__ __forceinline__ void dia_spmv(const MI* __restrict__ vt, const int (&
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
             if (UNIT && d == ND / 2)   // offset 0: the row's own p, read once for both uses
-                acc = fmaf(1.0f, P[tid + k * kSmemThreads], acc);
+                acc = fmaf(1.0f, P[tid + k * T], acc);
             else
-                acc = fmaf(mval<float>(vt[(k * ND + d) * kSmemThreads]), P[po[d] + k * kSmemThreads], acc);
+                acc = fmaf(mval<float>(vt[dia_vidx<T, ND>(k, d)]), P[po[d] + k * T], acc);
         }
         q[k] = acc;
-        pq += P[tid + k * kSmemThreads] * acc;
+        pq += P[tid + k * T] * acc;
     }
 }
 
 // r -= alpha q over the NK slots; s1 += r_i^2 in slot order. q[k] then holds
 // the new r_i (q is not needed again), for the p update.
-template <int NK>
+template <int NK, int T>
 __device__ __forceinline__ void dia_update(float* R, int tid, float alpha, float (&q)[kSmemNK], float& s1) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-        const int i = tid + k * kSmemThreads;
+        const int i = tid + k * T;
         const float ri = R[i] - alpha * q[k];
         R[i] = ri;
         s1 += ri * ri;
@@ -59,12 +67,12 @@ __device__ __forceinline__ void dia_update(float* R, int tid, float alpha, float
 // residual replacement) xh += alpha p, the iteration's x increment, from the
 // same read of p, with r from the registers dia_update left it in; after a
 // replacement the fold took the increment and r comes from shared memory.
-template <int NK, bool STEP>
+template <int NK, bool STEP, int T>
 __device__ __forceinline__ void dia_pupdate(float* P, const float* R, float* XH, int tid, float alpha, float beta,
                                             const float (&rr)[kSmemNK]) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-        const int i = tid + k * kSmemThreads;
+        const int i = tid + k * T;
         const float pi = P[i];
         if (STEP) XH[i] += alpha * pi;
         P[i] = (STEP ? rr[k] : R[i]) + beta * pi;
@@ -72,11 +80,11 @@ __device__ __forceinline__ void dia_pupdate(float* P, const float* R, float* XH,
 }
 
 // xh += alpha p over the NK slots (the pending increment before a fold)
-template <int NK>
+template <int NK, int T>
 __device__ __forceinline__ void dia_xinc(const float* P, float* XH, int tid, float alpha) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-        const int i = tid + k * kSmemThreads;
+        const int i = tid + k * T;
         XH[i] += alpha * P[i];
     }
 }
@@ -116,27 +124,27 @@ static_assert(kSmemNK == 16, "CMCG_DIA_SLOTS covers 16 row slots");
 // tests; p carries a zero halo of `margin` entries on both sides in shared
 // memory, and nmax is a multiple of 1024. The FP64 residual keeps the compact
 // sliced layout.
-template <typename MI, typename MO, int ND>
-__global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
+template <typename MI, typename MO, int ND, int T>
+__global__ void __launch_bounds__(T, T / T) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
     extern __shared__ __align__(16) float smf[];
     __shared__ SliceEnt tab[32][kSmemNK];
-    __shared__ float red[2 * (kSmemThreads / 32)];
-    __shared__ double red64[2 * (kSmemThreads / 32)];
+    __shared__ float red[2 * (T / 32)];
+    __shared__ double red64[2 * (T / 32)];
     __shared__ int slot;
     const int M = ND > 0 ? a.margin : 0;
     float* P = smf + M;
     float* R = smf + nmax + 2 * M;
     float* XH = R + nmax;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int n_inst = a.n_sys * a.ob;
+
     const float d2 = a.delta * a.delta;
     for (;;) {
-        const int item = fetch_item(a.next, &slot);
-        if (item >= n_inst) return;
+        const int item = a.item_begin + fetch_item(a.next, &slot);
+        if (item >= a.item_end) return;
         const int s = a.order[item / a.ob], bi = item % a.ob, inst = bi * a.n_sys + s;
         const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
         const int sl0 = __ldg(a.c.sys_slice0 + s), nsl = __ldg(a.c.sys_slice0 + s + 1) - sl0;
-        load_slice_table(tab, a.c.off32, a.c.sw, sl0, nsl);
+        load_slice_table<T>(tab, a.c.off32, a.c.sw, sl0, nsl);
         const int64_t vo = static_cast<int64_t>(bi) * a.rows;
         const MI* vin = a.vin + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vin_stride);
         const MO* vout = a.vout + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vout_stride);
@@ -146,7 +154,7 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         // diagonal layout: the thread's value pointer (first row), the p index
         // of its first row plus each offset, and zero p, r, xh past the
         // system's end (to the end of its last slot, and the halos of p)
-        const int nk = (n + kSmemThreads - 1) / kSmemThreads;
+        const int nk = (n + T - 1) / T;
         const MI* vt = nullptr;
         int po[ND > 0 ? ND : 1] = {};
         bool unit = false;
@@ -155,10 +163,10 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             vt = a.vdia + (a.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.vdia_stride) + __ldg(a.dia_base + s) + tid;
 #pragma unroll
             for (int d = 0; d < ND; ++d) po[d] = tid + __ldg(a.dia_off + s * kDiaMax + d);
-            const int nend = nk * kSmemThreads;
-            for (int t = tid; t < M; t += kSmemThreads) P[-1 - t] = 0.0f;
-            for (int i = n + tid; i < nend + M; i += kSmemThreads) P[i] = 0.0f;
-            for (int i = n + tid; i < nend; i += kSmemThreads) {
+            const int nend = nk * T;
+            for (int t = tid; t < M; t += T) P[-1 - t] = 0.0f;
+            for (int i = n + tid; i < nend + M; i += T) P[i] = 0.0f;
+            for (int i = n + tid; i < nend; i += T) {
                 R[i] = 0.0f;
                 XH[i] = 0.0f;
             }
@@ -169,8 +177,8 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         float rz1[1] = {0.0f};
 #pragma unroll
         for (int k = 0; k < kSmemNK; ++k) {
-            if (k * kSmemThreads >= n) break;
-            const int i = tid + k * kSmemThreads;
+            if (k * T >= n) break;
+            const int i = tid + k * T;
             if (i < n) {
                 const double b_i = bv[i];
                 x[i] = 0.0;
@@ -205,16 +213,16 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             float pq[1] = {0.0f};
             if constexpr (ND > 0) {
                 if (unit) {
-                    CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND, true>(vt, po, P, tid, q, pq[0])))
+                    CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND, true, T>(vt, po, P, tid, q, pq[0])))
                 } else {
-                    CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND, false>(vt, po, P, tid, q, pq[0])))
+                    CMCG_DIA_SLOTS(nk, (dia_spmv<NK, ND, false, T>(vt, po, P, tid, q, pq[0])))
                 }
             } else {
                 // two row slots at a time (slices past the system have width 0)
 #pragma unroll
                 for (int k = 0; k < kSmemNK; k += 2) {
-                    if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                    const int i0 = tid + k * kSmemThreads, i1 = i0 + kSmemThreads;
+                    if (k * T >= n) break;   // uniform: skip row slots past the system
+                    const int i0 = tid + k * T, i1 = i0 + T;
                     float q0 = 0.0f, q1 = 0.0f;
                     fast_rows2<float>(a.c.col16, vin, tab[warp][k], tab[warp][k + 1], lane, LocalX<float>{P}, q0, q1);
                     q[k] = i0 < n ? q0 : 0.0f;
@@ -230,14 +238,14 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             float s1[1] = {0.0f};
             if constexpr (ND > 0) {
                 // the x increment alpha p is added by the p update (or before a fold)
-                CMCG_DIA_SLOTS(nk, (dia_update<NK>(R, tid, alpha, q, s1[0])))
+                CMCG_DIA_SLOTS(nk, (dia_update<NK, T>(R, tid, alpha, q, s1[0])))
                 alpha_pend = alpha;
                 pend = true;
             } else {
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
-                    if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                    const int i = tid + k * kSmemThreads;
+                    if (k * T >= n) break;   // uniform: skip row slots past the system
+                    const int i = tid + k * T;
                     if (i < n) {
                         XH[i] += alpha * P[i];
                         const float ri = R[i] - alpha * q[k];
@@ -255,13 +263,13 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             // that the FP64 residual may have reached the target
             if (rzn < d2 * rmax || rzn < goal) {
                 if (ND > 0 && pend) {
-                    CMCG_DIA_SLOTS(nk, (dia_xinc<NK>(P, XH, tid, alpha_pend)))
+                    CMCG_DIA_SLOTS(nk, (dia_xinc<NK, T>(P, XH, tid, alpha_pend)))
                     pend = false;
                 }
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
-                    if (k * kSmemThreads >= n) break;
-                    const int i = tid + k * kSmemThreads;
+                    if (k * T >= n) break;
+                    const int i = tid + k * T;
                     if (i < n) {
                         x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
                         XH[i] = 0.0f;
@@ -271,8 +279,8 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
                 double t2[2] = {0.0, 0.0};
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
-                    if (k * kSmemThreads >= n) break;
-                    const int i = tid + k * kSmemThreads;
+                    if (k * T >= n) break;
+                    const int i = tid + k * T;
                     if (i < n) {
                         const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
                         const float rh = static_cast<float>(__ldg(sv + i) * r64);
@@ -297,16 +305,16 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
             if constexpr (ND > 0) {
                 // pend: no replacement this iteration (the fold clears it)
                 if (pend) {
-                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, true>(P, R, XH, tid, alpha_pend, beta, q)))
+                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, true, T>(P, R, XH, tid, alpha_pend, beta, q)))
                 } else {
-                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, false>(P, R, XH, tid, alpha_pend, beta, q)))
+                    CMCG_DIA_SLOTS(nk, (dia_pupdate<NK, false, T>(P, R, XH, tid, alpha_pend, beta, q)))
                 }
                 pend = false;
             } else {
 #pragma unroll
                 for (int k = 0; k < kSmemNK; ++k) {
-                    if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                    const int i = tid + k * kSmemThreads;
+                    if (k * T >= n) break;   // uniform: skip row slots past the system
+                    const int i = tid + k * T;
                     if (i < n) P[i] = R[i] + beta * P[i];
                 }
             }
@@ -314,19 +322,19 @@ __global__ void __launch_bounds__(kSmemThreads, 1) k_mixed_fast(MixArgs<MI, MO> 
         }
         if (!folded) {
             // fold the pending increments and report the true residual
-            if (ND > 0 && pend) CMCG_DIA_SLOTS(nk, (dia_xinc<NK>(P, XH, tid, alpha_pend)))
+            if (ND > 0 && pend) CMCG_DIA_SLOTS(nk, (dia_xinc<NK, T>(P, XH, tid, alpha_pend)))
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
+                if (k * T >= n) break;   // uniform: skip row slots past the system
+                const int i = tid + k * T;
                 if (i < n) x[i] += __ldg(sv + i) * static_cast<double>(XH[i]);
             }
             __syncthreads();
             double t1[1] = {0.0};
 #pragma unroll
             for (int k = 0; k < kSmemNK; ++k) {
-                if (k * kSmemThreads >= n) break;   // uniform: skip row slots past the system
-                const int i = tid + k * kSmemThreads;
+                if (k * T >= n) break;   // uniform: skip row slots past the system
+                const int i = tid + k * T;
                 if (i < n) {
                     const double r64 = bv[i] - fast_row<double>(a.c.col16, vout, tab[warp][k], lane, LocalX<double>{x});
                     t1[0] += r64 * r64;
@@ -356,20 +364,20 @@ cmcg_status allow_smem_once(K kern, size_t bytes) {
 
 }  // namespace
 
-template <typename MI, typename MO>
-cmcg_status launch_mixed_fast(const MixArgs<MI, MO>& m, int nmax, size_t smem, int nd, int grid, cudaStream_t stream) {
+template <typename MI, typename MO, int T>
+cmcg_status launch_mixed_t(const MixArgs<MI, MO>& m, int nmax, size_t smem, int nd, int grid, cudaStream_t stream) {
     switch (nd) {
         case 0:
-            CMCG_TRY(allow_smem_once(k_mixed_fast<MI, MO, 0>, smem));
-            k_mixed_fast<MI, MO, 0><<<grid, kSmemThreads, smem, stream>>>(m, nmax);
+            CMCG_TRY(allow_smem_once(k_mixed_fast<MI, MO, 0, T>, smem));
+            k_mixed_fast<MI, MO, 0, T><<<grid, T, smem, stream>>>(m, nmax);
             break;
         case 5:
-            CMCG_TRY(allow_smem_once(k_mixed_fast<MI, MO, 5>, smem));
-            k_mixed_fast<MI, MO, 5><<<grid, kSmemThreads, smem, stream>>>(m, nmax);
+            CMCG_TRY(allow_smem_once(k_mixed_fast<MI, MO, 5, T>, smem));
+            k_mixed_fast<MI, MO, 5, T><<<grid, T, smem, stream>>>(m, nmax);
             break;
         case 7:
-            CMCG_TRY(allow_smem_once(k_mixed_fast<MI, MO, 7>, smem));
-            k_mixed_fast<MI, MO, 7><<<grid, kSmemThreads, smem, stream>>>(m, nmax);
+            CMCG_TRY(allow_smem_once(k_mixed_fast<MI, MO, 7, T>, smem));
+            k_mixed_fast<MI, MO, 7, T><<<grid, T, smem, stream>>>(m, nmax);
             break;
         default:
             return fail(CMCG_ERR_INVALID_ARGUMENT, "unsupported number of diagonals");
@@ -377,11 +385,21 @@ cmcg_status launch_mixed_fast(const MixArgs<MI, MO>& m, int nmax, size_t smem, i
     return CMCG_OK;
 }
 
-template cmcg_status launch_mixed_fast<float, float>(const MixArgs<float, float>&, int, size_t, int, int, cudaStream_t);
-template cmcg_status launch_mixed_fast<float, double>(const MixArgs<float, double>&, int, size_t, int, int, cudaStream_t);
-template cmcg_status launch_mixed_fast<__nv_bfloat16, float>(const MixArgs<__nv_bfloat16, float>&, int, size_t, int, int,
-                                                             cudaStream_t);
-template cmcg_status launch_mixed_fast<__nv_bfloat16, double>(const MixArgs<__nv_bfloat16, double>&, int, size_t, int,
-                                                              int, cudaStream_t);
+template <typename MI, typename MO>
+cmcg_status launch_mixed_fast(const MixArgs<MI, MO>& m, int threads, int nmax, size_t smem, int nd, int grid,
+                              cudaStream_t stream) {
+    if (threads == 512) return launch_mixed_t<MI, MO, 512>(m, nmax, smem, nd, grid, stream);
+    if (threads == kSmemThreads) return launch_mixed_t<MI, MO, kSmemThreads>(m, nmax, smem, nd, grid, stream);
+    return fail(CMCG_ERR_INVALID_ARGUMENT, "unsupported CTA size");
+}
+
+template cmcg_status launch_mixed_fast<float, float>(const MixArgs<float, float>&, int, int, size_t, int, int,
+                                                     cudaStream_t);
+template cmcg_status launch_mixed_fast<float, double>(const MixArgs<float, double>&, int, int, size_t, int, int,
+                                                      cudaStream_t);
+template cmcg_status launch_mixed_fast<__nv_bfloat16, float>(const MixArgs<__nv_bfloat16, float>&, int, int, size_t,
+                                                             int, int, cudaStream_t);
+template cmcg_status launch_mixed_fast<__nv_bfloat16, double>(const MixArgs<__nv_bfloat16, double>&, int, int, size_t,
+                                                              int, int, cudaStream_t);
 
 }  // namespace cmcg
