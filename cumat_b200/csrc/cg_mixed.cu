@@ -125,7 +125,8 @@ static_assert(kSmemNK == 16, "CMCG_DIA_SLOTS covers 16 row slots");
 // memory, and nmax is a multiple of 1024. The FP64 residual keeps the compact
 // sliced layout.
 template <typename MI, typename MO, int ND, int T>
-__global__ void __launch_bounds__(T, T / T) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
+// (1024 / T CTAs per SM: 64 registers per thread for both CTA sizes)
+__global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI, MO> a, int nmax) {
     extern __shared__ __align__(16) float smf[];
     __shared__ SliceEnt tab[32][kSmemNK];
     __shared__ float red[2 * (T / 32)];
@@ -359,6 +360,8 @@ __global__ void __launch_bounds__(T, T / T) k_mixed_fast(MixArgs<MI, MO> a, int 
 template <typename K>
 cmcg_status allow_smem_once(K kern, size_t bytes) {
     CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    // the largest shared-memory carveout, so that two 512-thread CTAs fit
+    CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     return CMCG_OK;
 }
 
