@@ -1456,10 +1456,10 @@ struct cmcg_solver_s {
     double refine_delta = 0.0;   // 0: by the inner value type (refine_delta_for)
     // mixed kernel: systems at order positions >= mix_split on 512-thread CTAs
     // (CUMAT_CG_SMALL=0 keeps every system on 1024-thread CTAs)
-    int32_t mix_split = 0;
+    int32_t mix_split = 0, mix_split2 = 0;   // and >= mix_split2 on 256-thread CTAs
     bool mix_small = true;
-    cudaStream_t aux_stream = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t aux_stream[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     bool use_smem = true;     // shared-memory-resident kernels where the systems fit
     bool inner_solve = false; // set while the solver runs the inner solves of a refinement
     bool fast_kernels = true; // compact-layout kernels where available (CUMAT_CG_FAST=0 disables)
@@ -1550,9 +1550,12 @@ cmcg_status build_plan(cmcg_solver s) {
     s->n_sys = n_sys;
     s->max_sys_rows = maxr;
     // last position of the size order with a system above kMixSmallRows rows
-    s->mix_split = 0;
-    for (int32_t i = 0; i < n_sys; ++i)
-        if (ro[order[i] + 1] - ro[order[i]] > kMixSmallRows) s->mix_split = i + 1;
+    s->mix_split = s->mix_split2 = 0;
+    for (int32_t i = 0; i < n_sys; ++i) {
+        const int64_t r = ro[order[i] + 1] - ro[order[i]];
+        if (r > kMixSmallRows) s->mix_split = i + 1;
+        if (r > kMixTinyRows) s->mix_split2 = i + 1;
+    }
     s->n_tiles = static_cast<int32_t>(t_row0.size());
     s->systems_version = p->systems_version;
     // grid path: contiguous tile ranges per CTA, cut into segments at system
@@ -1744,19 +1747,21 @@ cmcg_status allow_smem(K kern, size_t bytes) {
 
 inline int smem_rows(int32_t max_rows) { return (max_rows + 3) / 4 * 4; }
 
-// dynamic shared memory of a 512-thread mixed-kernel CTA such that two fit on
-// an SM next to their static arrays
+// dynamic shared memory of a 512-thread (256-thread) mixed-kernel CTA such
+// that two (four) fit on an SM next to their static arrays
 constexpr size_t kMixSmallSmemLimit = 104 * 1024;
+constexpr size_t kMixTinySmemLimit = 50 * 1024;
 
-// Stream of the highest priority and fork / join events for running the two
-// CTA sizes of the mixed kernel side by side (created on first use).
+// Streams of the highest and the next priority, and fork / join events, for
+// running the CTA tiers of the mixed kernel side by side (created on first use).
 cmcg_status ensure_aux_stream(cmcg_solver s) {
-    if (s->aux_stream) return CMCG_OK;
+    if (s->aux_stream[0]) return CMCG_OK;
     int least = 0, greatest = 0;
     CMCG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    CMCG_CUDA(cudaStreamCreateWithPriority(&s->aux_stream, cudaStreamNonBlocking, greatest));
+    CMCG_CUDA(cudaStreamCreateWithPriority(&s->aux_stream[0], cudaStreamNonBlocking, greatest));
+    CMCG_CUDA(cudaStreamCreateWithPriority(&s->aux_stream[1], cudaStreamNonBlocking, std::min(least, greatest + 1)));
     CMCG_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
-    CMCG_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    for (auto& e : s->ev_join) CMCG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return CMCG_OK;
 }
 
@@ -2186,46 +2191,55 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
             m.dia_unit = s->dia_unit;
             nd = p->dia.max_nd;
         }
-        // Systems past position mix_split of the size order have at most
-        // kMixSmallRows rows: they run on 512-thread CTAs, two per SM, so that
-        // two systems share an SM's latencies; they go to the SMs that the
-        // 1024-thread CTAs of the larger systems leave (those launch first, on
-        // a higher-priority stream, and take every SM while work is left).
-        const int nmax_big = use_dia ? nmax_dia : nmax;
-        const size_t sm_big = use_dia ? sm_dia : sm;
-        const int small_rows = std::min<int>(s->max_sys_rows, kMixSmallRows);
-        const int nmax_small = use_dia ? (small_rows + kDiaBlockRows - 1) / kDiaBlockRows * kDiaBlockRows
-                                       : smem_rows(small_rows);
-        const size_t sm_small = smem_bytes(nmax_small) + halo;
-        int32_t split = n_inst;
-        if (s->mix_small && sm_small <= kMixSmallSmemLimit) split = std::min<int32_t>(n_inst, s->mix_split * ob);
-        MixArgs<MI, MO> mb = m;
-        m.item_begin = 0;
-        m.item_end = split;
-        m.next = s->counters;
-        mb.item_begin = split;
-        mb.item_end = n_inst;
-        mb.next = s->counters + 1;
-        const int grid_big = std::max(1, std::min(split, ctx->sm_count));
-        const int grid_small = std::max(1, std::min(n_inst - split, 2 * ctx->sm_count));
-        if (split == n_inst) {
-            CMCG_TRY((launch_mixed_fast<MI, MO>(m, kSmemThreads, nmax_big, sm_big, nd, grid_big, ctx->stream)));
-            count_launch();
-        } else if (split == 0) {
-            CMCG_TRY((launch_mixed_fast<MI, MO>(mb, 512, nmax_small, sm_small, nd, grid_small, ctx->stream)));
-            count_launch();
-        } else {
+        // Three tiers by position in the size order: systems above
+        // kMixSmallRows rows on 1024-thread CTAs (one per SM), then systems of
+        // at most kMixSmallRows rows on 512-thread CTAs (two per SM), then
+        // systems of at most kMixTinyRows rows on 256-thread CTAs (four per
+        // SM), so that small systems share an SM's latencies. Larger tiers
+        // launch on higher-priority streams and take the SMs first; the next
+        // tier's CTAs fill the SMs they leave.
+        const int cta[3] = {kSmemThreads, 512, 256};
+        const int tier_rows[3] = {s->max_sys_rows, std::min<int>(s->max_sys_rows, kMixSmallRows),
+                                  std::min<int>(s->max_sys_rows, kMixTinyRows)};
+        const size_t tier_limit[3] = {use_dia ? kDiaSmemLimit : sm, kMixSmallSmemLimit, kMixTinySmemLimit};
+        int nmax_t[3];
+        size_t sm_t[3];
+        for (int t = 0; t < 3; ++t) {
+            nmax_t[t] = use_dia ? (tier_rows[t] + kDiaBlockRows - 1) / kDiaBlockRows * kDiaBlockRows
+                                : smem_rows(tier_rows[t]);
+            sm_t[t] = smem_bytes(nmax_t[t]) + halo;
+        }
+        // item ranges [lo[t], lo[t + 1])
+        int32_t lo[4] = {0, n_inst, n_inst, n_inst};
+        if (s->mix_small && sm_t[1] <= tier_limit[1]) {
+            lo[1] = std::min<int32_t>(n_inst, s->mix_split * ob);
+            if (sm_t[2] <= tier_limit[2]) lo[2] = std::max(lo[1], std::min<int32_t>(n_inst, s->mix_split2 * ob));
+        }
+        int tiers[3], nt = 0;
+        for (int t = 0; t < 3; ++t)
+            if (lo[t + 1] > lo[t]) tiers[nt++] = t;
+        if (nt > 1) {
             CMCG_TRY(ensure_aux_stream(s));
             CMCG_CUDA(cudaEventRecord(s->ev_fork, ctx->stream));
-            CMCG_CUDA(cudaStreamWaitEvent(s->aux_stream, s->ev_fork, 0));
-            CMCG_TRY((launch_mixed_fast<MI, MO>(m, kSmemThreads, nmax_big, sm_big, nd, grid_big, s->aux_stream)));
-            CMCG_CHECK_LAUNCH();
-            CMCG_TRY((launch_mixed_fast<MI, MO>(mb, 512, nmax_small, sm_small, nd, grid_small, ctx->stream)));
-            CMCG_CUDA(cudaEventRecord(s->ev_join, s->aux_stream));
-            CMCG_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join, 0));
-            count_launch(2);
         }
-        CMCG_CHECK_LAUNCH();
+        for (int j = 0; j < nt; ++j) {
+            const int t = tiers[j];
+            // the last (smallest) tier runs on the caller's stream
+            cudaStream_t st = (j == nt - 1) ? ctx->stream : s->aux_stream[j];
+            if (j < nt - 1) CMCG_CUDA(cudaStreamWaitEvent(st, s->ev_fork, 0));
+            MixArgs<MI, MO> mt = m;
+            mt.item_begin = lo[t];
+            mt.item_end = lo[t + 1];
+            mt.next = s->counters + t;
+            const int grid = std::max(1, std::min(lo[t + 1] - lo[t], ctx->sm_count * (kSmemThreads / cta[t])));
+            CMCG_TRY((launch_mixed_fast<MI, MO>(mt, cta[t], nmax_t[t], sm_t[t], nd, grid, st)));
+            CMCG_CHECK_LAUNCH();
+            count_launch();
+        }
+        for (int j = 0; j < nt - 1; ++j) {
+            CMCG_CUDA(cudaEventRecord(s->ev_join[j], s->aux_stream[j]));
+            CMCG_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join[j], 0));
+        }
         s->last_inst = n_inst;
         s->last_refined = true;
         return CMCG_OK;
@@ -2511,9 +2525,11 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
     cudaStreamSynchronize(s->A->pat->ctx->stream);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
-    if (s->aux_stream) cudaStreamDestroy(s->aux_stream);
+    for (cudaStream_t st : s->aux_stream)
+        if (st) cudaStreamDestroy(st);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
-    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    for (cudaEvent_t e : s->ev_join)
+        if (e) cudaEventDestroy(e);
     if (s->gexec_mix) cudaGraphExecDestroy(s->gexec_mix);
     if (s->graph_mix) cudaGraphDestroy(s->graph_mix);
     for (void* p : {static_cast<void*>(s->d_order), static_cast<void*>(s->d_tile_row0), static_cast<void*>(s->d_seg_t0),

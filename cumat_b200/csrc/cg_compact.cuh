@@ -187,10 +187,12 @@ struct MixArgs {
     const int32_t* dia_unit;   // [mb][n_sys]: 1 = middle diagonal is offset 0 with all values 1
 };
 
-// Systems of at most this many rows may run on 512-thread CTAs, two per SM.
+// Systems of at most this many rows may run on 512-thread CTAs, two per SM,
+// or on 256-thread CTAs, four per SM.
 constexpr int kMixSmallRows = kSmemNK * 512;
+constexpr int kMixTinyRows = kSmemNK * 256;
 
-// Launches k_mixed_fast (cg_mixed.cu) with `threads` (1024 or 512) threads per
+// Launches k_mixed_fast (cg_mixed.cu) with `threads` (1024, 512 or 256) threads per
 // CTA and `smem` bytes of dynamic shared memory: nd = 0 sliced layout, nd = 5
 // or 7 diagonal layout.
 template <typename MI, typename MO>

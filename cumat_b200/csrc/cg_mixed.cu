@@ -360,7 +360,8 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
 template <typename K>
 cmcg_status allow_smem_once(K kern, size_t bytes) {
     CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
-    // the largest shared-memory carveout, so that two 512-thread CTAs fit
+    // the largest shared-memory carveout, so that two 512-thread or four
+    // 256-thread CTAs fit
     CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     return CMCG_OK;
 }
@@ -391,6 +392,7 @@ cmcg_status launch_mixed_t(const MixArgs<MI, MO>& m, int nmax, size_t smem, int 
 template <typename MI, typename MO>
 cmcg_status launch_mixed_fast(const MixArgs<MI, MO>& m, int threads, int nmax, size_t smem, int nd, int grid,
                               cudaStream_t stream) {
+    if (threads == 256) return launch_mixed_t<MI, MO, 256>(m, nmax, smem, nd, grid, stream);
     if (threads == 512) return launch_mixed_t<MI, MO, 512>(m, nmax, smem, nd, grid, stream);
     if (threads == kSmemThreads) return launch_mixed_t<MI, MO, kSmemThreads>(m, nmax, smem, nd, grid, stream);
     return fail(CMCG_ERR_INVALID_ARGUMENT, "unsupported CTA size");

@@ -289,8 +289,9 @@ def test_reliable_updates_vs_oracle_and_truth(cuda):
     before = m.launch_count()
     x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=A, outer_tol=1e-10, max_outer=200).cpu().numpy()
     # one persistent launch per CTA size: 1024 threads for the systems above
-    # 8192 rows, 512 threads (two CTAs per SM) for the others
-    assert m.launch_count() - before == 2
+    # 8192 rows, 512 threads (two CTAs per SM) down to 4097 rows, 256 threads
+    # (four per SM) for the others
+    assert m.launch_count() - before == 3
     st = cg.system_stats()
     assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-10)
     xo, it_o, up_o, err_o = O.reliable_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, b64, 1e-10)
