@@ -375,16 +375,114 @@ def reference_suite(cm, torch, dev, stream, hbm_peak):
     return out
 
 
-def traffic_per_alg_byte():
-    """DRAM bytes per algorithmic byte of the headline kernel, from the committed
-    ncu summary of its small-case capture (None when the summary is absent)."""
-    p = ROOT / "profiles" / "k_mixed_fast_fv2d512.md"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_alg_byte:"):
-            return float(line.split(":", 1)[1])
-    return None
+# DRAM bytes per algorithmic (streaming-model) byte of k_mixed_fast, measured
+# by ncu (dram__bytes_read.sum + dram__bytes_write.sum over the three CTA-tier
+# launches: 577.3 MB) on the first 512 systems of this batch, whose streaming
+# model is 136.48 GB (`python bench.py --profile-small`); DRAM traffic grows
+# with the work, so the full launch's traffic is this ratio times its model
+# bytes. Source capture: the k_mixed_fast profile summary under profiles/.
+DRAM_PER_MODEL_BYTE = 0.004229
+
+# L1 / shared-memory data-pipe bytes that k_mixed_fast moves per row and inner
+# iteration on a 5-point system in the diagonal block layout with the unit
+# middle diagonal: 4 value loads (16 B) and 5 p reads (20 B) in the product,
+# r read + write (8 B), p read + write and the x-increment read + write
+# (16 B) in the updates. Each FP64 residual replacement moves per row 5 FP32
+# values, 5 16-bit columns and 5 FP64 x gathers (70 B), b (8 B) and the new
+# FP32 residual (4 B), and its fold x += s * xh (read x, xh, s, write x: 28 B).
+L1_BYTES_PER_ROW_ITER = 60
+L1_BYTES_PER_ROW_REPLACEMENT = 110
+# Nominal L1 data-pipe width: 128 B per clock per SM (32 banks x 4 B).
+L1_BYTES_PER_CLK_SM = 128
+
+
+def l1_model_bytes(bt, inner_iters, outer_steps):
+    n = np.diff(bt.row_off).astype(np.float64)
+    return float(np.sum(n * (inner_iters * L1_BYTES_PER_ROW_ITER + outer_steps * L1_BYTES_PER_ROW_REPLACEMENT)))
+
+
+def _ev_time(torch, stream, fn, reps, warm=1):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(reps):
+        fn()
+    e.record(stream)
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def cg_config2(cm, torch, dev, stream, hbm_peak):
+    """The plain method at scale: Jacobi-CG on the 1024^2 Poisson matrix
+    (FP32 CSR, b ~ U[-1,1] seed 1) to 1e-6, at most 4000 iterations, one
+    system (the grid path). Bytes per iteration follow the three-pass
+    schedule: the matrix without the x / y terms (nnz * 8 + (n + 1) * 4) plus
+    13 FP32 n-vectors; the whole working set (about 70 MB) fits in L2, so the
+    GB/s figure is L2-fed, not an HBM number."""
+    from cumat_b200 import problems as P
+    pr = P.poisson2d(1024, 1)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    cg = cm.ConjugateGradient(A).setTolerance(1e-6).setMaxIterations(4000)
+    b = torch.from_numpy(pr.b).to(dev)
+    x = torch.empty_like(b)
+    ms = _ev_time(torch, stream, lambda: cg.solve(b, out=x), 3)
+    it = cg.iterations()
+    per_iter = pr.nnz * 8 + (pr.n + 1) * 4 + 13 * pr.n * 4
+    gbs = per_iter * it / (ms / 1e3) / 1e9
+    return {"ms": round(ms, 3), "iterations": int(it), "error": cg.error(),
+            "iters_per_s": round(it / (ms / 1e3), 1), "us_per_iter": round(ms * 1e3 / it, 2),
+            "gbs_model": round(gbs, 1), "frac_model": round(gbs / hbm_peak, 3)}
+
+
+def precision_c4(cm, torch, dev, stream, reps=2):
+    """The precision configuration: 3D 7-point finite-volume system on a 256^3
+    grid (kappa = exp(N(0, 1)), seed 3, values exact in FP32), solved to a
+    relative residual of 1e-10 by (a) FP32 values + FP32 inner Jacobi-CG with
+    FP64 residual replacement, (b) the same with BF16-stored values, and (c)
+    plain FP64 Jacobi-CG (FP64 values and vectors); each solution's true
+    relative residual |b - A x| / |b| is computed afterwards on the host in FP64
+    (scipy CSR product, outside the timed region)."""
+    import scipy.sparse as sp
+    from cumat_b200 import problems as P
+    pr = P.fv3d(256, 1.0, 3)
+    n = pr.n
+    A64h = sp.csr_matrix((pr.val.astype(np.float64), pr.col, pr.row_ptr), shape=(n, n))
+    b64h = pr.b.astype(np.float64)
+    bn = float(np.linalg.norm(b64h))
+    pat = cm.SparsityPattern.csr(n, n, pr.row_ptr, pr.col)
+    A32 = cm.SparseMatrix(pat, dtype=torch.float32).setData(pr.val)
+    b64 = torch.from_numpy(b64h).to(dev)
+    x = torch.empty_like(b64)
+    out = {"rows": n, "nnz": pr.nnz}
+
+    def true_res():
+        xh = x.cpu().numpy()
+        return float(np.linalg.norm(b64h - A64h @ xh) / bn)
+
+    for name, mat in [("mixed_f32", A32), ("mixed_bf16", None)]:
+        if mat is None:
+            mat = cm.SparseMatrix(pat, dtype=torch.bfloat16).setData(pr.val)
+        cg = cm.ConjugateGradient(mat).setTolerance(1e-4)
+        ms = _ev_time(torch, stream, lambda: cg.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=60, out=x),
+                      reps)
+        st = cg.system_stats()
+        out[name] = {"ms": round(ms, 2), "inner_iterations": int(st["iterations"].max()),
+                     "replacements": int(st["outer"].max()), "status": int(st["status"].max()),
+                     "reported_error": float(st["error"].max()), "true_rel_residual": true_res()}
+        del cg
+    A64 = cm.SparseMatrix(pat, dtype=torch.float64).setData(pr.val.astype(np.float64))
+    cg64 = cm.ConjugateGradient(A64).setTolerance(1e-10).setMaxIterations(20000)
+    ms = _ev_time(torch, stream, lambda: cg64.solve(b64, out=x), reps)
+    out["fp64"] = {"ms": round(ms, 2), "iterations": int(cg64.iterations()), "reported_error": cg64.error(),
+                   "true_rel_residual": true_res()}
+    out["ratio_f32"] = round(out["fp64"]["ms"] / out["mixed_f32"]["ms"], 3)
+    out["ratio_bf16"] = round(out["fp64"]["ms"] / out["mixed_bf16"]["ms"], 3)
+    del cg64, A64, A32
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline(bt, budget_s=15.0):
@@ -437,10 +535,19 @@ def run_ours(args):
     assert np.all(st["status"] == 0), "some systems did not converge"
     assert float(st["error"].max()) < OUTER_TOL
     value = whole_job_rate(N_SYS, world, ms)
-    # roofline of the dominant (only) kernel: the persistent refined launch
-    alg = refined_bytes(bt, st["iterations"].astype(np.float64), st["outer"].astype(np.float64))
-    achieved = alg / (ms / 1e3) / 1e9
-    traffic_ratio = traffic_per_alg_byte()
+    # roofline of the dominant (only) kernel, k_mixed_fast: bound by the L1 /
+    # shared-memory data pipe (vectors live in shared memory, the values of the
+    # systems in flight in L2); the streaming model is kept as model_speedup
+    inner = st["iterations"].astype(np.float64)
+    outer = st["outer"].astype(np.float64)
+    alg = refined_bytes(bt, inner, outer)
+    l1_bytes = l1_model_bytes(bt, inner, outer)
+    sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+    clk_sum = clk.summary()
+    sm_mhz = clk_sum.get("sm_mhz") or 1965.0
+    l1_peak = L1_BYTES_PER_CLK_SM * sm_count * sm_mhz * 1e6 / 1e9
+    l1_achieved = l1_bytes / (ms / 1e3) / 1e9
+    traffic = alg * DRAM_PER_MODEL_BYTE
 
     # plain FP64 batched CG on the same batch (FP64 values and vectors)
     A64 = cm.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
@@ -472,6 +579,9 @@ def run_ours(args):
             extra["spmv_poisson1024"][k]["frac"] = round(extra["spmv_poisson1024"][k]["gbs"] / hbm_peak, 3)
     if rank == 0 and world == 1 and not args.no_suite:
         extra["reference_suite"] = reference_suite(cm, torch, dev, stream, hbm_peak)
+    if rank == 0 and world == 1 and not args.no_configs:
+        extra["cg_poisson1024"] = cg_config2(cm, torch, dev, stream, hbm_peak)
+        extra["precision_c4"] = precision_c4(cm, torch, dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(bt, args.cpu_budget)
@@ -486,20 +596,23 @@ def run_ours(args):
                        "systems_per_gpu": N_SYS, "rows_per_gpu": int(bt.n), "nnz_per_gpu": int(bt.nnz),
                        "parallelism": f"batch sharding x{world}, no collective",
                        "l2": "inputs larger than L2 (FP32 CSR batch %.2f GB)" % ((bt.nnz * 8 + bt.n * 4) / 1e9)},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved / hbm_peak, 3),
-                         "traffic": round(alg * traffic_ratio) if traffic_ratio else None,
-                         "traffic_note": "dram bytes per launch, ncu capture of the first 512 systems scaled by "
-                                         "algorithmic bytes (profiles/k_mixed_fast_fv2d512.md)",
-                         "kernel": "k_mixed_fast", "peak_source": peak_src,
-                         "alg_bytes_per_launch": alg,
-                         "note": "achieved = streaming-model bytes / time; vectors stay on chip and matrices in L2, "
-                                 "so frac > 1 means the kernel avoids the modelled DRAM passes (it is issue-bound)"},
+            "roofline": {"bound": "l1_pipe", "achieved": round(l1_achieved, 1), "peak": round(l1_peak, 1),
+                         "unit": "GB/s", "frac": round(l1_achieved / l1_peak, 3), "traffic": round(traffic),
+                         "kernel": "k_mixed_fast",
+                         "peak_source": f"nominal 128 B/clk/SM x {sm_count} SMs x median sampled SM clock {sm_mhz} MHz",
+                         "l1_bytes_per_launch": l1_bytes,
+                         "dram_frac": round(traffic / (ms / 1e3) / 1e9 / hbm_peak, 4),
+                         "dram_peak_gbs": hbm_peak, "dram_peak_source": peak_src,
+                         "model_speedup": round(alg / (ms / 1e3) / 1e9 / hbm_peak, 3),
+                         "ncu_l1_pipe_pct_by_tier": {"1024": 54.9, "512": 32.8, "256": 19.6},
+                         "note": "achieved = L1-pipe model bytes (60 B per row and inner iteration) / time; traffic = "
+                                 "DRAM bytes per launch scaled from an ncu capture; model_speedup = HBM streaming "
+                                 "model time / measured time"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(N_SYS * world / (ms_e2e / 1e3), 1), "unit": UNIT,
                     "h2d_bytes_per_step": int(bt.n * 8), "d2h_bytes_per_step": int(bt.n * 8)},
             "gpu_launches": int(launches),
-            "clocks": clk.summary(),
+            "clocks": clk_sum,
             "fp64_plain": fp64,
             "mixed_vs_fp64": round(value / fp64["value"], 3),
             "solve_stats": {"inner_iterations_max": int(st["iterations"].max()),
@@ -507,6 +620,24 @@ def run_ours(args):
                             "outer_steps_max": int(st["outer"].max()), "max_error": float(st["error"].max())},
             **extra,
         }
+        # short summary last, so that it survives in any tail of the line
+        hl = {"mixed_vs_fp64": line["mixed_vs_fp64"], "fp64_solves_s": fp64["value"],
+              "e2e_solves_s": line["e2e"]["value"], "l1_frac": line["roofline"]["frac"],
+              "dram_frac": line["roofline"]["dram_frac"]}
+        if "spmv_poisson1024" in extra:
+            sp_ = extra["spmv_poisson1024"]
+            hl.update(spmv_csr_gbs=sp_["csr"]["gbs"], spmv_ell_gbs=sp_["ell"]["gbs"],
+                      spmv_csr_frac=sp_["csr"]["frac"], spmv_ell_frac=sp_["ell"]["frac"])
+        if "cg_poisson1024" in extra:
+            c2 = extra["cg_poisson1024"]
+            hl.update(c2_iters=c2["iterations"], c2_ms=c2["ms"], c2_us_per_iter=c2["us_per_iter"])
+        if "precision_c4" in extra:
+            c4 = extra["precision_c4"]
+            hl.update(c4_f32_ms=c4["mixed_f32"]["ms"], c4_bf16_ms=c4["mixed_bf16"]["ms"], c4_fp64_ms=c4["fp64"]["ms"],
+                      c4_ratio_f32=c4["ratio_f32"], c4_ratio_bf16=c4["ratio_bf16"],
+                      c4_true_res=[c4["mixed_f32"]["true_rel_residual"], c4["mixed_bf16"]["true_rel_residual"],
+                                   c4["fp64"]["true_rel_residual"]])
+        line["headline"] = hl
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -517,12 +648,28 @@ def run_ours(args):
 # reference arm: the reference's bundled Eigen CPU path on the host cores
 # ---------------------------------------------------------------------------
 
+def _standalone_generators():
+    """The seeded generators without importing the package (whose import maps
+    the CUDA library): cumat_b200/problems.py loaded by path and pointed at the
+    oracle's own build of the same generator source (oracle/libgen.so)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_cmgen", ROOT / "cumat_b200" / "problems.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["_cmgen"] = mod   # (its dataclasses look their module up)
+    spec.loader.exec_module(mod)
+    lib = ROOT / "oracle" / "libgen.so"
+    if not lib.exists():
+        raise RuntimeError(f"{lib} missing: run `make -C oracle`")
+    mod._LIB_PATH = lib
+    return mod
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from cumat_b200 import problems as P
     from oracle import oracle as O
+    P = _standalone_generators()
     if O.ref_lib() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libeigen_ref.so (bundled Eigen) not built"}))
         return
@@ -622,6 +769,8 @@ def main():
     ap.add_argument("--no-spmv", action="store_true", help="skip the SpMV GB/s sub-benchmark")
     ap.add_argument("--no-suite", action="store_true",
                     help="skip the reference's own benchmark shapes (SpMV grids 10..10000, CG grids 10..1000)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 1024^2 Poisson Jacobi-CG and the 256^3 precision comparison")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile-small", action="store_true",
                     help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "

@@ -55,14 +55,25 @@ class SparseSolve(torch.autograd.Function):
         x = op.solve(b)
         ctx.op = op
         ctx.values_shape = values.shape
-        ctx.save_for_backward(x)
+        ctx.b_shape = b.shape
+        # the op is shared and later forwards overwrite its values, so the
+        # values of this call are saved and set again before its adjoint
+        ctx.save_for_backward(x, values.detach().to(torch.float64))
         return x
 
     @staticmethod
     def backward(ctx, gx: torch.Tensor):
-        (x,) = ctx.saved_tensors
+        x, values = ctx.saved_tensors
+        ctx.op.set_values(values)
         gb, gA = ctx.op.adjoint(x, gx)
-        return gA.reshape(ctx.values_shape), gb.reshape(x.shape), None
+        gA = gA.reshape(-1, gA.shape[-1])
+        if len(ctx.values_shape) < 2 or ctx.values_shape[0] == 1:
+            # one value set broadcast over the batches of b: its gradient sums them
+            gA = gA.sum(0)
+        gb = gb.reshape(-1, x.shape[-1])
+        if len(ctx.b_shape) < 2 or ctx.b_shape[0] == 1:
+            gb = gb.sum(0)   # a one-batch b broadcast over batched values
+        return gA.reshape(ctx.values_shape), gb.reshape(ctx.b_shape), None
 
 
 def sparse_solve(values: torch.Tensor, b: torch.Tensor, op: SparseSolveOp) -> torch.Tensor:

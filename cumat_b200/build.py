@@ -84,7 +84,13 @@ def build_problems() -> Path:
 def build_oracle() -> None:
     if shutil.which("make") is None:
         raise RuntimeError("make is required to build the oracle")
-    _run(["make", "-s", "-C", str(ROOT / "oracle"), f"OCXX={CXX}"])
+    cmd = ["make", "-s", "-C", str(ROOT / "oracle"), f"OCXX={CXX}"]
+    # the reference checkout, whose bundled Eigen the timed CPU reference is
+    # compiled from; absent on hosts that only run the prebuilt libraries
+    ref = Path(os.environ.get("CUMAT_REFERENCE", "/root/reference"))
+    if (ref / "third-party" / "Eigen" / "Core").exists():
+        cmd.append(f"REF={ref}")
+    _run(cmd)
 
 
 def build_all(verbose: bool = False) -> None:

@@ -1754,14 +1754,32 @@ constexpr size_t kMixTinySmemLimit = 50 * 1024;
 
 // Streams of the highest and the next priority, and fork / join events, for
 // running the CTA tiers of the mixed kernel side by side (created on first use).
+// The five handles are created into locals and kept only when every creation
+// succeeded (a partial set is destroyed), so a failure leaves the solver
+// without any and the next call tries again.
 cmcg_status ensure_aux_stream(cmcg_solver s) {
-    if (s->aux_stream[0]) return CMCG_OK;
+    if (s->aux_stream[0] && s->aux_stream[1] && s->ev_fork && s->ev_join[0] && s->ev_join[1]) return CMCG_OK;
     int least = 0, greatest = 0;
     CMCG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    CMCG_CUDA(cudaStreamCreateWithPriority(&s->aux_stream[0], cudaStreamNonBlocking, greatest));
-    CMCG_CUDA(cudaStreamCreateWithPriority(&s->aux_stream[1], cudaStreamNonBlocking, std::min(least, greatest + 1)));
-    CMCG_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
-    for (auto& e : s->ev_join) CMCG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaStream_t st[2] = {nullptr, nullptr};
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaError_t e = cudaStreamCreateWithPriority(&st[0], cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&st[1], cudaStreamNonBlocking, std::min(least, greatest + 1));
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        for (auto x : st)
+            if (x) cudaStreamDestroy(x);
+        for (auto x : ev)
+            if (x) cudaEventDestroy(x);
+        cudaGetLastError();
+        return fail(CMCG_ERR_CUDA, std::string("creating the tier streams: ") + cudaGetErrorString(e));
+    }
+    s->aux_stream[0] = st[0];
+    s->aux_stream[1] = st[1];
+    s->ev_fork = ev[0];
+    s->ev_join[0] = ev[1];
+    s->ev_join[1] = ev[2];
     return CMCG_OK;
 }
 

@@ -105,7 +105,65 @@ def eigen() -> dict:
     return out
 
 
+SAMPLE = 4096   # rows at which a full-size FP64 direct solution is kept
+
+
+def sample_rows(n: int, seed: int) -> np.ndarray:
+    return np.sort(np.random.default_rng(seed).choice(n, size=min(n, SAMPLE), replace=False)).astype(np.int64)
+
+
+def scale_c2() -> dict:
+    """Configuration 2: 1024^2 Poisson, b ~ U[-1,1] seed 1, Jacobi-CG to 1e-6."""
+    pr = P.poisson2d(1024, 1)
+    out = {}
+    x32, it32, err32 = O.eigen_cg(pr.n, pr.row_ptr, pr.col, pr.val, pr.b, 1e-6, 4000, 1)
+    _, it64, err64 = O.eigen_cg(pr.n, pr.row_ptr, pr.col, pr.val, pr.b.astype(np.float64), 1e-6, 4000, 1)
+    _, ito, erro = O.cg_csr(pr.n, pr.row_ptr, pr.col, pr.val, pr.b, 1e-6, 4000, 1)
+    xl = O.eigen_llt(pr.n, pr.row_ptr, pr.col, pr.val, pr.b.astype(np.float64))
+    idx = sample_rows(pr.n, 21)
+    out.update(c2_eigen_f32_iters=np.int64(it32), c2_eigen_f32_err=np.float64(err32),
+               c2_eigen_f64_iters=np.int64(it64), c2_eigen_f64_err=np.float64(err64),
+               c2_oracle_f32_iters=np.int64(ito[0]), c2_oracle_f32_err=np.float64(erro[0]),
+               c2_idx=idx, c2_llt_x=xl[idx], c2_llt_norm=np.float64(np.linalg.norm(xl)),
+               c2_eigen_f32_x=x32[idx].astype(np.float32))
+    return out
+
+
+def scale_c3() -> dict:
+    """Configuration 3: the 4096-system batch (sides 16..128, sigma 0.5, seed 2),
+    Jacobi-CG per system to 1e-6 in FP32 by the oracle."""
+    bt = P.fv2d_batch(4096, 16, 128, 0.5, 2)
+    _, it, err = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val, bt.b, 1e-6, -1, 1)
+    return {"c3_oracle_iters": it.astype(np.int16), "c3_oracle_err": err.astype(np.float32)}
+
+
+def scale_c4() -> dict:
+    """The precision configuration's 3D system at 64^3 (sigma 1, seed 3)."""
+    p3 = P.fv3d(64, 1.0, 3)
+    b64 = p3.b.astype(np.float64)
+    _, it, err = O.eigen_cg(p3.n, p3.row_ptr, p3.col, p3.val, b64, 1e-10, -1, 1)
+    xl = O.eigen_llt(p3.n, p3.row_ptr, p3.col, p3.val, b64)
+    idx = sample_rows(p3.n, 43)
+    return {"c4_64_eigen_f64_iters": np.int64(it), "c4_64_eigen_f64_err": np.float64(err), "c4_64_idx": idx,
+            "c4_64_llt_x": xl[idx], "c4_64_llt_norm": np.float64(np.linalg.norm(xl))}
+
+
+def scale(parts) -> None:
+    path = HERE / "scale_golden.npz"
+    out = dict(np.load(path)) if path.exists() else {}
+    for part in parts:
+        out = {k: v for k, v in out.items() if not k.startswith(part + "_")}
+        out.update({"c2": scale_c2, "c3": scale_c3, "c4": scale_c4}[part]())
+    np.savez_compressed(path, **out)
+    print("wrote", path, sorted(out))
+
+
 if __name__ == "__main__":
-    (HERE / "reference_kats.json").write_text(json.dumps(kats(), indent=1))
-    np.savez_compressed(HERE / "eigen_golden.npz", **eigen())
-    print("wrote", HERE / "reference_kats.json", HERE / "eigen_golden.npz")
+    if O.ref_lib() is None:
+        raise SystemExit("oracle/_ref/libeigen_ref.so is required (make -C oracle REF=<reference checkout>)")
+    if len(sys.argv) > 1 and sys.argv[1] == "scale":
+        scale(sys.argv[2:] or ["c2", "c3", "c4"])
+    else:
+        (HERE / "reference_kats.json").write_text(json.dumps(kats(), indent=1))
+        np.savez_compressed(HERE / "eigen_golden.npz", **eigen())
+        print("wrote", HERE / "reference_kats.json", HERE / "eigen_golden.npz")

@@ -67,9 +67,12 @@ def test_validation_without_device(native):
 
 def test_product_path_has_no_oracle_dependency():
     # the package never imports, links or loads the oracle
+    # no product source names the oracle outside the build script, which only
+    # compiles it (comments included: the product does not describe itself in
+    # terms of its checker)
     for p in (ROOT / "cumat_b200").rglob("*"):
-        if p.suffix in {".py", ".cu", ".cuh", ".h", ".cpp"}:
-            assert "oracle" not in p.read_text().replace("oracle/", "").lower().split("the oracle")[0] or True
+        if p.suffix in {".py", ".cu", ".cuh", ".h", ".cpp"} and p.name != "build.py":
+            assert "oracle" not in p.read_text().lower(), p
     src = "\n".join(p.read_text() for p in (ROOT / "cumat_b200").rglob("*.py") if p.name != "build.py")
     assert "import oracle" not in src and "from oracle" not in src
     out = subprocess.run(["ldd", str(LIB)], capture_output=True, text=True).stdout if LIB.exists() else ""
