@@ -30,9 +30,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                   "-I" + str(ROOT / "include")]
 
-CU_SOURCES = ["runtime.cu", "spmv.cu", "sell.cu", "cg.cu", "cg_mixed.cu", "cg_coop.cu", "lincomb.cu"]
+CU_SOURCES = ["runtime.cu", "spmv.cu", "sell.cu", "cg.cu", "cg_mixed.cu", "cg_plain.cu", "cg_coop.cu", "lincomb.cu"]
 HEADERS = ["common.cuh", "objects.h", "spmv_dev.cuh", "cg_dev.cuh", "tma.cuh", "cg_smem.cuh", "cg_grid.cuh",
-           "grid_sync.cuh", "cg_compact.cuh"]
+           "grid_sync.cuh", "cg_compact.cuh", "cg_plain.cuh"]
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -49,17 +49,31 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"build step failed: {cmd[0]} ({r.returncode})")
 
 
+def _local_deps(src: Path) -> list[Path]:
+    """The source and every header of this tree it includes, transitively."""
+    import re
+    seen: dict[Path, None] = {}
+    todo = [src]
+    while todo:
+        f = todo.pop()
+        if f in seen or not f.exists():
+            continue
+        seen[f] = None
+        for inc in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read_text(), re.M):
+            todo.append((f.parent / inc).resolve())
+    return list(seen)
+
+
 def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     LIB.mkdir(exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [ROOT / "include" / "cumat_cg.h"]
     jobs = []
     objs = []
     for src in CU_SOURCES:
         s = CSRC / src
         o = OBJ / (src + ".o")
         objs.append(o)
-        if _stale(o, [s] + headers) or ptxas_info:
+        if _stale(o, _local_deps(s)) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
             jobs.append([NVCC] + NVFLAGS + extra + ["-c", str(s), "-o", str(o)])
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:

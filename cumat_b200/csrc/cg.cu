@@ -35,6 +35,7 @@
 #include "cg_smem.cuh"
 #include "common.cuh"
 #include "cg_grid.cuh"
+#include "cg_plain.cuh"
 #include "objects.h"
 
 namespace cmcg {
@@ -852,6 +853,69 @@ __global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __r
 }
 
 // ---------------------------------------------------------------------------
+// Diagonal-layout products of the grid path (stencil-shaped CSR patterns)
+// ---------------------------------------------------------------------------
+
+// q[i] = sum_d v_d[i] p[i + off_d] for the rows [r0, r1) of one system (global
+// rows sr0 .. send - 1; v points at the system's first value), diagonals in
+// ascending offset order, the row's CSR order, with fused multiply-adds:
+// absent entries hold 0 and add 0 * p exactly, so the sum equals the sliced
+// layout's. p indices are clamped into the system, where a zero value meets
+// them. Thread t takes rows r0 + t + kTile u with U rows in flight. UNIT: the
+// middle diagonal is offset 0 with every value 1 and is not loaded.
+// emit(global row, value).
+template <typename VT, typename MT, int ND, bool UNIT, typename F>
+__device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int (&off)[ND], int sr0, int send, int r0,
+                                             int r1, const VT* __restrict__ p, F&& emit) {
+    constexpr int U = sizeof(VT) == 8 ? 2 : 4;
+    for (int i0 = r0 + threadIdx.x; i0 < r1; i0 += U * kTile) {
+        VT acc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * kTile;
+            acc[u] = VT(0);
+            if (i < r1) {
+                const int li = i - sr0;
+                const MT* vr = v + (static_cast<int64_t>(li / kDiaBlockRows) * ND * kDiaBlockRows) + li % kDiaBlockRows;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    if (UNIT && d == ND / 2) {
+                        acc[u] = fma(VT(1), p[i], acc[u]);
+                    } else {
+                        const int c = min(max(i + off[d], sr0), send - 1);
+                        acc[u] = fma(mval<VT>(__ldg(vr + d * kDiaBlockRows)), p[c], acc[u]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (i0 + u * kTile < r1) emit(i0 + u * kTile, acc[u]);
+    }
+}
+
+// The segment's system values and offsets in the diagonal layout.
+template <typename MT, int ND>
+__device__ __forceinline__ const MT* dia_system(const DiaArgs<MT>& d, int b, int s, int (&off)[ND]) {
+#pragma unroll
+    for (int j = 0; j < ND; ++j) off[j] = __ldg(d.off + s * kDiaMax + j);
+    return d.vals + (d.mb == 1 ? 0 : static_cast<int64_t>(b) * d.vstride) + __ldg(d.base + s);
+}
+
+// Values of a CSR matrix in the pattern's diagonal layout, unscaled:
+// dst[b][pos[k]] = vals[b][k] (thread per entry; other slots stay zero).
+template <typename MT>
+__global__ void k_dia_gather(const int32_t* __restrict__ pos, int64_t nnz, const MT* __restrict__ vals, int64_t vstride,
+                             int32_t mb, MT* __restrict__ dst, int64_t dstride) {
+    const int64_t items = nnz * mb;
+    for (int64_t it = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t b = it / nnz, k = it - b * nnz;
+        dst[b * dstride + pos[k]] = vals[b * vstride + k];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Grid path kernels
 // ---------------------------------------------------------------------------
 
@@ -951,8 +1015,9 @@ __global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
     }
 }
 
-// iteration kernel 1: q = A p, p.q -> alpha
-template <typename VT, typename MT, int FMT>
+// iteration kernel 1: q = A p, p.q -> alpha (ND > 0: the values in the
+// pattern's diagonal layout, ND diagonals per system)
+template <typename VT, typename MT, int FMT, int ND = 0>
 __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
     __shared__ VT red[kTile / 32];
     __shared__ bool last_s;
@@ -962,12 +1027,19 @@ __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const VT* p = a.p + vo;
         VT* q = a.q + vo;
-        const auto A = inst_matrix<MT, FMT>(a.m, b_);
         VT acc[1] = {VT(0)};
-        cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, [&](int row, VT v) {
+        const auto emit = [&](int row, VT v) {
             q[row] = v;
             acc[0] += p[row] * v;
-        });
+        };
+        if constexpr (ND > 0) {
+            int off[ND];
+            const MT* v = dia_system<MT, ND>(a.dia, b_, g.s, off);
+            dia_rows_seg<VT, MT, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit);
+        } else {
+            const auto A = inst_matrix<MT, FMT>(a.m, b_);
+            cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, emit);
+        }
         block_sum<VT, 1>(acc, red);
         VT tot[1];
         VT* const parts[1] = {a.part1};
@@ -1179,8 +1251,10 @@ __device__ __forceinline__ bool gmix_tail_status(int32_t st) {
     return st == ST_RUNNING || st == CMCG_SOLVE_BREAKDOWN || st == CMCG_SOLVE_NON_FINITE;
 }
 
-// product q = (S A S) p and p.q -> alpha
-template <typename MI, typename MO>
+// product q = (S A S) p and p.q -> alpha (ND > 0: the scaled values in the
+// pattern's diagonal layout, the unit middle diagonal not loaded where the
+// system's flag says so)
+template <typename MI, typename MO, int ND = 0>
 __global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     __shared__ float red[kTile / 32];
@@ -1191,12 +1265,21 @@ __global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         const float* p = a.p + vo;
         float* q = a.q + vo;
-        const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
         float acc[1] = {0.0f};
-        cta_rows4_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, [&](int row, float v) {
+        const auto emit = [&](int row, float v) {
             q[row] = v;
             acc[0] += p[row] * v;
-        });
+        };
+        if constexpr (ND > 0) {
+            int off[ND];
+            const MI* v = dia_system<MI, ND>(a.dia, b_, g.s, off);
+            const bool unit = a.dia.unit && __ldg(a.dia.unit + (a.dia.mb == 1 ? 0 : b_ * a.n_sys) + g.s);
+            if (unit) dia_rows_seg<float, MI, ND, true>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit);
+            else dia_rows_seg<float, MI, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit);
+        } else {
+            const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
+            cta_rows4_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, emit);
+        }
         block_sum<float, 1>(acc, red);
         float tot[1];
         float* const parts[1] = {a.part1};
@@ -1504,6 +1587,12 @@ struct cmcg_solver_s {
     bool dia_kernels = true;  // CUMAT_CG_DIA=0 keeps the sliced layout
     void* dia_vals = nullptr;      // diagonal-layout values, then the unit-diagonal flags
     int32_t* dia_unit = nullptr;   // inside dia_vals
+    // the matrix's own (unscaled) values in the diagonal layout, for the plain
+    // grid-path product
+    void* dia_plain = nullptr;
+    int64_t dia_plain_stride = 0;
+    int64_t dia_plain_version = -1, dia_plain_plan_id = -1;
+    int32_t dia_plain_dtype = -1;
     int64_t dia_stride = 0;
     int64_t dia_version = -1, dia_plan_id = -1;
     int32_t dia_dtype = -1;
@@ -1899,6 +1988,44 @@ cmcg_status ensure_dia_vals(cmcg_solver s, bool* ok) {
     return CMCG_OK;
 }
 
+// The matrix's values, unscaled, in the pattern's diagonal layout (rebuilt
+// when the values or the systems change); false when the pattern has no
+// diagonal plan or it is switched off.
+cmcg_status ensure_dia_plain(cmcg_solver s, bool* ok) {
+    *ok = false;
+    cmcg_matrix A = s->A;
+    cmcg_pattern p = A->pat;
+    if (!s->dia_kernels || p->format != CMCG_CSR) return CMCG_OK;
+    CMCG_TRY(ensure_dia(p));
+    const DiaPlan& D = p->dia;
+    if (!D.ok) return CMCG_OK;
+    if (!(s->dia_plain && s->dia_plain_version == A->version && s->dia_plain_plan_id == D.plan_id &&
+          s->dia_plain_dtype == A->dtype)) {
+        cmcg_ctx ctx = p->ctx;
+        dev_free(s->dia_plain);
+        s->dia_plain = nullptr;
+        s->dia_plain_stride = (D.n_slots + 7) / 8 * 8 + 8;
+        const size_t bytes = static_cast<size_t>(s->dia_plain_stride) * A->batches * dtype_size(A->dtype);
+        CMCG_TRY(dev_alloc(&s->dia_plain, bytes));
+        CMCG_CUDA(cudaMemsetAsync(s->dia_plain, 0, bytes, ctx->stream));
+        const int blocks = ctx->sm_count * 8;
+#define CMCG_DIA_GATHER(MT)                                                                                   \
+    k_dia_gather<MT><<<blocks, 256, 0, ctx->stream>>>(D.d_pos, p->nnz, static_cast<const MT*>(A->d_vals), A->stride, \
+                                                      A->batches, static_cast<MT*>(s->dia_plain), s->dia_plain_stride)
+        if (A->dtype == CMCG_F32) CMCG_DIA_GATHER(float);
+        else if (A->dtype == CMCG_BF16) CMCG_DIA_GATHER(__nv_bfloat16);
+        else CMCG_DIA_GATHER(double);
+#undef CMCG_DIA_GATHER
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        s->dia_plain_version = A->version;
+        s->dia_plain_plan_id = D.plan_id;
+        s->dia_plain_dtype = A->dtype;
+    }
+    *ok = true;
+    return CMCG_OK;
+}
+
 template <typename VT, typename MT, bool RX>
 cmcg_status launch_cg_fast(cmcg_solver s, SolveArgs<VT, MT>& a, int nmax) {
     cmcg_ctx ctx = s->A->pat->ctx;
@@ -1913,9 +2040,101 @@ cmcg_status launch_cg_fast(cmcg_solver s, SolveArgs<VT, MT>& a, int nmax) {
     return CMCG_OK;
 }
 
+// Plain FP64 batched PCG over the diagonal layout in three CTA tiers (the
+// mixed kernel's machinery): systems above kMixSmallRows rows on 1024-thread
+// CTAs, then up to kMixSmallRows on 512-thread CTAs (two per SM), then up to
+// kMixTinyRows on 256-thread CTAs (four per SM), larger tiers on
+// higher-priority streams. *done = false when the shared memory of p with its
+// halo does not fit.
+template <typename MT>
+cmcg_status run_plain_dia(cmcg_solver s, SolveArgs<double, MT>& a, bool* done) {
+    *done = false;
+    cmcg_pattern p = s->A->pat;
+    cmcg_ctx ctx = p->ctx;
+    const DiaPlan& D = p->dia;
+    const int32_t n_inst = a.n_sys * a.ob;
+    const int cta[3] = {kSmemThreads, 512, 256};
+    const int tier_rows[3] = {s->max_sys_rows, std::min<int>(s->max_sys_rows, kMixSmallRows),
+                              std::min<int>(s->max_sys_rows, kMixTinyRows)};
+    const size_t tier_limit[3] = {kDiaSmemLimit, kMixSmallSmemLimit, kMixTinySmemLimit};
+    int nmax_t[3];
+    size_t sm_t[3];
+    for (int t = 0; t < 3; ++t) {
+        nmax_t[t] = (tier_rows[t] + cta[t] - 1) / cta[t] * cta[t];
+        sm_t[t] = (static_cast<size_t>(nmax_t[t]) + 2 * static_cast<size_t>(D.margin)) * sizeof(double);
+    }
+    if (sm_t[0] > tier_limit[0]) return CMCG_OK;
+    PlainDiaArgs<MT> m{};
+    m.rows = p->rows;
+    m.n_sys = s->n_sys;
+    m.ob = a.ob;
+    m.mb = s->A->batches;
+    m.row_off = p->d_row_off;
+    m.order = s->d_order;
+    m.vals = static_cast<const MT*>(s->dia_plain);
+    m.vstride = s->dia_plain_stride;
+    m.base = D.d_sys_base;
+    m.off = D.d_sys_off;
+    m.margin = D.margin;
+    m.dinv = a.dinv;
+    m.dinv_b = a.dinv_b;
+    m.b = a.b;
+    m.b_b = a.b_b;
+    m.x = a.x;
+    m.r = a.r;
+    m.q = a.q;
+    m.tol = a.tol;
+    m.max_iter = a.max_iter;
+    m.abs_zero_test = a.abs_zero_test;
+    m.st = a.st;
+    int32_t lo[4] = {0, n_inst, n_inst, n_inst};
+    if (s->mix_small && sm_t[1] <= tier_limit[1]) {
+        lo[1] = std::min<int32_t>(n_inst, s->mix_split * a.ob);
+        if (sm_t[2] <= tier_limit[2]) lo[2] = std::max(lo[1], std::min<int32_t>(n_inst, s->mix_split2 * a.ob));
+    }
+    int tiers[3], nt = 0;
+    for (int t = 0; t < 3; ++t)
+        if (lo[t + 1] > lo[t]) tiers[nt++] = t;
+    CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), ctx->stream));
+    if (nt > 1) {
+        CMCG_TRY(ensure_aux_stream(s));
+        CMCG_CUDA(cudaEventRecord(s->ev_fork, ctx->stream));
+    }
+    for (int j = 0; j < nt; ++j) {
+        const int t = tiers[j];
+        cudaStream_t st = (j == nt - 1) ? ctx->stream : s->aux_stream[j];
+        if (j < nt - 1) CMCG_CUDA(cudaStreamWaitEvent(st, s->ev_fork, 0));
+        PlainDiaArgs<MT> mt = m;
+        mt.item_begin = lo[t];
+        mt.item_end = lo[t + 1];
+        mt.next = s->counters + t;
+        const int grid = std::max(1, std::min(lo[t + 1] - lo[t], ctx->sm_count * (kSmemThreads / cta[t])));
+        CMCG_TRY(launch_plain_dia<MT>(mt, cta[t], nmax_t[t], sm_t[t], D.max_nd, grid, st));
+        CMCG_CHECK_LAUNCH();
+        count_launch();
+    }
+    for (int j = 0; j < nt - 1; ++j) {
+        CMCG_CUDA(cudaEventRecord(s->ev_join[j], s->aux_stream[j]));
+        CMCG_CUDA(cudaStreamWaitEvent(ctx->stream, s->ev_join[j], 0));
+    }
+    *done = true;
+    return CMCG_OK;
+}
+
 template <typename VT, typename MT, int FMT>
 cmcg_status run_persistent(cmcg_solver s, SolveArgs<VT, MT>& a) {
     cmcg_ctx ctx = s->A->pat->ctx;
+    // FP64 vectors on stencil-shaped patterns: the diagonal-layout tiers
+    if constexpr (std::is_same<VT, double>::value &&
+                  (std::is_same<MT, double>::value || std::is_same<MT, float>::value)) {
+        if (FMT == CMCG_CSR && !a.guess && s->fast_kernels && s->use_smem && s->max_sys_rows <= kSmemMaxRows) {
+            bool dia = false;
+            CMCG_TRY(ensure_dia_plain(s, &dia));
+            bool done = false;
+            if (dia) CMCG_TRY(run_plain_dia<MT>(s, a, &done));
+            if (done) return CMCG_OK;
+        }
+    }
     if (FMT == CMCG_CSR && compact_ok(s)) {
         const int nmax = smem_rows(s->max_sys_rows);
         // FP32: p, r, x in shared memory (12 B/row); FP64: all three when they
@@ -1969,6 +2188,20 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     else cap = 2 * static_cast<int64_t>(s->max_sys_rows);
     a.loop_cap = static_cast<int32_t>(std::min<int64_t>(cap + 2, INT32_MAX - 1));
 
+    // stencil-shaped CSR patterns: the product reads the diagonal layout
+    int nd = 0;
+    a.dia = DiaArgs<MT>{};
+    if (FMT == CMCG_CSR) {
+        bool dia = false;
+        CMCG_TRY(ensure_dia_plain(s, &dia));
+        if (dia) {
+            const DiaPlan& D = s->A->pat->dia;
+            nd = D.max_nd;
+            a.dia = DiaArgs<MT>{static_cast<const MT*>(s->dia_plain), s->dia_plain_stride, D.d_sys_base, D.d_sys_off,
+                                nullptr, s->A->batches};
+        }
+    }
+
     CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), st));
     k_grid_init<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
     k_grid_init2<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
@@ -2005,7 +2238,13 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
         if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
         cudaStream_t cs = ctx->capture_stream;
         CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        if constexpr (FMT == CMCG_CSR) {
+            if (nd == 5) k_grid_spmv_pq<VT, MT, FMT, 5><<<grid, kTile, 0, cs>>>(a);
+            else if (nd == 7) k_grid_spmv_pq<VT, MT, FMT, 7><<<grid, kTile, 0, cs>>>(a);
+            else k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        } else {
+            k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        }
         k_grid_update<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
         k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
         k_grid_cond<<<1, 1, 0, cs>>>(a.active, a.loops, a.loop_cap, h);
@@ -2437,6 +2676,19 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     m.max_updates = max_outer;
     m.delta = refine_delta_for(s);
     const int grid = s->grid_ctas;
+    // stencil-shaped patterns: the inner product reads the scaled values in the
+    // diagonal layout
+    int nd = 0;
+    if (s->dia_kernels) {
+        bool dia = false;
+        CMCG_TRY(ensure_dia_vals(s, &dia));
+        if (dia) {
+            const DiaPlan& D = p->dia;
+            nd = D.max_nd;
+            m.g.dia = DiaArgs<MI>{static_cast<const MI*>(s->dia_vals), s->dia_stride, D.d_sys_base, D.d_sys_off,
+                                  s->dia_unit, s->A->batches};
+        }
+    }
 
     CMCG_CUDA(cudaMemcpyAsync(b64, b, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), st));
@@ -2471,7 +2723,9 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
         cudaStream_t cs = ctx->capture_stream;
         CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        k_gmix_spmv<MI, MO><<<grid, kTile, 0, cs>>>(m);
+        if (nd == 5) k_gmix_spmv<MI, MO, 5><<<grid, kTile, 0, cs>>>(m);
+        else if (nd == 7) k_gmix_spmv<MI, MO, 7><<<grid, kTile, 0, cs>>>(m);
+        else k_gmix_spmv<MI, MO><<<grid, kTile, 0, cs>>>(m);
         k_gmix_update<MI, MO><<<grid, kTile, 0, cs>>>(m);
         k_gmix_fold<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
         k_gmix_residual<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
@@ -2556,7 +2810,7 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
                     static_cast<void*>(s->d_cseg_sys), static_cast<void*>(s->d_ccta_seg0),
                     static_cast<void*>(s->d_csys_seg0), s->dinv[0], s->dinv[1], s->vec_ws, s->ref_ws, s->part_ws,
                     s->st_ws, static_cast<void*>(s->counters), s->mix_vals, static_cast<void*>(s->mix_s),
-                    s->dia_vals})
+                    s->dia_vals, s->dia_plain})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);
     cmcg_matrix A = s->A;

@@ -21,6 +21,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdlib>
+
 #include "cg_grid.cuh"
 #include "grid_sync.cuh"
 
@@ -57,6 +60,7 @@ struct CoopArgs {
     int32_t* err;
     int32_t n_inst;
     VT* p_alt;   // second p buffer, [batch][rows]
+    BarrierLimits lim;
 };
 
 // Totals of NV partial arrays over the segments of instance `inst` (whole CTA,
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
         block_sum<VT, 2>(acc, red);
         if (threadIdx.x == 0) { a.part1[pidx] = acc[0]; a.part2[pidx] = acc[1]; }
     }
-    if (!grid_barrier(c.sync, c.err, epoch, [&] {
+    if (!grid_barrier(c.sync, c.err, c.lim, epoch, [&] {
             for (int inst = 0; inst < c.n_inst; ++inst) {
                 VT tot[2];
                 coop_inst_sum<VT, MT, 2>(a, parts2, inst, tot, red);
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
         block_sum<VT, 1>(acc, red);
         if (threadIdx.x == 0) a.part1[pidx] = acc[0];
     }
-    if (!grid_barrier(c.sync, c.err, epoch, [&] {
+    if (!grid_barrier(c.sync, c.err, c.lim, epoch, [&] {
             int32_t running = 0;
             for (int inst = 0; inst < c.n_inst; ++inst) {
                 VT tot[1];
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
             block_sum<VT, 1>(acc, red);
             if (threadIdx.x == 0) a.part1[pidx] = acc[0];
         }
-        if (!grid_barrier(c.sync, c.err, epoch, [&] {
+        if (!grid_barrier(c.sync, c.err, c.lim, epoch, [&] {
                 int32_t running = 0;
                 for (int inst = 0; inst < c.n_inst; ++inst) {
                     VT tot[1];
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
             block_sum<VT, 2>(acc, red);
             if (threadIdx.x == 0) { a.part1[pidx] = acc[0]; a.part2[pidx] = acc[1]; }
         }
-        if (!grid_barrier(c.sync, c.err, epoch, [&] {
+        if (!grid_barrier(c.sync, c.err, c.lim, epoch, [&] {
                 int32_t running = 0;
                 for (int inst = 0; inst < c.n_inst; ++inst) {
                     VT tot[2];
@@ -319,7 +323,13 @@ template <typename VT, typename MT, int FMT>
 cmcg_status coop_cg_launch(const SolveArgs<VT, MT>& a, void* sync, int32_t* err, int n_inst, VT* p_alt, int grid,
                            cudaStream_t st) {
     SolveArgs<VT, MT> args = a;
-    CoopArgs<VT> c{static_cast<GridSync*>(sync), err, n_inst, p_alt};
+    // the barrier's wait limit; CUMAT_TEST_GRID_SPINS / CUMAT_TEST_GRID_EXTRA
+    // (tests of the bounded wait) set a short limit and an arrival that never
+    // comes
+    BarrierLimits lim{kGridBarrierSpins, 0u};
+    if (const char* e = std::getenv("CUMAT_TEST_GRID_SPINS")) lim.spins = std::max(1LL, std::atoll(e));
+    if (const char* e = std::getenv("CUMAT_TEST_GRID_EXTRA")) lim.extra = static_cast<unsigned>(std::max(0, std::atoi(e)));
+    CoopArgs<VT> c{static_cast<GridSync*>(sync), err, n_inst, p_alt, lim};
     void* params[] = {&args, &c};
     CMCG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_coop_cg<VT, MT, FMT>), grid, kCoopThreads,
                                           params, 0, st));

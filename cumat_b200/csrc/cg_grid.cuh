@@ -52,6 +52,20 @@ __device__ __forceinline__ InstMatrix<MT, FMT> inst_matrix(const MatArgs<MT>& m,
     return A;
 }
 
+// Diagonal-layout copy of a stencil-shaped CSR pattern's values (see DiaPlan):
+// system s stores diagonal d (offset off[s * 8 + d], ascending) of its local
+// row i at vals[b * vstride + base[s] + 1024 ((i / 1024) nd + d) + i % 1024];
+// absent entries hold zeros. vals == nullptr: not used.
+template <typename MT>
+struct DiaArgs {
+    const MT* vals;
+    int64_t vstride;
+    const int64_t* base;
+    const int32_t* off;
+    const int32_t* unit;   // [mb][n_sys]: middle diagonal is offset 0 with all values 1 (null: none)
+    int32_t mb;
+};
+
 // Per-instance state (instance = batch * n_sys + system).
 struct InstState {
     double* bb;      // |b|^2
@@ -73,6 +87,7 @@ struct InstState {
 template <typename VT, typename MT>
 struct SolveArgs {
     MatArgs<MT> m;
+    DiaArgs<MT> dia;
     int32_t rows, n_sys, ob;
     const int32_t* row_off;
     const int32_t* order;          // persistent: systems, largest first

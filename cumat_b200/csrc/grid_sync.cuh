@@ -15,7 +15,10 @@
 // The poll is bounded: a CTA that waits longer than the limit records
 // DEVERR_GRID_BARRIER in the device error word and the barrier returns false,
 // after which the caller leaves the kernel (the other CTAs then run out at
-// their next barrier the same way).
+// their next barrier the same way). The limit is a launch argument
+// (kGridBarrierSpins unless a test sets a short one), and so is a count of
+// extra arrivals the barrier waits for (0; a test sets 1, an arrival that never
+// comes, to make every CTA's wait run out).
 //
 // Data written before the barrier by other CTAs is read after it through L2
 // (ld.global.cg / volatile), never through the non-coherent read-only path.
@@ -50,14 +53,20 @@ __device__ __forceinline__ void st_release_gpu(unsigned long long* p, unsigned l
 }
 
 // epoch: this CTA's count of barriers passed (same in all CTAs), advanced here.
+struct BarrierLimits {
+    long long spins;        // polls before giving up
+    unsigned extra;         // arrivals expected besides the grid's CTAs (0)
+};
+
 template <typename F>
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, int32_t* err, unsigned long long& epoch, F&& last_step) {
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, int32_t* err, const BarrierLimits& lim,
+                                             unsigned long long& epoch, F&& last_step) {
     __shared__ int s_last, s_ok;
     const unsigned long long target = epoch + 1;
     __syncthreads();
     if (threadIdx.x == 0) {
         s_ok = 1;
-        s_last = atom_add_acq_rel_gpu(&gs->arrive, 1ull) == target * gridDim.x - 1;
+        s_last = atom_add_acq_rel_gpu(&gs->arrive, 1ull) == target * (gridDim.x + lim.extra) - 1;
     }
     __syncthreads();
     if (s_last) {
@@ -67,7 +76,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, int32_t* err, unsigne
     } else if (threadIdx.x == 0) {
         long long spins = 0;
         while (ld_acquire_gpu(&gs->release) < target) {
-            if (++spins > kGridBarrierSpins) {
+            if (++spins > lim.spins) {
                 s_ok = 0;
                 if (err) atomicOr(err, DEVERR_GRID_BARRIER);
                 break;

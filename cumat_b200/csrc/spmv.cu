@@ -18,8 +18,12 @@
 // partial per CTA and a single deterministic combine by the last CTA of each
 // batch (ticket counter, no spinning).
 
+#include <sys/stat.h>
+
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -36,15 +40,12 @@ constexpr int kSpmvThreads = 256;
 
 // Stand-alone product kernels: 0 = row-unrolled CSR / four-rows-per-thread
 // ELLPACK, 1 = warp row-block CSR / thread-per-row ELLPACK, 2 = bulk-staged
-// CSR / four-rows-per-thread ELLPACK. CUMAT_SPMV_VARIANT forces one for the
-// whole process (a comparison knob); unset, each pattern picks by timing on
+// CSR / four-rows-per-thread ELLPACK. CUMAT_SPMV_VARIANT forces one (a
+// comparison knob, read at each product); unset, each pattern picks by timing on
 // its first product (see launch_spmv).
 int spmv_variant() {
-    static const int v = [] {
-        const char* e = std::getenv("CUMAT_SPMV_VARIANT");
-        return e ? std::atoi(e) : -1;
-    }();
-    return v;
+    const char* e = std::getenv("CUMAT_SPMV_VARIANT");
+    return e ? std::atoi(e) : -1;
 }
 
 template <int MODE, typename VT>
@@ -134,6 +135,54 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_rows(const int32_t* _
     }
 }
 
+// ---- CSR, V lanes per row (long or skewed rows) ----------------------------------
+//
+// V lanes (4, 8, 16 or 32) share a row: its entries are read in 4-entry chunks
+// aligned to 16 bytes (one int4 of column indices and one 16-byte load of
+// values per lane and chunk, 8-byte for BF16; the index and value arrays are
+// padded so the last chunk stays in bounds, and entries of a chunk outside the
+// row are masked), lane l of the group taking chunks l, l + V, ...; the group's
+// partial sums are combined with __shfl_xor_sync. Used for rows much longer
+// than a stencil's, where thread per row serialises a long row on one thread.
+
+template <typename MT, typename VT, int MODE, int V>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_vec(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                               const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                               const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                               VT* __restrict__ y, int32_t rows, int32_t ob) {
+    static_assert(V >= 4 && V <= 32 && (V & (V - 1)) == 0, "V lanes per row: 4, 8, 16 or 32");
+    constexpr int GPW = 32 / V;   // rows per warp and step
+    const int lane = threadIdx.x & 31, sub = lane & (V - 1);
+    const int64_t items = static_cast<int64_t>(rows) * ob;
+    const int64_t warp = (static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x) >> 5;
+    const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * kSpmvThreads) >> 5;
+    // the loop bound is the warp's (uniform), so every lane reaches the shuffles
+    for (int64_t w = warp; w * GPW < items; w += nwarps) {
+        const int64_t it = w * GPW + lane / V;
+        VT acc = VT(0);
+        if (it < items) {
+            const int b = static_cast<int>(it / rows);
+            const int r = static_cast<int>(it - static_cast<int64_t>(b) * rows);
+            const MT* v = vals + (mb == 1 ? 0 : b * vstride);
+            const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+            const int a = __ldg(rp + r), e = __ldg(rp + r + 1);
+#pragma unroll 2
+            for (int k = (a & ~3) + 4 * sub; k < e; k += 4 * V) {
+                const int4 c = __ldg(reinterpret_cast<const int4*>(ci + k));
+                Vals4<MT> w4;
+                w4.load(v + k);
+                if (k >= a && k < e) acc += mval<VT>(w4.v[0]) * __ldg(xv + c.x);
+                if (k + 1 >= a && k + 1 < e) acc += mval<VT>(w4.v[1]) * __ldg(xv + c.y);
+                if (k + 2 >= a && k + 2 < e) acc += mval<VT>(w4.v[2]) * __ldg(xv + c.z);
+                if (k + 3 >= a && k + 3 < e) acc += mval<VT>(w4.v[3]) * __ldg(xv + c.w);
+            }
+        }
+#pragma unroll
+        for (int o = V / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        if (sub == 0 && it < items) assign_out<MODE>(y + it, acc);
+    }
+}
+
 // ---- bulk-staged CSR product ----------------------------------------------------
 //
 // Persistent CTAs walk precomputed row tiles (<= kTileRows rows, <= kTileNnz
@@ -165,7 +214,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_spmv_csr_tma(const int32_t* __r
                                                              const VT* __restrict__ x, int32_t cols, int32_t xb,
                                                              VT* __restrict__ y, int32_t rows, int32_t ob,
                                                              const int32_t* __restrict__ tiles, int32_t ntiles,
-                                                             int32_t* err) {
+                                                             int32_t* err, uint32_t wait_limit, int32_t test_no_copy) {
     using L = TileSmem<MT>;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar[2];
@@ -192,6 +241,9 @@ __global__ void __launch_bounds__(kTmaThreads) k_spmv_csr_tma(const int32_t* __r
             bytes += static_cast<uint32_t>(cb - ca) * 4u + static_cast<uint32_t>(vb - va) * static_cast<uint32_t>(sizeof(MT));
         }
         mbar_arrive_expect_tx(&bar[s], bytes);
+        // (test of the bounded wait: the stage is armed but nothing is copied,
+        // so the wait runs out with no copy in flight)
+        if (test_no_copy) return;
         bulk_g2s(st, rp + ra, static_cast<uint32_t>(rb - ra) * 4u, &bar[s]);
         if (stage_entries) {
             const MT* vb_ = vals + (mb == 1 ? 0 : b * vstride);
@@ -214,7 +266,18 @@ __global__ void __launch_bounds__(kTmaThreads) k_spmv_csr_tma(const int32_t* __r
     for (int64_t it = blockIdx.x; it < items; it += G, ++j) {
         const int s = j & 1;
         // uniform over the CTA: the compute below has barriers
-        const bool ok = __syncthreads_and(mbar_wait(&bar[s], (j >> 1) & 1, err)) != 0;
+        const bool ok = __syncthreads_and(mbar_wait(&bar[s], (j >> 1) & 1, err, wait_limit)) != 0;
+        if (!ok) {
+            // the wait ran out (recorded in *err): wait once more, bounded, for
+            // this stage's copies and for the other stage's, which may still be
+            // in flight, then leave without issuing anything
+            if (tid == 0) {
+                mbar_wait(&bar[s], (j >> 1) & 1, nullptr, wait_limit);
+                if (it + G < items) mbar_wait(&bar[s ^ 1], ((j + 1) >> 1) & 1, nullptr, wait_limit);
+            }
+            __syncthreads();
+            return;
+        }
         const int b = static_cast<int>(it / ntiles);
         const int t = static_cast<int>(it - static_cast<int64_t>(b) * ntiles);
         const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
@@ -225,7 +288,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_spmv_csr_tma(const int32_t* __r
         const int ra = r0 & ~3;
         const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
         VT* yv = y + static_cast<int64_t>(b) * rows;
-        if (ok) {
+        {
             const int k0 = srp[r0 - ra], k1 = srp[r1 - ra];
             if (k1 - k0 <= kTileNnz) {
                 const int ca = k0 & ~3, va = k0 & ~(L::kEpv - 1);
@@ -371,9 +434,16 @@ cmcg_status launch_csr_tma(cmcg_matrix A, const VT* xv, int32_t xb, VT* yv, int3
     CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTmaThreads, sm));
     const int64_t items = static_cast<int64_t>(p->n_spmv_tiles) * ob;
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, static_cast<int64_t>(ctx->sm_count) * std::max(occ, 1))));
+    // wait limit of the stage barriers; CUMAT_TEST_WAIT_LIMIT and
+    // CUMAT_TEST_NO_COPY (tests of the bounded wait) set a short limit and
+    // stages that are armed but never filled
+    uint32_t limit = kWaitLimit;
+    int32_t no_copy = 0;
+    if (const char* e = std::getenv("CUMAT_TEST_WAIT_LIMIT")) limit = static_cast<uint32_t>(std::max(1, std::atoi(e)));
+    if (const char* e = std::getenv("CUMAT_TEST_NO_COPY")) no_copy = std::atoi(e) != 0;
     kern<<<grid, kTmaThreads, sm, ctx->stream>>>(p->d_row_ptr, p->d_col, static_cast<const MT*>(A->d_vals), A->stride,
                                                 A->batches, xv, p->cols, xb, yv, p->rows, ob, p->d_spmv_tiles,
-                                                p->n_spmv_tiles, ctx->d_err);
+                                                p->n_spmv_tiles, ctx->d_err, limit, no_copy);
     count_launch();
     CMCG_CHECK_LAUNCH();
     return CMCG_OK;
@@ -423,6 +493,30 @@ cmcg_status launch_spmv_variant(cmcg_matrix A, const void* x, int32_t xb, void* 
         if (mode == CMCG_ASSIGN) return launch_csr_tma<MT, VT, CMCG_ASSIGN>(A, xv, xb, yv, ob);
         if (mode == CMCG_ADD) return launch_csr_tma<MT, VT, CMCG_ADD>(A, xv, xb, yv, ob);
         return launch_csr_tma<MT, VT, CMCG_SUB>(A, xv, xb, yv, ob);
+    }
+    if (p->format == CMCG_CSR && variant >= 3 && variant <= 6) {
+        const int V = 4 << (variant - 3);
+        const int64_t threads = static_cast<int64_t>(p->rows) * ob * V;
+        const int needed = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
+#define CMCG_LAUNCH_CSR_VEC(M, VV)                                                                                   \
+    k_spmv_csr_vec<MT, VT, M, VV><<<resident_grid(k_spmv_csr_vec<MT, VT, M, VV>, needed, ctx->sm_count), kSpmvThreads, \
+                                    0, ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride, A->batches, xv, p->cols,  \
+                                                      xb, yv, p->rows, ob)
+#define CMCG_LAUNCH_CSR_VEC_V(M)              \
+    switch (V) {                              \
+        case 4: CMCG_LAUNCH_CSR_VEC(M, 4); break;   \
+        case 8: CMCG_LAUNCH_CSR_VEC(M, 8); break;   \
+        case 16: CMCG_LAUNCH_CSR_VEC(M, 16); break; \
+        default: CMCG_LAUNCH_CSR_VEC(M, 32);        \
+    }
+        if (mode == CMCG_ASSIGN) { CMCG_LAUNCH_CSR_VEC_V(CMCG_ASSIGN) }
+        else if (mode == CMCG_ADD) { CMCG_LAUNCH_CSR_VEC_V(CMCG_ADD) }
+        else { CMCG_LAUNCH_CSR_VEC_V(CMCG_SUB) }
+#undef CMCG_LAUNCH_CSR_VEC_V
+#undef CMCG_LAUNCH_CSR_VEC
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        return CMCG_OK;
     }
     if (p->format == CMCG_CSR && variant == 0) {
         const int64_t threads = static_cast<int64_t>(p->rows) * ob;
@@ -619,8 +713,83 @@ cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub,
 
 }  // namespace
 
+// Row-length rule of the CSR product (deterministic, from the pattern): a
+// longest row of at least 256 entries and 32 times the mean takes a warp per
+// row (V = 32); a mean row length of at least 12 takes V lanes per row with V
+// about the row's number of 4-entry chunks (4 .. 32); shorter rows stay
+// thread per row. Returns the variant (3 + log2(V / 4)) or -1.
+int csr_vec_variant(cmcg_pattern p) {
+    const auto& rp = p->h_row_ptr;
+    int64_t mx = 0;
+    for (int32_t r = 0; r < p->rows; ++r) mx = std::max<int64_t>(mx, rp[r + 1] - rp[r]);
+    const double mean = static_cast<double>(p->nnz) / std::max(1, p->rows);
+    if (mx >= 256 && static_cast<double>(mx) >= 32.0 * mean) return 6;
+    if (mean < 12.0) return -1;
+    const int chunks = static_cast<int>(mean / 4.0) + 2;
+    int v = 4, variant = 3;
+    while (v < chunks && v < 32) {
+        v *= 2;
+        ++variant;
+    }
+    return variant;
+}
+
+// Persistent cache of the timed choices: one line "key variant" per tuned
+// case, key = GPU name | format | value type | vector type | rows | nnz |
+// width, in $CUMAT_TUNE_CACHE (default ~/.cache/cumat_b200/spmv_tune.txt;
+// empty: no file). A process reuses the choice a previous one timed on the
+// same GPU model and pattern shape instead of timing again.
+std::mutex g_tune_mu;
+
+std::string tune_path() {
+    if (const char* e = std::getenv("CUMAT_TUNE_CACHE")) return e;
+    const char* h = std::getenv("HOME");
+    return h ? std::string(h) + "/.cache/cumat_b200/spmv_tune.txt" : std::string();
+}
+
+std::string tune_key(cmcg_pattern p, int mt, int vt) {
+    cudaDeviceProp prop{};
+    std::string gpu = cudaGetDeviceProperties(&prop, p->ctx->device) == cudaSuccess ? prop.name : "unknown";
+    for (char& c : gpu)
+        if (c == ' ' || c == '|') c = '_';
+    return gpu + "|" + (p->format == CMCG_CSR ? "csr" : "ell") + "|" + std::to_string(mt) + "|" + std::to_string(vt) +
+           "|" + std::to_string(p->rows) + "|" + std::to_string(p->nnz) + "|" + std::to_string(p->width);
+}
+
+int tune_lookup(const std::string& key) {
+    const std::string path = tune_path();
+    if (path.empty()) return -1;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return -1;
+    char line[512];
+    int found = -1;
+    while (std::fgets(line, sizeof(line), f)) {
+        const char* sp = std::strrchr(line, ' ');
+        if (!sp) continue;
+        if (std::string(line, sp - line) == key) found = std::atoi(sp + 1);   // the last entry wins
+    }
+    std::fclose(f);
+    return found;
+}
+
+void tune_store(const std::string& key, int variant) {
+    const std::string path = tune_path();
+    if (path.empty()) return;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    // create the parent directories (a failure shows as the open failing)
+    for (size_t i = path.find('/', 1); i != std::string::npos; i = path.find('/', i + 1))
+        ::mkdir(path.substr(0, i).c_str(), 0755);
+    if (FILE* f = std::fopen(path.c_str(), "a")) {
+        std::fprintf(f, "%s %d\n", key.c_str(), variant);
+        std::fclose(f);
+    }
+}
+
 // Internal entry used by the solver (device pointers, no validation).
-// Autotuner of the stand-alone product: among the kernels that add every
+// Autotuner of the stand-alone product: CSR patterns with long or skewed rows
+// take the V-lanes-per-row kernel by the row-length rule above. Otherwise,
+// among the kernels that add every
 // row's products in the same order (CSR: row-unrolled, bulk-staged; ELLPACK:
 // four rows per thread, thread per row), so that the choice never changes a
 // result, it times each candidate on the caller's operands (one warm-up and
@@ -636,6 +805,19 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     cmcg_pattern p = A->pat;
     int8_t& choice = p->spmv_choice[DT<MT>::id][DT<VT>::id];
     if (choice >= 0) return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, choice);
+    if (p->format == CMCG_CSR) {
+        const int vec = csr_vec_variant(p);
+        if (vec >= 0) {
+            choice = static_cast<int8_t>(vec);
+            return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, vec);
+        }
+    }
+    const std::string key = tune_key(p, DT<MT>::id, DT<VT>::id);
+    const int cached = tune_lookup(key);
+    if (cached == 0 || cached == 1 || cached == 2) {
+        choice = static_cast<int8_t>(cached);
+        return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, cached);
+    }
     cudaStream_t st = p->ctx->stream;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (mode != CMCG_ASSIGN || cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
@@ -669,6 +851,7 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     cudaEventDestroy(e1);
     if (rc != CMCG_OK) return rc;
     choice = static_cast<int8_t>(pick);
+    tune_store(key, pick);
     // the last candidate's output is in y; rerun the pick if it was another one
     return pick == cands[1] ? CMCG_OK : launch_spmv_variant<MT, VT>(A, x, xb, y, mode, pick);
 }

@@ -51,10 +51,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return done != 0;
 }
 
-// Bounded wait for the phase with the given parity; false if it timed out
-// (the error is recorded in *err).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* err) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
+// Bounded wait (limit try_wait rounds) for the phase with the given parity;
+// false if it timed out (the error is recorded in *err).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* err, uint32_t limit = kWaitLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     if (err) atomicOr(err, DEVERR_MBAR_TIMEOUT);
     return false;

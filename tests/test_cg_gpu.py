@@ -629,3 +629,95 @@ def test_plain_fp64_cg_matches_eigen_3d(cuda):
         assert abs(cg.iterations() - int(EIG["fv3d12_f64_iters_1e-10"])) <= 2
         xt = EIG["fv3d12_llt_x"]
         assert np.linalg.norm(x - xt) / np.linalg.norm(xt) < 1e-8
+
+
+def test_fp64_diagonal_tiers_match_sliced_and_oracle(cuda, monkeypatch):
+    # plain FP64 PCG on stencil patterns runs on the diagonal layout in three
+    # CTA tiers (1024 / 512 / 256 threads by system size); with
+    # CUMAT_CG_DIA=0 on the sliced layout with one CTA size. The sums are taken
+    # in other orders, so counts agree to +-1 and solutions to FP64 rounding.
+    m = cm()
+    bt = P.fv2d_batch(60, 16, 128, 0.5, 41)
+    assert bt.sides.min() ** 2 <= 4096 < 8192 < bt.sides.max() ** 2   # every tier has systems
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    A = m.SparseMatrix(p, dtype=torch.float64).setData(bt.val.astype(np.float64))
+    b64 = bt.b.astype(np.float64)
+    cg = m.ConjugateGradient(A).setTolerance(1e-10)
+    x1 = cg.solve(torch.from_numpy(b64).to(cuda)).cpu().numpy()
+    s1 = cg.system_stats()
+    monkeypatch.setenv("CUMAT_CG_DIA", "0")
+    cg0 = m.ConjugateGradient(A).setTolerance(1e-10)
+    x0 = cg0.solve(torch.from_numpy(b64).to(cuda)).cpu().numpy()
+    s0 = cg0.system_stats()
+    assert np.all(s1["status"] == 0) and np.all(s0["status"] == 0)
+    assert np.abs(s1["iterations"] - s0["iterations"]).max() <= 1
+    _, it_o, _ = O.cg_packed(bt.row_off, bt.row_ptr, bt.col, bt.val.astype(np.float64), b64, 1e-10)
+    assert np.abs(s1["iterations"] - it_o).max() <= 2
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(x1[r0:r1] - x0[r0:r1]) <= 1e-8 * np.linalg.norm(x0[r0:r1])
+
+
+def test_fp64_diagonal_tiers_mixed_offset_sets(cuda, monkeypatch):
+    # 2D (5 offsets) and 1D (3 offsets in 5 diagonal slots) systems in one
+    # batch on the plain FP64 diagonal kernel, against the oracle
+    m = cm()
+    rng = np.random.default_rng(43)
+    bt = P.fv2d_batch(5, 16, 80, 0.5, 47)
+    rps, cols, vals, offs = [bt.row_ptr], [bt.col], [bt.val], list(bt.row_off)
+    n, nnz = bt.n, int(bt.row_ptr[-1])
+    for m1 in (300, 5000, 9000):
+        rp, c, v = _tridiag(m1, rng)
+        rps.append(rp[1:] + nnz); cols.append(c + n); vals.append(v)
+        n += m1; nnz += int(rp[-1]); offs.append(n)
+    row_ptr, col, val = np.concatenate(rps), np.concatenate(cols), np.concatenate(vals)
+    row_off = np.array(offs, np.int64)
+    b = rng.uniform(-1.0, 1.0, n)
+    p = m.SparsityPattern.csr(n, n, row_ptr, col)
+    p.set_systems(row_off)
+    A = m.SparseMatrix(p, dtype=torch.float64).setData(val.astype(np.float64))
+    cg = m.ConjugateGradient(A).setTolerance(1e-10)
+    x = cg.solve(torch.from_numpy(b).to(cuda)).cpu().numpy()
+    st = cg.system_stats()
+    _, it_o, _ = O.cg_packed(row_off, row_ptr, col, val.astype(np.float64), b, 1e-10)
+    assert np.all(st["status"] == 0) and np.abs(st["iterations"] - it_o).max() <= 2
+    r = b - O.spmv_csr_f32_in_f64(n, n, row_ptr, col, val, x)[0]
+    for s in range(len(offs) - 1):
+        r0, r1 = offs[s], offs[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b[r0:r1]) < 2e-10
+
+
+@pytest.mark.parametrize("kind", ["fp64", "mixed_f32", "mixed_bf16"])
+def test_grid_diagonal_layout_matches_sliced(cuda, monkeypatch, kind):
+    # the grid path (one 3D system, graph loop) reads the values in the
+    # diagonal layout on stencil patterns; the products add the same terms in
+    # the same order as the sliced layout, so both runs agree bit for bit
+    m = cm()
+    monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    p3 = P.fv3d(32, 1.0, 5)
+    pat = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    A64 = m.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
+    A32 = m.SparseMatrix(pat, dtype=torch.float32).setData(p3.val)
+    b64 = torch.from_numpy(p3.b.astype(np.float64)).to(cuda)
+
+    def run():
+        if kind == "fp64":
+            cg = m.ConjugateGradient(A64).setTolerance(1e-10).set_path(2)
+            x = cg.solve(b64)
+        else:
+            Ai = A32 if kind == "mixed_f32" else m.SparseMatrix(pat, dtype=torch.bfloat16).setData(p3.val)
+            cg = m.ConjugateGradient(Ai).setTolerance(1e-4).set_path(2)
+            x = cg.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=60)
+        return x.cpu().numpy(), cg.system_stats()
+
+    x1, s1 = run()
+    monkeypatch.setenv("CUMAT_CG_DIA", "0")
+    x0, s0 = run()
+    assert np.array_equal(s1["iterations"], s0["iterations"]) and np.array_equal(s1["status"], s0["status"])
+    assert np.array_equal(x1, x0, equal_nan=True)
+    if kind == "mixed_bf16":
+        return   # (whether BF16 values converge here depends on the conditioning)
+    assert s1["status"][0] == 0
+    r = p3.b.astype(np.float64) - O.spmv_csr_f32_in_f64(p3.n, p3.n, p3.row_ptr, p3.col, p3.val, x1)[0]
+    assert np.linalg.norm(r) / np.linalg.norm(p3.b.astype(np.float64)) < 1.5e-10

@@ -215,3 +215,89 @@ def test_autotuned_product_is_deterministic(cuda, fmt):
     assert np.array_equal(y1, y2)
     yo = O.spmv_csr(pr.n, pr.n, pr.row_ptr, pr.col, vals, pr.b)[0]
     assert np.allclose(y1, yo, rtol=1e-6, atol=1e-6 * np.abs(yo).max())
+
+
+def _row_abs_sums(rp, w):
+    """Per-row sums of w over CSR rows (0 for empty rows)."""
+    out = np.add.reduceat(np.append(w, 0.0), rp[:-1].astype(np.int64))
+    out[np.diff(rp) == 0] = 0.0
+    return out
+
+
+def _power_law_csr(n, seed, alpha=1.1, scale=2.0, max_len=None):
+    """Rows whose lengths follow a heavy-tailed (Pareto) law, sorted distinct
+    random columns, values U[-1, 1]: the skewed case thread-per-row handles
+    worst (a few rows hold thousands of entries)."""
+    rng = np.random.default_rng(seed)
+    max_len = max_len or n
+    lens = np.minimum((rng.pareto(alpha, n) * scale + 1).astype(np.int64), max_len)
+    rp = np.zeros(n + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    col = np.empty(int(rp[-1]), np.int32)
+    for r in range(n):
+        col[rp[r]:rp[r + 1]] = np.sort(rng.choice(n, size=int(lens[r]), replace=False))
+    val = rng.uniform(-1.0, 1.0, col.size)
+    return rp.astype(np.int32), col, val
+
+
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+def test_power_law_csr_vs_oracle(cuda, dt):
+    # the row-length rule gives this pattern the warp-per-row kernel (its
+    # longest rows are far above 32 times the mean)
+    cm = _cm()
+    n = 20000
+    rp, col, val = _power_law_csr(n, 5)
+    lens = np.diff(rp)
+    assert lens.max() >= 256 and lens.max() >= 32 * lens.mean()
+    npdt = np.float32 if dt == torch.float32 else np.float64
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(n, n, rp, col), dtype=dt).setData(val.astype(npdt))
+    xh = np.random.default_rng(6).uniform(-1.0, 1.0, n).astype(npdt)
+    y = (A * torch.from_numpy(xh).to(cuda)).cpu().numpy()
+    ref = O.spmv_csr(n, n, rp, col, val.astype(npdt), xh)[0].astype(np.float64)
+    scale = _row_abs_sums(rp, np.abs(val) * np.abs(xh.astype(np.float64))[col])
+    tol = 1e-6 if dt == torch.float32 else 1e-13
+    # relative to the row's sum of |a_ij x_j| (the conditioning of each row sum)
+    assert np.all(np.abs(y - ref) <= tol * np.maximum(scale, 1e-30)), np.max(np.abs(y - ref) / scale)
+
+
+@pytest.mark.parametrize("variant", [3, 4, 5, 6])
+def test_lanes_per_row_kernels_vs_oracle(cuda, monkeypatch, variant):
+    # every V-lanes-per-row kernel (V = 4, 8, 16, 32), forced, on a random CSR
+    # matrix with rows of 0..60 entries, batched values and vectors
+    cm = _cm()
+    monkeypatch.setenv("CUMAT_SPMV_VARIANT", str(variant))
+    rng = np.random.default_rng(variant)
+    n = 3000
+    lens = rng.integers(0, 61, n)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    col = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) for k in lens]).astype(np.int32)
+    vals = rng.uniform(-1.0, 1.0, (2, col.size)).astype(np.float32)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(n, n, rp, col), batches=2).setData(vals)
+    X = rng.uniform(-1.0, 1.0, (2, n)).astype(np.float32)
+    y = A.product(torch.from_numpy(X).to(cuda)).cpu().numpy()
+    ref = O.spmv_csr(n, n, rp, col, vals, X)
+    scale = np.stack([_row_abs_sums(rp, np.abs(vals[b]).astype(np.float64) * np.abs(X[b])[col]) for b in range(2)])
+    scale[:, lens == 0] = 1.0
+    assert np.all(np.abs(y - ref) <= 1e-6 * scale)
+    assert np.all(y[:, lens == 0] == 0)
+
+
+def test_tuning_cache_records_the_choice(cuda, monkeypatch, tmp_path):
+    # a timed choice is written to the cache file and read back by a new
+    # pattern of the same shape (no second timing: one launch per product)
+    cm = _cm()
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("CUMAT_TUNE_CACHE", str(cache))
+    pr = P.poisson2d(300, 2)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    x = torch.from_numpy(pr.b).to(cuda)
+    y0 = (A * x).cpu().numpy()
+    lines = cache.read_text().split("\n")
+    key = f"|csr|0|0|{pr.n}|{pr.nnz}|0 "
+    assert any(key in (l + " ") and l.split()[-1] in ("0", "2") for l in lines if l), lines
+    B = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    before = cm.launch_count()
+    y1 = (B * x).cpu().numpy()
+    assert cm.launch_count() - before == 1
+    assert np.array_equal(y0, y1)
