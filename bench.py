@@ -6,15 +6,18 @@ variable-coefficient diffusion systems (5-point finite volume, kappa = exp(g),
 g ~ N(0, 0.5^2), sides ~ U{16..128}, seed 2, FP32 CSR packed into one buffer)
 solved to a relative residual of 1e-10 by the mixed-precision solver: FP32 CG
 on the Jacobi-scaled systems whose residual is replaced by the FP64 residual
-b - A x whenever it has dropped by 0.1 (reliable updates), FP64 solution and
-norms, one persistent launch for the whole batch. Metric: solves/s. The same
-line also carries plain FP64 batched CG on the same batch (the comparison named
-by the metric), SpMV GB/s on the 1024^2 Poisson matrix (CSR and ELLPACK), the
-reference's own benchmark shapes (SpMV on 2D Poisson grids 10..10000, CG on
-grids 10..1000) beside its published times, the HBM roofline of the dominant
+b - A x whenever it has dropped by 0.01 (reliable updates), FP64 solution and
+norms, one persistent launch per CTA size. Metric: solves/s. The same line
+also carries plain FP64 batched CG on the same batch (the comparison named by
+the metric, on the same diagonal layout and CTA tiers), the mixed solve on the
+sliced layout (patterns that are not stencils), SpMV GB/s on the 1024^2
+Poisson matrix (CSR and ELLPACK), Jacobi-CG on that matrix (configuration 2),
+the 256^3 precision configuration (FP32 / BF16 values with FP64 residual
+replacement against plain FP64, true residuals), the reference's own
+benchmark shapes beside its published times, the roofline of the dominant
 kernel, the CPU baseline (the reference's bundled Eigen FP64 Jacobi-CG, all
 host threads) and the end-to-end number through the public API with host
-buffers.
+buffers. A short summary closes the line ("headline").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 N > 1: launch with torch.distributed.run; every rank solves its own batch
@@ -471,6 +474,7 @@ def precision_c4(cm, torch, dev, stream, reps=2):
         st = cg.system_stats()
         out[name] = {"ms": round(ms, 2), "inner_iterations": int(st["iterations"].max()),
                      "replacements": int(st["outer"].max()), "status": int(st["status"].max()),
+                     "fp32_fallback": int(st["fallback"].max()),
                      "reported_error": float(st["error"].max()), "true_rel_residual": true_res()}
         del cg
     A64 = cm.SparseMatrix(pat, dtype=torch.float64).setData(pr.val.astype(np.float64))
@@ -560,6 +564,18 @@ def run_ours(args):
             "iterations_max": int(st64["iterations"].max()),
             "gbs_alg": round(plain_bytes(bt, st64["iterations"].astype(np.float64)) / (ms64 / 1e3) / 1e9, 1)}
 
+    # the same mixed solve on the sliced layout (CUMAT_CG_DIA=0, read when the
+    # solver is created): the number for patterns that are not stencils
+    os.environ["CUMAT_CG_DIA"] = "0"
+    cg_sl = cm.ConjugateGradient(A32).setTolerance(INNER_TOL)
+    del os.environ["CUMAT_CG_DIA"]
+    ms_sl = time_device(lambda: cg_sl.solve_refined(b64, outer=A32, outer_tol=OUTER_TOL, max_outer=MAX_OUTER, out=xp),
+                        max(1, args.steps // 2), 1, stream, world)
+    st_sl = cg_sl.system_stats()
+    sliced = {"value": round(N_SYS * world / (ms_sl / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms_sl, 3),
+              "converged": int((st_sl["status"] == 0).sum()), "max_error": float(st_sl["error"].max())}
+    del cg_sl
+
     # end to end through the public API with pinned host buffers
     hb = torch.from_numpy(bt.b.astype(np.float64)).pin_memory()
     hx = torch.empty(bt.n, dtype=torch.float64).pin_memory()
@@ -615,6 +631,7 @@ def run_ours(args):
             "clocks": clk_sum,
             "fp64_plain": fp64,
             "mixed_vs_fp64": round(value / fp64["value"], 3),
+            "mixed_sliced_layout": sliced,
             "solve_stats": {"inner_iterations_max": int(st["iterations"].max()),
                             "inner_iterations_mean": round(float(st["iterations"].mean()), 1),
                             "outer_steps_max": int(st["outer"].max()), "max_error": float(st["error"].max())},
@@ -622,6 +639,7 @@ def run_ours(args):
         }
         # short summary last, so that it survives in any tail of the line
         hl = {"mixed_vs_fp64": line["mixed_vs_fp64"], "fp64_solves_s": fp64["value"],
+              "mixed_sliced_solves_s": sliced["value"],
               "e2e_solves_s": line["e2e"]["value"], "l1_frac": line["roofline"]["frac"],
               "dram_frac": line["roofline"]["dram_frac"]}
         if "spmv_poisson1024" in extra:
@@ -759,6 +777,80 @@ def run_profile_small():
                       "fp64_converged": bool(np.all(cg64.system_stats()["status"] == 0))}))
 
 
+def run_profile_case(case: str):
+    """Small single-purpose workloads for one-kernel ncu captures (each well
+    above L2 in its streamed data, a few GB on the device at most):
+
+    grid3d      the 128^3 3D system (kappa = exp(N(0, 1)), seed 3) on the grid
+                path: plain FP64 Jacobi-CG and the mixed FP32 / FP64 solve,
+                each capped at 20 inner iterations (k_grid_*, k_gmix_*)
+    plain_dia   plain FP64 batched CG of the first 512 systems of the batch
+                to 1e-10 (k_plain_dia, three CTA tiers)
+    vectors     dot, squared norm, linear combination of 4 terms and the
+                sampled outer product on n = 64 Mi entries (k_dot, k_lincomb,
+                k_sddmm_csr on the 8192^2 Poisson pattern)
+    spmv_big    CSR and ELLPACK products on the 8192^2 Poisson matrix (3 each)
+    """
+    import torch
+
+    import cumat_b200 as cm
+    from cumat_b200 import problems as P
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    out = {"profile_case": case}
+    if case == "grid3d":
+        p3 = P.fv3d(128, 1.0, 3)
+        pat = cm.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+        A64 = cm.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
+        A32 = cm.SparseMatrix(pat, dtype=torch.float32).setData(p3.val)
+        b64 = torch.from_numpy(p3.b.astype(np.float64)).to(dev)
+        cg64 = cm.ConjugateGradient(A64).setTolerance(1e-10).setMaxIterations(20).set_path(2)
+        cg64.solve(b64)
+        cgm = cm.ConjugateGradient(A32).setTolerance(1e-4).setMaxIterations(20).set_path(2)
+        cgm.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=3)
+        out.update(rows=p3.n, nnz=p3.nnz)
+    elif case == "plain_dia":
+        bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED)
+        k = int(bt.row_off[512])
+        kz = int(bt.row_ptr[k])
+        p = cm.SparsityPattern.csr(k, k, bt.row_ptr[:k + 1], bt.col[:kz])
+        p.set_systems(bt.row_off[:513])
+        A64 = cm.SparseMatrix(p, dtype=torch.float64).setData(bt.val[:kz].astype(np.float64))
+        cg64 = cm.ConjugateGradient(A64).setTolerance(OUTER_TOL)
+        cg64.solve(torch.from_numpy(bt.b[:k].astype(np.float64)).to(dev))
+        st = cg64.system_stats()
+        out.update(systems=512, rows=k, nnz=kz, iterations_sum=int(st["iterations"].sum()),
+                   converged=bool(np.all(st["status"] == 0)))
+    elif case == "vectors":
+        n = 64 << 20
+        g = torch.Generator(device=dev).manual_seed(3)
+        x = torch.rand(n, device=dev, generator=g)
+        y = torch.rand(n, device=dev, generator=g)
+        cm.dot(x, y)
+        cm.squaredNorm(x)
+        vs = [torch.rand(n, device=dev, generator=g) for _ in range(4)]
+        cm.linear_combination([0.5, -1.0, 2.0, 0.25], vs)
+        pr = P.poisson2d(8192, 0)
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+        u = torch.rand(pr.n, device=dev, generator=g)
+        cm.sddmm(A, u, u)
+        out.update(n=n, sddmm_rows=pr.n, sddmm_nnz=pr.nnz)
+    elif case == "spmv_big":
+        pr = P.poisson2d(8192, 1)
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+        idx, ev = P.csr_to_ell(pr.n, pr.row_ptr, pr.col, pr.val)
+        E = cm.SparseMatrix(cm.SparsityPattern.ell(pr.n, pr.n, idx)).setData(ev)
+        x = torch.from_numpy(pr.b).to(dev)
+        for _ in range(3):
+            A * x
+            E * x
+        out.update(rows=pr.n, nnz=pr.nnz)
+    else:
+        raise SystemExit(f"unknown profile case {case}")
+    torch.cuda.synchronize()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -775,10 +867,14 @@ def main():
     ap.add_argument("--profile-small", action="store_true",
                     help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "
                          "mixed and FP64 solvers on the first 512 systems of the batch")
+    ap.add_argument("--profile-case", default=None,
+                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
-    if args.profile_small:
+    if args.profile_case:
+        run_profile_case(args.profile_case)
+    elif args.profile_small:
         run_profile_small()
     elif args.impl == "reference":
         run_reference(args)

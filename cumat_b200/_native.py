@@ -12,7 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libcumat_cg.so"
 
 # element types / formats / enums (include/cumat_cg.h)
 F32, F64, BF16 = 0, 1, 2
-CSR, ELLPACK = 0, 1
+CSR, ELLPACK, CSC, BSR = 0, 1, 2, 3
 PRECOND_IDENTITY, PRECOND_JACOBI = 0, 1
 ASSIGN, ADD, SUB = 0, 1, 2
 SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_ZERO_RHS, SOLVE_BREAKDOWN, SOLVE_NON_FINITE = 0, 1, 2, 3, 4
@@ -44,6 +44,8 @@ SIGNATURES = {
     "cmcg_memset_zero": (_i32, [_vp, _vp, _i64]),
     "cmcg_pattern_create_csr": (_i32, [_vp, _i32, _i32, _i64, _vp, _vp, _i32, C.POINTER(_vp)]),
     "cmcg_pattern_create_ell": (_i32, [_vp, _i32, _i32, _i32, _vp, _i32, C.POINTER(_vp)]),
+    "cmcg_pattern_create_csc": (_i32, [_vp, _i32, _i32, _i64, _vp, _vp, _i32, C.POINTER(_vp)]),
+    "cmcg_pattern_create_bsr": (_i32, [_vp, _i32, _i32, _i32, _i64, _vp, _vp, _i32, C.POINTER(_vp)]),
     "cmcg_pattern_set_systems": (_i32, [_vp, _i64, _vp]),
     "cmcg_pattern_info": (_i32, [_vp, _pi32, _pi32, _pi64, _pi32, _pi64, _pi32]),
     "cmcg_pattern_download": (_i32, [_vp, _vp, _vp]),
@@ -54,6 +56,9 @@ SIGNATURES = {
     "cmcg_matrix_info": (_i32, [_vp, _pi32, _pi32]),
     "cmcg_matrix_destroy": (_i32, [_vp]),
     "cmcg_spmv": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32]),
+    "cmcg_spmv_transposed": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32]),
+    "cmcg_matrix_to_dense": (_i32, [_vp, _vp, _i32]),
+    "cmcg_matrix_from_dense": (_i32, [_vp, _vp, _i32]),
     "cmcg_dot": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp, _i32, _vp]),
     "cmcg_squared_norm": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp]),
     "cmcg_dot_noalloc": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp, _i32, _vp]),
@@ -71,6 +76,7 @@ SIGNATURES = {
     "cmcg_cg_iterations": (_i32, [_vp, _pi64]),
     "cmcg_cg_error": (_i32, [_vp, _pf64]),
     "cmcg_cg_system_stats": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "cmcg_cg_fallbacks": (_i32, [_vp, _vp, _vp]),
     "cmcg_cg_solve_refined": (_i32, [_vp, _vp, _vp, _i32, _vp, _f64, _i32]),
     "cmcg_cg_adjoint": (_i32, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _f64, _i32]),
 }

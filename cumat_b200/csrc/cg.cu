@@ -857,40 +857,42 @@ __global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __r
 // ---------------------------------------------------------------------------
 
 // q[i] = sum_d v_d[i] p[i + off_d] for the rows [r0, r1) of one system (global
-// rows sr0 .. send - 1; v points at the system's first value), diagonals in
-// ascending offset order, the row's CSR order, with fused multiply-adds:
-// absent entries hold 0 and add 0 * p exactly, so the sum equals the sliced
-// layout's. p indices are clamped into the system, where a zero value meets
-// them. Thread t takes rows r0 + t + kTile u with U rows in flight. UNIT: the
-// middle diagonal is offset 0 with every value 1 and is not loaded.
+// rows sr0 .. send - 1, r0 - sr0 a multiple of 4; v points at the system's
+// first value), diagonals in ascending offset order, the row's CSR order, with
+// fused multiply-adds: absent entries hold 0 and add 0 * p exactly, so each
+// sum equals the sliced layout's. Thread t takes the four rows r0 + 4 t ..
+// r0 + 4 t + 3, then r0 + 4 (t + kTile) ..., the rows the sliced path gives
+// it, and emits them in the same order, so partial sums over the emitted
+// rows match too; the values of a diagonal for its four rows are one 16-byte
+// (8-byte for BF16) load. p indices are clamped into the system, where a zero
+// value (or, past the system's end, a row that is not emitted) meets them.
+// UNIT: the middle diagonal is offset 0 with every value 1 and is not loaded.
 // emit(global row, value).
 template <typename VT, typename MT, int ND, bool UNIT, typename F>
 __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int (&off)[ND], int sr0, int send, int r0,
                                              int r1, const VT* __restrict__ p, F&& emit) {
-    constexpr int U = sizeof(VT) == 8 ? 2 : 4;
-    for (int i0 = r0 + threadIdx.x; i0 < r1; i0 += U * kTile) {
-        VT acc[U];
+    for (int ib = r0 + 4 * threadIdx.x; ib < r1; ib += 4 * kTile) {
+        const int li = ib - sr0;
+        const MT* vr = v + (static_cast<int64_t>(li / kDiaBlockRows) * ND * kDiaBlockRows) + li % kDiaBlockRows;
+        VT acc[4] = {VT(0), VT(0), VT(0), VT(0)};
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int i = i0 + u * kTile;
-            acc[u] = VT(0);
-            if (i < r1) {
-                const int li = i - sr0;
-                const MT* vr = v + (static_cast<int64_t>(li / kDiaBlockRows) * ND * kDiaBlockRows) + li % kDiaBlockRows;
+        for (int d = 0; d < ND; ++d) {
+            if (UNIT && d == ND / 2) {
 #pragma unroll
-                for (int d = 0; d < ND; ++d) {
-                    if (UNIT && d == ND / 2) {
-                        acc[u] = fma(VT(1), p[i], acc[u]);
-                    } else {
-                        const int c = min(max(i + off[d], sr0), send - 1);
-                        acc[u] = fma(mval<VT>(__ldg(vr + d * kDiaBlockRows)), p[c], acc[u]);
-                    }
+                for (int q = 0; q < 4; ++q) acc[q] = fma(VT(1), p[min(ib + q, send - 1)], acc[q]);
+            } else {
+                Vals4<MT> w;
+                w.load(vr + d * kDiaBlockRows);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int c = min(max(ib + q + off[d], sr0), send - 1);
+                    acc[q] = fma(mval<VT>(w.v[q]), p[c], acc[q]);
                 }
             }
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (i0 + u * kTile < r1) emit(i0 + u * kTile, acc[u]);
+        for (int q = 0; q < 4; ++q)
+            if (ib + q < r1) emit(ib + q, acc[q]);
     }
 }
 
@@ -1233,6 +1235,9 @@ __global__ void __launch_bounds__(kTile) k_gmix_init(GMixArgs<MI, MO> m) {
             a.st.it[g.inst] = 0;
             a.st.outer[g.inst] = 0;
             a.st.flag[g.inst] = 0;
+            a.st.rep_it[g.inst] = 0;
+            a.st.cyc0[g.inst] = 0;
+            a.st.stall[g.inst] = 0;
             int32_t status = ST_RUNNING;
             if (bb == 0.0) status = CMCG_SOLVE_ZERO_RHS;
             else if (!finite_(bb) || !finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
@@ -1354,7 +1359,8 @@ __global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
                 a.st.status[g.inst] = CMCG_SOLVE_NON_FINITE;
                 atomicSub(a.active, 1);
             } else if (rzn < d2 * static_cast<float>(a.st.rmax[g.inst]) || rzn < static_cast<float>(a.st.goal[g.inst]) ||
-                       it >= sys_max_iter(a.max_iter, n)) {
+                       it >= sys_max_iter(a.max_iter, n) ||
+                       it - a.st.rep_it[g.inst] >= stall_len(a.st.outer[g.inst], a.st.cyc0[g.inst])) {
                 a.st.flag[g.inst] = 1;   // fold and replace in this iteration
             } else if (!(rzn > 0.0f)) {
                 a.st.status[g.inst] = CMCG_SOLVE_BREAKDOWN;
@@ -1423,6 +1429,11 @@ __global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
             const double thr = m.outer_tol * m.outer_tol * bb;
             const int32_t outer = a.st.outer[g.inst] + 1;
             a.st.outer[g.inst] = outer;
+            // progress guard: the true residual against the last replacement's
+            const int32_t stall = rr64 > kStallRatio * a.st.rr[g.inst] ? a.st.stall[g.inst] + 1 : 0;
+            a.st.stall[g.inst] = stall;
+            if (outer == 1) a.st.cyc0[g.inst] = a.st.it[g.inst];
+            a.st.rep_it[g.inst] = a.st.it[g.inst];
             a.st.rr[g.inst] = rr64;
             a.st.rmax[g.inst] = rzn;
             a.st.goal[g.inst] = static_cast<double>(static_cast<float>(thr / rr64) * rzn);
@@ -1432,7 +1443,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
             if (!finite_(rr64)) status = CMCG_SOLVE_NON_FINITE;
             else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
             else if (a.st.it[g.inst] >= sys_max_iter(a.max_iter, n) || outer >= m.max_updates) status = CMCG_SOLVE_MAX_ITER;
-            else if (!(rzn > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
+            else if (!(rzn > 0.0f) || stall >= kStallMax) status = CMCG_SOLVE_BREAKDOWN;
             if (status != ST_RUNNING) {
                 a.st.status[g.inst] = status;
                 atomicSub(a.active, 1);
@@ -1609,6 +1620,17 @@ struct cmcg_solver_s {
     // last solve
     int32_t last_inst = 0;
     bool last_refined = false;
+    // BF16 inner values: systems the BF16 solve left unconverged are solved
+    // again with FP32 values (CUMAT_CG_BF16_FALLBACK=0 disables); fb_* are the
+    // FP32 matrix (when the outer one is FP64) and solver used for that
+    bool bf16_fallback = true;
+    cmcg_matrix fb_mat = nullptr;
+    cmcg_solver fb = nullptr;
+    double* fb_x = nullptr;
+    size_t fb_x_bytes = 0;
+    int32_t* fb_list = nullptr;
+    size_t fb_list_bytes = 0;
+    std::vector<int32_t> fallback;   // per instance of the last refined solve: 1 = re-solved with FP32 values
 };
 
 namespace {
@@ -1753,7 +1775,7 @@ cmcg_status get_dinv(cmcg_solver s, int32_t vdt, const void** out) {
 }
 
 cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
-    const size_t per = 8 * sizeof(double) + 4 * sizeof(int32_t) + 2 * sizeof(unsigned);
+    const size_t per = 8 * sizeof(double) + 7 * sizeof(int32_t) + 2 * sizeof(unsigned);
     const size_t need = per * static_cast<size_t>(n_inst) + 256;
     if (s->st_inst >= n_inst && s->st_ws) return CMCG_OK;
     dev_free(s->st_ws);
@@ -1775,6 +1797,9 @@ cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
     s->st.it = reinterpret_cast<int32_t*>(b); b += 4 * n;
     s->st.status = reinterpret_cast<int32_t*>(b); b += 4 * n;
     s->st.outer = reinterpret_cast<int32_t*>(b); b += 4 * n;
+    s->st.rep_it = reinterpret_cast<int32_t*>(b); b += 4 * n;
+    s->st.cyc0 = reinterpret_cast<int32_t*>(b); b += 4 * n;
+    s->st.stall = reinterpret_cast<int32_t*>(b); b += 4 * n;
     s->st.tk1 = reinterpret_cast<unsigned*>(b); b += 4 * n;
     s->st.tk2 = reinterpret_cast<unsigned*>(b); b += 4 * n;
     CMCG_CUDA(cudaMemsetAsync(s->st_ws, 0, need, s->A->pat->ctx->stream));
@@ -2293,6 +2318,12 @@ cmcg_status run_coop(cmcg_solver s, SolveArgs<VT, MT>& a, VT* p_alt, bool* done)
     c.loop_cap = static_cast<int32_t>(std::min<int64_t>(cap + 2, INT32_MAX - 1));
     // counters: next, active, loops, -, grid barrier (count, generation)
     CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 8 * sizeof(int32_t), ctx->stream));
+    // every instance starts as running (-1), so that a launch that leaves
+    // early (a grid barrier whose wait ran out) is finalised as not converged
+    // instead of keeping a previous solve's status; its norms read as zero
+    CMCG_CUDA(cudaMemsetAsync(s->st.status, 0xFF, sizeof(int32_t) * static_cast<size_t>(n_inst), ctx->stream));
+    CMCG_CUDA(cudaMemsetAsync(s->st.rr, 0, sizeof(double) * static_cast<size_t>(n_inst), ctx->stream));
+    CMCG_CUDA(cudaMemsetAsync(s->st.bb, 0, sizeof(double) * static_cast<size_t>(n_inst), ctx->stream));
     // counters[4..7]: the grid barrier's two 64-bit words
     CMCG_TRY((coop_cg_launch<VT, MT, FMT>(c, s->counters + 4, ctx->d_err, n_inst, p_alt, s->coop_ctas, ctx->stream)));
     count_launch();
@@ -2777,6 +2808,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     if (const char* e = std::getenv("CUMAT_CG_DIA")) s->dia_kernels = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_SMALL")) s->mix_small = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::atoi(e) != 0;
+    if (const char* e = std::getenv("CUMAT_CG_BF16_FALLBACK")) s->bf16_fallback = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);
     if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);
     if (st == CMCG_OK && cudaMemsetAsync(s->counters, 0, 64, A->pat->ctx->stream) != cudaSuccess) st = fail(CMCG_ERR_CUDA, "memset");
@@ -2813,6 +2845,10 @@ cmcg_status cmcg_cg_destroy(cmcg_solver s) {
                     s->dia_vals, s->dia_plain})
         dev_free(p);
     if (s->host_io) cudaFreeHost(s->host_io);
+    dev_free(s->fb_x);
+    dev_free(s->fb_list);
+    if (s->fb) cmcg_cg_destroy(s->fb);
+    if (s->fb_mat) cmcg_matrix_destroy(s->fb_mat);
     cmcg_matrix A = s->A;
     delete s;
     matrix_release(A);
@@ -2947,8 +2983,122 @@ cmcg_status cmcg_cg_system_stats(cmcg_solver s, int32_t* iters, double* err, int
     return CMCG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+cmcg_status solve_refined_impl(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_batches, double* x,
+                               double outer_tol, int32_t max_outer);
+
+// Takes the FP32-value re-solve of the listed instances: their rows of x and
+// their statistics (one CTA per instance).
+__global__ void k_take_fallback(const int32_t* __restrict__ list, int32_t n_list, InstState dst, InstState src,
+                                const int32_t* __restrict__ row_off, int32_t n_sys, int32_t rows, double* __restrict__ x,
+                                const double* __restrict__ xf) {
+    for (int j = blockIdx.x; j < n_list; j += gridDim.x) {
+        const int inst = list[j];
+        const int b = inst / n_sys, sys = inst - b * n_sys;
+        const int64_t o = static_cast<int64_t>(b) * rows;
+        for (int i = row_off[sys] + threadIdx.x; i < row_off[sys + 1]; i += blockDim.x) x[o + i] = xf[o + i];
+        if (threadIdx.x == 0) {
+            dst.it[inst] = src.it[inst];
+            dst.status[inst] = src.status[inst];
+            dst.outer[inst] = src.outer[inst];
+            dst.err[inst] = src.err[inst];
+            dst.rr[inst] = src.rr[inst];
+            dst.bb[inst] = src.bb[inst];
+        }
+    }
+}
+
+// BF16 inner values round the Jacobi-scaled matrix by up to 2^-9 relative;
+// where that times the condition number approaches 1 the reliable updates
+// stop contracting and the system ends unconverged. Such systems are solved
+// again with the FP32 values of the outer matrix (converted once when the
+// outer matrix is FP64) and their results replace the BF16 ones; the
+// instances are reported by cmcg_cg_fallbacks.
+cmcg_status bf16_fallback(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_batches, double* x, double outer_tol,
+                          int32_t max_outer) {
+    cmcg_ctx ctx = s->A->pat->ctx;
+    const int32_t n = s->last_inst;
+    s->fallback.assign(n, 0);
+    std::vector<int32_t> st(n);
+    CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
+    CMCG_CUDA(cudaMemcpy(st.data(), s->st.status, 4 * static_cast<size_t>(n), cudaMemcpyDeviceToHost));
+    std::vector<int32_t> list;
+    for (int32_t i = 0; i < n; ++i)
+        if (st[i] != CMCG_SOLVE_CONVERGED && st[i] != CMCG_SOLVE_ZERO_RHS) list.push_back(i);
+    if (list.empty()) return CMCG_OK;
+    cmcg_matrix Af = Ao;
+    if (Ao->dtype != CMCG_F32) {
+        if (!s->fb_mat || s->fb_mat->version != Ao->version) {
+            if (!s->fb_mat) CMCG_TRY(cmcg_matrix_create(Ao->pat, CMCG_F32, Ao->batches, &s->fb_mat));
+            // FP64 values rounded to FP32 on the device (same layout and stride)
+            CMCG_TRY(convert(ctx, Ao->dtype, Ao->d_vals, CMCG_F32, s->fb_mat->d_vals, Ao->stride * Ao->batches));
+            s->fb_mat->version = Ao->version;   // tracks the source's values
+        }
+        Af = s->fb_mat;
+    }
+    if (!s->fb || s->fb->A != Af) {
+        if (s->fb) cmcg_cg_destroy(s->fb);
+        s->fb = nullptr;
+        CMCG_TRY(cmcg_cg_create(Af, s->precond, &s->fb));
+    }
+    cmcg_solver f = s->fb;
+    f->tol = s->tol;
+    f->max_iter = s->max_iter;
+    f->path = s->path;
+    f->refine_method = s->refine_method;
+    f->refine_delta = 0.0;   // the FP32 default
+    const size_t nv = static_cast<size_t>(s->A->pat->rows) * std::max(s->A->batches, b_batches);
+    CMCG_TRY(ensure_buffer(reinterpret_cast<void**>(&s->fb_x), &s->fb_x_bytes, nv * sizeof(double)));
+    CMCG_TRY(solve_refined_impl(f, Ao, b, b_batches, s->fb_x, outer_tol, max_outer));
+    CMCG_TRY(ensure_buffer(reinterpret_cast<void**>(&s->fb_list), &s->fb_list_bytes, list.size() * sizeof(int32_t)));
+    CMCG_CUDA(cudaMemcpyAsync(s->fb_list, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    const int grid = static_cast<int>(std::min<size_t>(list.size(), 65535));
+    k_take_fallback<<<grid, 256, 0, ctx->stream>>>(s->fb_list, static_cast<int32_t>(list.size()), s->st, f->st,
+                                                   s->A->pat->d_row_off, s->n_sys, s->A->pat->rows, x, s->fb_x);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    // the list upload must finish before the host vector goes away
+    CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int32_t i : list) s->fallback[i] = 1;
+    return CMCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_batches, double* x,
                                   double outer_tol, int32_t max_outer) {
+    CMCG_REQUIRE(s && b && x, "cmcg_cg_solve_refined: NULL argument");
+    if (!Ao) Ao = s->A;
+    s->fallback.clear();
+    CMCG_TRY(solve_refined_impl(s, Ao, b, b_batches, x, outer_tol, max_outer));
+    if (s->A->dtype == CMCG_BF16 && s->bf16_fallback) CMCG_TRY(bf16_fallback(s, Ao, b, b_batches, x, outer_tol, max_outer));
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_cg_fallbacks(cmcg_solver s, int32_t* flags, int64_t* count) {
+    CMCG_REQUIRE(s, "cmcg_cg_fallbacks: NULL solver");
+    CMCG_REQUIRE(s->last_inst > 0, "cmcg_cg_fallbacks: no solve has been run");
+    int64_t c = 0;
+    for (int32_t i = 0; i < s->last_inst; ++i) {
+        const int32_t v = (s->last_refined && i < static_cast<int32_t>(s->fallback.size())) ? s->fallback[i] : 0;
+        if (flags) flags[i] = v;
+        c += v;
+    }
+    if (count) *count = c;
+    return CMCG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+cmcg_status solve_refined_impl(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_batches, double* x,
+                               double outer_tol, int32_t max_outer) {
     CMCG_REQUIRE(s && b && x, "cmcg_cg_solve_refined: NULL argument");
     if (!Ao) Ao = s->A;
     CMCG_REQUIRE(Ao->pat == s->A->pat, "cmcg_cg_solve_refined: outer matrix must share the solver's pattern");
@@ -2988,6 +3138,10 @@ cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b
     return fmt == CMCG_CSR ? refined_mi<__nv_bfloat16, CMCG_CSR>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer)
                            : refined_mi<__nv_bfloat16, CMCG_ELLPACK>(s, Ao, b, b_batches, x, ob, outer_tol, max_outer);
 }
+
+}  // namespace
+
+extern "C" {
 
 cmcg_status cmcg_cg_adjoint(cmcg_solver s, cmcg_matrix Ao, const double* x, const double* gx, int32_t batches, double* gb,
                             double* gA, double outer_tol, int32_t max_outer) {

@@ -82,7 +82,27 @@ struct InstState {
     double* rmax;    // mixed solver: scaled |r|^2 at the last residual replacement
     double* goal;    //   scaled |r|^2 that would meet the FP64 target
     int32_t* flag;   //   1: replace the residual in this iteration
+    int32_t* rep_it; //   iteration of the last replacement
+    int32_t* cyc0;   //   length of the first replacement cycle
+    int32_t* stall;  //   consecutive replacements whose true residual did not drop
 };
+
+// Progress guard of the reliable updates. Inner values too coarse for the
+// system's conditioning (BF16 at a condition number of ~1e6) make the inner
+// recursion stagnate or diverge, and its residual may then never drop far
+// enough to trigger a replacement. A replacement is therefore also forced
+// after kStallFirst iterations in the first cycle, and after 4 times the
+// first cycle's length plus kStallPad (at least kStallFirst) later. A
+// replacement whose true residual norm fell by less than 10 % is a stall;
+// kStallMax stalls in a row stop the system with CMCG_SOLVE_BREAKDOWN.
+constexpr int kStallFirst = 4096;
+constexpr int kStallPad = 256;
+constexpr int kStallMax = 3;
+constexpr double kStallRatio = 0.81;   // |r|^2 ratio of a 10 % norm drop
+__host__ __device__ __forceinline__ int stall_len(int replacements, int cyc0) {
+    const int l = 4 * cyc0 + kStallPad;
+    return (replacements == 0 || l < kStallFirst) ? kStallFirst : l;
+}
 
 template <typename VT, typename MT>
 struct SolveArgs {

@@ -205,6 +205,8 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
         else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
         else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
         const int64_t maxit = sys_max_iter(a.max_inner, n);
+        // progress guard (stall_len): forced replacements, stalls in a row
+        int it_rep = 0, cyc0 = 0, stalls = 0;
         bool folded = true;
         // diagonal layout: alpha of the x increment not yet added to xh
         bool pend = false;
@@ -261,8 +263,9 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
             float rzn = s1[0];
             if (!finite_(rzn)) { status = CMCG_SOLVE_NON_FINITE; break; }
             // replace the residual when it dropped by delta, or when it suggests
-            // that the FP64 residual may have reached the target
-            if (rzn < d2 * rmax || rzn < goal) {
+            // that the FP64 residual may have reached the target, or when the
+            // cycle has run too long (progress guard)
+            if (rzn < d2 * rmax || rzn < goal || it - it_rep >= stall_len(updates, cyc0)) {
                 if (ND > 0 && pend) {
                     CMCG_DIA_SLOTS(nk, (dia_xinc<NK, T>(P, XH, tid, alpha_pend)))
                     pend = false;
@@ -293,12 +296,16 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
                 block_sum<double, 2>(t2, red64);
                 ++updates;
                 folded = true;
+                stalls = t2[0] > kStallRatio * rr64 ? stalls + 1 : 0;
+                if (updates == 1) cyc0 = it;
+                it_rep = it;
                 rr64 = t2[0];
                 rzn = static_cast<float>(t2[1]);
                 rmax = rzn;
                 goal = static_cast<float>(thr / rr64) * rmax;
                 if (!finite_(rr64)) { status = CMCG_SOLVE_NON_FINITE; break; }
                 if (rr64 < thr) { status = CMCG_SOLVE_CONVERGED; break; }
+                if (stalls >= kStallMax) { status = CMCG_SOLVE_BREAKDOWN; break; }
             }
             if (!(rzn > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
             const float beta = rzn / rz;

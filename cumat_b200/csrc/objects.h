@@ -107,6 +107,25 @@ struct cmcg_pattern_s {
     // [value dtype][vector dtype] (-1: not tuned yet)
     int8_t spmv_choice[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
     int64_t systems_version = 0;      // incremented by cmcg_pattern_set_systems
+    // The caller's storage when it is not CSR or ELLPACK: CMCG_CSC (the
+    // reference's SparsityPattern<CSC>: column pointers + row indices, values in
+    // column order) or CMCG_BSR (block CSR, block x block values per stored
+    // block, row-major). The kernels see the equivalent CSR pattern (format ==
+    // CMCG_CSR; a BSR block row expands to `block` scalar rows) and matrices
+    // keep their values in its order: CSR entry k is the caller's value
+    // d_val_perm[k] (null for plain CSR / ELLPACK).
+    int32_t declared = -1;            // CMCG_CSC, CMCG_BSR, or -1 (as format)
+    int32_t* d_val_perm = nullptr;
+    int32_t block = 1;                // BSR block size
+    int64_t decl_nnz = 0;             // the caller's stored entries (CSC) or blocks (BSR)
+    int32_t decl_rows = 0, decl_cols = 0;   // BSR: block rows / block columns
+    std::vector<int32_t> h_decl_ptr, h_decl_idx;   // the caller's index arrays (for download)
+    // transpose of the CSR pattern (built by the first transposed product):
+    // row r of A^T holds entries d_t_col[k] of A's column r, k in
+    // [d_t_row_ptr[r], d_t_row_ptr[r + 1]), whose values are A's entries d_t_perm[k]
+    int32_t* d_t_row_ptr = nullptr;
+    int32_t* d_t_col = nullptr;
+    int32_t* d_t_perm = nullptr;
     int refs = 1;
 };
 
@@ -145,4 +164,10 @@ void free_sell(SellPlan& s);
 // builds the pattern's diagonal plan (CSR; dia.ok tells whether it applies)
 cmcg_status ensure_dia(cmcg_pattern p);
 void free_dia(DiaPlan& d);
+// values between the caller's order and the internal CSR order of a pattern
+// with d_val_perm (sparse_ops.cu): to_internal gathers dst[b][k] =
+// src[b][perm[k]], otherwise dst[b][perm[k]] = src[b][k]; dtype of both
+cmcg_status permute_values(cmcg_pattern p, int32_t dtype, const void* src, int64_t src_stride, void* dst,
+                           int64_t dst_stride, int32_t batches, bool to_internal);
+void free_declared(cmcg_pattern p);
 }  // namespace cmcg

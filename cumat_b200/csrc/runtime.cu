@@ -85,6 +85,7 @@ void pattern_release(cmcg_pattern p) {
     dev_free(p->d_spmv_tiles);
     free_sell(p->sell);
     free_dia(p->dia);
+    free_declared(p);
     cmcg_ctx c = p->ctx;
     delete p;
     ctx_release(c);
@@ -439,9 +440,9 @@ cmcg_status cmcg_pattern_info(cmcg_pattern p, int32_t* rows, int32_t* cols, int6
     if (rows) *rows = p->rows;
     if (cols) *cols = p->cols;
     if (nnz) *nnz = p->nnz;
-    if (format) *format = p->format;
+    if (format) *format = p->declared >= 0 ? p->declared : p->format;
     if (n_sys) *n_sys = static_cast<int64_t>(p->row_off.size()) - 1;
-    if (width) *width = p->width;
+    if (width) *width = p->declared == CMCG_BSR ? p->block : p->width;
     return CMCG_OK;
 }
 
@@ -449,7 +450,11 @@ cmcg_status cmcg_pattern_download(cmcg_pattern p, int32_t* a, int32_t* b) {
     CMCG_REQUIRE(p && a, "cmcg_pattern_download: NULL argument");
     CMCG_CUDA(cudaSetDevice(p->ctx->device));
     CMCG_CUDA(cudaStreamSynchronize(p->ctx->stream));
-    if (p->format == CMCG_CSR) {
+    if (p->declared >= 0) {
+        // the caller's CSC / BSR arrays, as given
+        std::copy(p->h_decl_ptr.begin(), p->h_decl_ptr.end(), a);
+        if (b) std::copy(p->h_decl_idx.begin(), p->h_decl_idx.end(), b);
+    } else if (p->format == CMCG_CSR) {
         CMCG_CUDA(cudaMemcpy(a, p->d_row_ptr, (p->rows + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
         if (b && p->nnz) CMCG_CUDA(cudaMemcpy(b, p->d_col, p->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost));
     } else {
@@ -514,6 +519,18 @@ cmcg_status cmcg_matrix_set_values(cmcg_matrix m, int32_t src_dtype, const void*
     }
     cmcg_status st = CMCG_OK;
     const size_t ed = dtype_size(m->dtype);
+    if (p->d_val_perm) {
+        // CSC / BSR: convert in the caller's order, then gather into CSR order
+        void* conv = nullptr;
+        st = dev_alloc(&conv, std::max<size_t>(static_cast<size_t>(per_batch) * m->batches * ed, 16));
+        if (st == CMCG_OK) st = convert(ctx, src_dtype, src, m->dtype, conv, per_batch * m->batches);
+        if (st == CMCG_OK) st = permute_values(p, m->dtype, conv, per_batch, m->d_vals, m->stride, m->batches, true);
+        cudaStreamSynchronize(ctx->stream);
+        dev_free(conv);
+        if (stage) dev_free(stage);
+        m->version++;
+        return st;
+    }
     for (int32_t b = 0; b < m->batches && st == CMCG_OK; ++b) {
         const char* sb = static_cast<const char*>(src) + static_cast<size_t>(b) * per_batch * es;
         char* db = static_cast<char*>(m->d_vals) + static_cast<size_t>(b) * m->stride * ed;
@@ -539,6 +556,18 @@ cmcg_status cmcg_matrix_get_values(cmcg_matrix m, void* host_values) {
     CMCG_CUDA(cudaSetDevice(p->ctx->device));
     CMCG_CUDA(cudaStreamSynchronize(p->ctx->stream));
     const size_t ed = dtype_size(m->dtype);
+    if (p->d_val_perm) {
+        // CSC / BSR: scatter from CSR order into the caller's order
+        void* tmp = nullptr;
+        const size_t bytes = std::max<size_t>(static_cast<size_t>(p->nnz) * m->batches * ed, 16);
+        CMCG_TRY(dev_alloc(&tmp, bytes));
+        cmcg_status st = permute_values(p, m->dtype, m->d_vals, m->stride, tmp, p->nnz, m->batches, false);
+        if (st == CMCG_OK && cudaMemcpy(host_values, tmp, static_cast<size_t>(p->nnz) * m->batches * ed,
+                                        cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = fail(CMCG_ERR_CUDA, "cmcg_matrix_get_values: download failed");
+        dev_free(tmp);
+        return st;
+    }
     for (int32_t b = 0; b < m->batches; ++b) {
         char* hb = static_cast<char*>(host_values) + static_cast<size_t>(b) * p->nnz * ed;
         const char* db = static_cast<const char*>(m->d_vals) + static_cast<size_t>(b) * m->stride * ed;

@@ -713,25 +713,20 @@ cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub,
 
 }  // namespace
 
-// Row-length rule of the CSR product (deterministic, from the pattern): a
-// longest row of at least 256 entries and 32 times the mean takes a warp per
-// row (V = 32); a mean row length of at least 12 takes V lanes per row with V
-// about the row's number of 4-entry chunks (4 .. 32); shorter rows stay
-// thread per row. Returns the variant (3 + log2(V / 4)) or -1.
+// Row-length rule of the CSR product (deterministic, from the pattern): when
+// the longest row has at least 256 entries and 32 times the mean, thread per
+// row would leave a few threads summing long rows alone, and a warp per row
+// (V = 32) takes over. Otherwise the product stays thread per row, which adds
+// every row in entry order exactly as the solvers' products do (so that, for
+// instance, b = A x0 followed by a solve from x0 finds a zero residual). The
+// V = 4 .. 16 kernels are there for callers that force them. Returns the
+// variant (3 + log2(V / 4)) or -1.
 int csr_vec_variant(cmcg_pattern p) {
     const auto& rp = p->h_row_ptr;
     int64_t mx = 0;
     for (int32_t r = 0; r < p->rows; ++r) mx = std::max<int64_t>(mx, rp[r + 1] - rp[r]);
     const double mean = static_cast<double>(p->nnz) / std::max(1, p->rows);
-    if (mx >= 256 && static_cast<double>(mx) >= 32.0 * mean) return 6;
-    if (mean < 12.0) return -1;
-    const int chunks = static_cast<int>(mean / 4.0) + 2;
-    int v = 4, variant = 3;
-    while (v < chunks && v < 32) {
-        v *= 2;
-        ++variant;
-    }
-    return variant;
+    return (mx >= 256 && static_cast<double>(mx) >= 32.0 * mean) ? 6 : -1;
 }
 
 // Persistent cache of the timed choices: one line "key variant" per tuned
@@ -882,9 +877,24 @@ cmcg_status dot_dispatch(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, 
 
 cmcg_status sddmm_dispatch(cmcg_matrix M, int32_t dt, double alpha, const void* u, int32_t ub, const void* v,
                            int32_t vb, void* out, int32_t ob) {
-    if (dt == CMCG_F32) return launch_sddmm<float>(M, alpha, u, ub, v, vb, out, ob);
-    if (dt == CMCG_F64) return launch_sddmm<double>(M, alpha, u, ub, v, vb, out, ob);
-    return fail(CMCG_ERR_INVALID_ARGUMENT, "sddmm: dtype must be F32 or F64");
+    if (dt != CMCG_F32 && dt != CMCG_F64) return fail(CMCG_ERR_INVALID_ARGUMENT, "sddmm: dtype must be F32 or F64");
+    cmcg_pattern p = M->pat;
+    // CSC / BSR patterns: the product in CSR order, then scattered into the
+    // caller's value order
+    void* tmp = nullptr;
+    void* dst = out;
+    if (p->d_val_perm) {
+        CMCG_TRY(dev_alloc(&tmp, std::max<size_t>(static_cast<size_t>(p->nnz) * ob * dtype_size(dt), 16)));
+        dst = tmp;
+    }
+    cmcg_status st = dt == CMCG_F32 ? launch_sddmm<float>(M, alpha, u, ub, v, vb, dst, ob)
+                                    : launch_sddmm<double>(M, alpha, u, ub, v, vb, dst, ob);
+    if (tmp) {
+        if (st == CMCG_OK) st = permute_values(p, dt, tmp, p->nnz, out, p->nnz, ob, false);
+        cudaStreamSynchronize(p->ctx->stream);
+        dev_free(tmp);
+    }
+    return st;
 }
 
 }  // namespace cmcg

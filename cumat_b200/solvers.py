@@ -141,7 +141,9 @@ class ConjugateGradient:
         return v.value
 
     def system_stats(self, n_inst: Optional[int] = None):
-        """Per (batch, system) arrays: iterations, error, status, refinement steps."""
+        """Per (batch, system) arrays: iterations, error, status, refinement steps,
+        and (refined solves with BF16 values) whether the system was solved again
+        with FP32 values."""
         if n_inst is None:
             ns = 1 if self.A.pattern.row_off is None else self.A.pattern.row_off.size - 1
             n_inst = self._last_batches * ns
@@ -151,7 +153,9 @@ class ConjugateGradient:
         ou = np.empty(n_inst, np.int32)
         N.call("cmcg_cg_system_stats", self.handle, it.ctypes.data_as(C.c_void_p), err.ctypes.data_as(C.c_void_p),
                st.ctypes.data_as(C.c_void_p), ou.ctypes.data_as(C.c_void_p))
-        return {"iterations": it, "error": err, "status": st, "outer": ou}
+        fb = np.zeros(n_inst, np.int32)
+        N.call("cmcg_cg_fallbacks", self.handle, fb.ctypes.data_as(C.c_void_p), None)
+        return {"iterations": it, "error": err, "status": st, "outer": ou, "fallback": fb}
 
     def __del__(self):
         try:

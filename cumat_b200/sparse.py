@@ -29,6 +29,8 @@ from . import _native as N
 
 CSR = N.CSR
 ELLPACK = N.ELLPACK
+CSC = N.CSC
+BSR = N.BSR
 
 _TORCH_DT = {torch.float32: N.F32, torch.float64: N.F64, torch.bfloat16: N.BF16}
 _NP_DT = {np.dtype(np.float32): N.F32, np.dtype(np.float64): N.F64}
@@ -87,19 +89,21 @@ class Context:
 
 
 class SparsityPattern:
-    """Mirror of ``cuMat::SparsityPattern<CSR|ELLPACK>``; fill the fields, then
-    ``assertValid()`` validates and uploads (the reference's assertValid only
-    checks sizes; here malformed patterns raise ``CuMatError``)."""
+    """Mirror of ``cuMat::SparsityPattern<CSR|CSC|ELLPACK>``; fill the fields,
+    then ``assertValid()`` validates and uploads (the reference's assertValid
+    only checks sizes; here malformed patterns raise ``CuMatError``). BSR
+    (block CSR) stands for the reference's CSR pattern of block scalars."""
 
     def __init__(self, fmt: int = CSR):
         self.format = fmt
         self.rows = 0
         self.cols = 0
-        self.nnz = 0            # CSR
-        self.IA = None          # CSR column indices (nnz)
-        self.JA = None          # CSR row pointers (rows + 1)
+        self.nnz = 0            # CSR / CSC: stored entries; BSR: stored blocks
+        self.IA = None          # CSR column indices / CSC row indices (nnz)
+        self.JA = None          # CSR row pointers (rows + 1) / CSC column pointers (cols + 1)
         self.nnzPerRow = 0      # ELLPACK
         self.indices = None     # ELLPACK (rows, nnzPerRow), -1 = padding
+        self.block = 1          # BSR block size; rows / cols count blocks
         self.handle = None
         self._ctx = None
         self.row_off = None
@@ -109,6 +113,27 @@ class SparsityPattern:
     def csr(cls, rows, cols, row_ptr, col_idx, ctx: Optional[Context] = None) -> "SparsityPattern":
         p = cls(CSR)
         p.rows, p.cols = int(rows), int(cols)
+        p.JA = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        p.IA = np.ascontiguousarray(col_idx, dtype=np.int32)
+        p.nnz = int(p.IA.size)
+        p.assertValid(ctx)
+        return p
+
+    @classmethod
+    def csc(cls, rows, cols, col_ptr, row_idx, ctx: Optional[Context] = None) -> "SparsityPattern":
+        p = cls(CSC)
+        p.rows, p.cols = int(rows), int(cols)
+        p.JA = np.ascontiguousarray(col_ptr, dtype=np.int32)
+        p.IA = np.ascontiguousarray(row_idx, dtype=np.int32)
+        p.nnz = int(p.IA.size)
+        p.assertValid(ctx)
+        return p
+
+    @classmethod
+    def bsr(cls, block_rows, block_cols, block, row_ptr, col_idx, ctx: Optional[Context] = None) -> "SparsityPattern":
+        """Block CSR: row_ptr / col_idx over blocks of block x block entries."""
+        p = cls(BSR)
+        p.rows, p.cols, p.block = int(block_rows), int(block_cols), int(block)
         p.JA = np.ascontiguousarray(row_ptr, dtype=np.int32)
         p.IA = np.ascontiguousarray(col_idx, dtype=np.int32)
         p.nnz = int(p.IA.size)
@@ -130,13 +155,22 @@ class SparsityPattern:
         ctx = ctx or Context.current()
         self._ctx = ctx
         h = C.c_void_p()
-        if self.format == CSR:
+        if self.format in (CSR, CSC, BSR):
             ja = np.ascontiguousarray(self.JA, dtype=np.int32)
             ia = np.ascontiguousarray(self.IA, dtype=np.int32)
-            if ja.size != self.rows + 1 or ia.size != self.nnz:
-                raise ValueError("SparsityPattern<CSR>: JA must have rows+1 and IA nnz entries")
-            N.call("cmcg_pattern_create_csr", ctx.handle, self.rows, self.cols, self.nnz,
-                   ja.ctypes.data_as(C.c_void_p), ia.ctypes.data_as(C.c_void_p) if ia.size else None, 0, C.byref(h))
+            outer = self.cols if self.format == CSC else self.rows
+            if ja.size != outer + 1 or ia.size != self.nnz:
+                raise ValueError("SparsityPattern: JA must have outer size + 1 and IA nnz entries")
+            iap = ia.ctypes.data_as(C.c_void_p) if ia.size else None
+            if self.format == CSR:
+                N.call("cmcg_pattern_create_csr", ctx.handle, self.rows, self.cols, self.nnz,
+                       ja.ctypes.data_as(C.c_void_p), iap, 0, C.byref(h))
+            elif self.format == CSC:
+                N.call("cmcg_pattern_create_csc", ctx.handle, self.rows, self.cols, self.nnz,
+                       ja.ctypes.data_as(C.c_void_p), iap, 0, C.byref(h))
+            else:
+                N.call("cmcg_pattern_create_bsr", ctx.handle, self.rows, self.cols, self.block, self.nnz,
+                       ja.ctypes.data_as(C.c_void_p), iap, 0, C.byref(h))
         else:
             ind = np.asarray(self.indices, dtype=np.int32)
             if ind.shape != (self.rows, self.nnzPerRow):
@@ -154,12 +188,26 @@ class SparsityPattern:
         self.row_off = ro
 
     def getNNZ(self) -> int:
-        return self.nnz if self.format == CSR else self.rows * self.nnzPerRow
+        """Stored values per batch (BSR: block^2 per block)."""
+        if self.format in (CSR, CSC):
+            return self.nnz
+        if self.format == BSR:
+            return self.nnz * self.block * self.block
+        return self.rows * self.nnzPerRow
+
+    @property
+    def scalar_rows(self) -> int:
+        return self.rows * self.block if self.format == BSR else self.rows
+
+    @property
+    def scalar_cols(self) -> int:
+        return self.cols * self.block if self.format == BSR else self.cols
 
     def download(self):
-        """Device copy of the index arrays: (JA, IA) for CSR, (rows, width) indices for ELLPACK."""
-        if self.format == CSR:
-            ja = np.empty(self.rows + 1, np.int32)
+        """Device copy of the index arrays as given: (JA, IA) for CSR / CSC / BSR,
+        (rows, width) indices for ELLPACK."""
+        if self.format in (CSR, CSC, BSR):
+            ja = np.empty((self.cols if self.format == CSC else self.rows) + 1, np.int32)
             ia = np.empty(max(self.nnz, 1), np.int32)
             N.call("cmcg_pattern_download", self.handle, ja.ctypes.data_as(C.c_void_p), ia.ctypes.data_as(C.c_void_p))
             return ja, ia[: self.nnz]
@@ -195,11 +243,12 @@ class SparseMatrix:
 
     @property
     def rows(self) -> int:
-        return self.pattern.rows
+        """Scalar rows (a BSR pattern's block rows times its block size)."""
+        return self.pattern.scalar_rows
 
     @property
     def cols(self) -> int:
-        return self.pattern.cols
+        return self.pattern.scalar_cols
 
     def getSparsityPattern(self) -> SparsityPattern:
         return self.pattern
@@ -244,7 +293,40 @@ class SparseMatrix:
             N.call("cmcg_matrix_get_values", self.handle, out.ctypes.data_as(C.c_void_p))
         if self.pattern.format == ELLPACK:
             return out.reshape(self.batches, self.pattern.nnzPerRow, self.rows).transpose(0, 2, 1)
+        if self.pattern.format == BSR:
+            b = self.pattern.block
+            return out.reshape(self.batches, self.pattern.nnz, b, b)
         return out.reshape(self.batches, self.pattern.nnz)
+
+    def transposed_product(self, x: torch.Tensor, out: Optional[torch.Tensor] = None,
+                           mode: int = N.ASSIGN) -> torch.Tensor:
+        """out (mode)= A^T * x; x is (rows,) or (xb, rows)."""
+        xb = 1 if x.dim() == 1 else x.shape[0]
+        ob = max(self.batches, xb)
+        if out is None:
+            shape = (self.cols,) if (x.dim() == 1 and self.batches == 1) else (ob, self.cols)
+            out = torch.empty(shape, dtype=x.dtype, device=x.device)
+        x = x.contiguous()
+        N.call("cmcg_spmv_transposed", self.handle, _TORCH_DT[x.dtype], _vp(x), xb, _vp(out), mode)
+        return out
+
+    def toDense(self, row_major: bool = True) -> torch.Tensor:
+        """Dense copy (zeros off the pattern): (batches, rows, cols), on the device."""
+        shape = (self.batches, self.rows, self.cols) if row_major else (self.batches, self.cols, self.rows)
+        out = torch.empty(shape, dtype=self.dtype, device=self.pattern._ctx.torch_device)
+        N.call("cmcg_matrix_to_dense", self.handle, _vp(out), 1 if row_major else 0)
+        return out if row_major else out.transpose(1, 2)
+
+    def setFromDense(self, dense: torch.Tensor) -> "SparseMatrix":
+        """Takes the dense matrix's values at the pattern's entries (a sparse
+        view of the dense matrix): dense (batches, rows, cols) or (rows, cols)."""
+        d = dense.to(self.dtype)
+        if d.dim() == 2:
+            d = d.unsqueeze(0).expand(self.batches, -1, -1)
+        d = d.contiguous()
+        N.call("cmcg_matrix_from_dense", self.handle, _vp(d), 1)
+        self.pattern._ctx.synchronize()
+        return self
 
     def product(self, x: torch.Tensor, out: Optional[torch.Tensor] = None, mode: int = N.ASSIGN) -> torch.Tensor:
         """out (mode)= A * x; x is (cols,) or (xb, cols) float32/float64 on the device."""

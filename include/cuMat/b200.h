@@ -356,6 +356,32 @@ struct SparsityPattern<CSR> {
     }
 };
 
+// reference SparsityPattern<CSC> (SparseMatrixBase.h:29-87): JA = column
+// pointers (cols + 1), IA = row index of every entry; values in column order
+template <>
+struct SparsityPattern<CSC> {
+    typedef int StorageIndex;
+    typedef Matrix<StorageIndex, Dynamic, 1, 1, ColumnMajor> IndexVector;
+    template <typename S, int B>
+    using DataMatrix = Matrix<S, Dynamic, 1, B, ColumnMajor>;
+
+    Index nnz = 0;
+    Index rows = 0;
+    Index cols = 0;
+    IndexVector IA;   // row index of every entry, size nnz
+    IndexVector JA;   // column pointers, size cols + 1
+
+    void assertValid() const {
+        if (!(JA.size() == cols + 1 && rows > 0 && cols > 0 && IA.size() == nnz))
+            throw std::invalid_argument("SparsityPattern<CSC>: inconsistent sizes");
+    }
+    Index getNNZ() const { return nnz; }
+    template <typename S, int B>
+    DataMatrix<S, B> allocateDataMatrix(Index batches) const {
+        return DataMatrix<S, B>(nnz, 1, batches);
+    }
+};
+
 template <>
 struct SparsityPattern<ELLPACK> {
     typedef int StorageIndex;
@@ -405,6 +431,14 @@ inline std::shared_ptr<PatternHandle> make_pattern(const SparsityPattern<CSR>& s
                                   sp.JA.data(), sp.IA.data(), 1, &h->p));
     return h;
 }
+inline std::shared_ptr<PatternHandle> make_pattern(const SparsityPattern<CSC>& sp) {
+    sp.assertValid();
+    auto h = std::make_shared<PatternHandle>();
+    h->ctx = Context::current().holder();
+    check(cmcg_pattern_create_csc(h->ctx->ctx, static_cast<int32_t>(sp.rows), static_cast<int32_t>(sp.cols), sp.nnz,
+                                  sp.JA.data(), sp.IA.data(), 1, &h->p));
+    return h;
+}
 inline std::shared_ptr<PatternHandle> make_pattern(const SparsityPattern<ELLPACK>& sp) {
     sp.assertValid();
     auto h = std::make_shared<PatternHandle>();
@@ -429,7 +463,8 @@ public:
     enum { Batches = _Batches, SFlags = _SparseFlags };
     typedef SparsityPattern<_SparseFlags> SparsityPatternType;
     typedef typename SparsityPatternType::template DataMatrix<_Scalar, _Batches> DataMatrix;
-    static_assert(_SparseFlags == CSR || _SparseFlags == ELLPACK, "SparseMatrix: CSR or ELLPACK storage");
+    static_assert(_SparseFlags == CSR || _SparseFlags == CSC || _SparseFlags == ELLPACK,
+                  "SparseMatrix: CSR, CSC or ELLPACK storage");
     static_assert(b200::DType<_Scalar>::id >= 0, "SparseMatrix: float or double values");
 
 private:
@@ -494,6 +529,88 @@ public:
         const Index ob = batches() > x.batches() ? batches() : x.batches();
         Matrix<S, Dynamic, 1, Dynamic, ColumnMajor> y(rows(), 1, ob);
         product(x, y);
+        return y;
+    }
+    // y = A^T * x, evaluated immediately (CSR / CSC storage)
+    template <typename S, int R, int C, int B, int F>
+    Matrix<S, Dynamic, 1, Dynamic, ColumnMajor> transposedProduct(const Matrix<S, R, C, B, F>& x) const {
+        if (x.rows() * x.cols() != rows()) throw std::invalid_argument("SparseMatrix^T * x: size mismatch");
+        const Index ob = batches() > x.batches() ? batches() : x.batches();
+        Matrix<S, Dynamic, 1, Dynamic, ColumnMajor> y(cols(), 1, ob);
+        b200::check(cmcg_spmv_transposed(handle(), b200::DType<S>::id, x.data(), static_cast<int32_t>(x.batches()),
+                                         y.data(), CMCG_ASSIGN));
+        return y;
+    }
+    // dense copy [batch][rows][cols] (row-major), zeros off the pattern: the
+    // reference's assignment of a sparse matrix to a dense one
+    Matrix<_Scalar, Dynamic, Dynamic, Dynamic, RowMajor> toDense() const {
+        Matrix<_Scalar, Dynamic, Dynamic, Dynamic, RowMajor> d(rows(), cols(), batches());
+        b200::check(cmcg_matrix_to_dense(handle(), d.data(), 1));
+        return d;
+    }
+};
+
+// Block CSR matrix of BlockSize x BlockSize blocks of Scalar (no reference
+// class: the reference puts a user-defined block scalar type, e.g. a
+// row-major float3x3 with float3 vectors, into SparseMatrix<Block, 1, CSR>,
+// tests/TestBlockedConjugateGradient.cu:10-237). The pattern's JA / IA index
+// blocks; values are BlockSize^2 per block, row-major, block after block;
+// vectors hold BlockSize entries per block row, so rows() counts scalars.
+// Works with ConjugateGradient like any SparseMatrix.
+template <typename _Scalar, int BlockSize, int _Batches = 1>
+class BlockSparseMatrix {
+public:
+    typedef _Scalar Scalar;
+    enum { Batches = _Batches, Block = BlockSize };
+    typedef Matrix<_Scalar, Dynamic, 1, _Batches, ColumnMajor> DataMatrix;
+
+private:
+    struct State {
+        SparsityPattern<CSR> blocks;
+        DataMatrix data;
+        std::shared_ptr<b200::MatrixHandle> handle;
+        bool dirty = true;
+    };
+    std::shared_ptr<State> s_;
+
+public:
+    BlockSparseMatrix() = default;
+    explicit BlockSparseMatrix(const SparsityPattern<CSR>& blocks, Index batches = (_Batches > 0 ? _Batches : 1))
+        : s_(std::make_shared<State>()) {
+        blocks.assertValid();
+        s_->blocks = blocks;
+        s_->data = DataMatrix(blocks.nnz * BlockSize * BlockSize, 1, batches);
+        s_->data.setZero();
+        auto h = std::make_shared<b200::MatrixHandle>();
+        h->pat = std::make_shared<b200::PatternHandle>();
+        h->pat->ctx = Context::current().holder();
+        b200::check(cmcg_pattern_create_bsr(h->pat->ctx->ctx, static_cast<int32_t>(blocks.rows),
+                                            static_cast<int32_t>(blocks.cols), BlockSize, blocks.nnz, blocks.JA.data(),
+                                            blocks.IA.data(), 1, &h->pat->p));
+        b200::check(cmcg_matrix_create(h->pat->p, b200::DType<_Scalar>::id, static_cast<int32_t>(batches), &h->m));
+        s_->handle = h;
+    }
+    DataMatrix& getData() {
+        s_->dirty = true;
+        return s_->data;
+    }
+    Index rows() const { return s_->blocks.rows * BlockSize; }
+    Index cols() const { return s_->blocks.cols * BlockSize; }
+    Index batches() const { return s_->data.batches(); }
+    cmcg_matrix handle() const {
+        if (s_->dirty) {
+            b200::check(cmcg_matrix_set_values(s_->handle->m, b200::DType<_Scalar>::id, s_->data.data(), 1));
+            s_->dirty = false;
+        }
+        return s_->handle->m;
+    }
+    template <typename S, int R, int C, int B, int F>
+    Matrix<S, Dynamic, 1, Dynamic, ColumnMajor> operator*(const Matrix<S, R, C, B, F>& x) const {
+        if (x.rows() * x.cols() != cols()) throw std::invalid_argument("BlockSparseMatrix * x: size mismatch");
+        const Index ob = batches() > x.batches() ? batches() : x.batches();
+        Matrix<S, Dynamic, 1, Dynamic, ColumnMajor> y(rows(), 1, ob);
+        b200::check(cmcg_spmv(handle(), b200::DType<S>::id, x.data(), static_cast<int32_t>(x.batches()), y.data(),
+                              CMCG_ASSIGN));
         return y;
     }
 };

@@ -49,8 +49,10 @@ enum {
 
 /* element types */
 enum { CMCG_F32 = 0, CMCG_F64 = 1, CMCG_BF16 = 2 };
-/* storage formats (reference SparseFlags, cuMat/src/Constants.h) */
-enum { CMCG_CSR = 0, CMCG_ELLPACK = 1 };
+/* storage formats (reference SparseFlags, cuMat/src/Constants.h; BSR, block
+ * CSR, has no reference SparseFlags value: the reference stores blocks as a
+ * block scalar type in a CSR pattern) */
+enum { CMCG_CSR = 0, CMCG_ELLPACK = 1, CMCG_CSC = 2, CMCG_BSR = 3 };
 /* preconditioners (reference ConjugateGradient.h:218-265) */
 enum { CMCG_PRECOND_IDENTITY = 0, CMCG_PRECOND_JACOBI = 1 };
 /* assignment modes of a product (reference AssignmentMode ASSIGN / ADD / SUB) */
@@ -131,15 +133,38 @@ cmcg_status cmcg_pattern_create_csr(cmcg_ctx ctx, int32_t rows, int32_t cols, in
  * 0 < nnz_per_row <= cols, every index in [-1, cols). */
 cmcg_status cmcg_pattern_create_ell(cmcg_ctx ctx, int32_t rows, int32_t cols, int32_t nnz_per_row,
                                     const int32_t* indices, int32_t is_device, cmcg_pattern* out);
+/* CSC pattern (reference SparsityPattern<CSC>, SparseMatrixBase.h:29-87:
+ * JA = col_ptr (cols+1), IA = row_idx (nnz)). Validated like CSR with rows and
+ * columns exchanged. Values of matrices on it are given and returned in CSC
+ * (column) order; products, solves and reductions run on the equivalent CSR
+ * pattern, whose value order is a permutation of the caller's. */
+cmcg_status cmcg_pattern_create_csc(cmcg_ctx ctx, int32_t rows, int32_t cols, int64_t nnz, const int32_t* col_ptr,
+                                    const int32_t* row_idx, int32_t is_device, cmcg_pattern* out);
+/* Block CSR pattern of block_rows x block_cols blocks of block_size x
+ * block_size (2 .. 8) entries: row_ptr (block_rows+1) and col_idx (nnz_blocks)
+ * index blocks. The reference's blocked solver (a block scalar type such as a
+ * row-major float3x3 in a CSR pattern with float3 vectors,
+ * tests/TestBlockedConjugateGradient.cu:10-237, ConjugateGradient.h:47-61).
+ * Values are block_size^2 per block, row-major, in block order; vectors hold
+ * block_size entries per block row. The pattern is block_rows * block_size
+ * square rows for every other call; each block row expands to block_size
+ * scalar rows, so products, CG (Jacobi = inverse of the scalar diagonal, the
+ * reference's ExtractDiagonalFunctor + cwiseInverseCheck) and the
+ * mixed-precision solves apply unchanged. */
+cmcg_status cmcg_pattern_create_bsr(cmcg_ctx ctx, int32_t block_rows, int32_t block_cols, int32_t block_size,
+                                    int64_t nnz_blocks, const int32_t* row_ptr, const int32_t* col_idx,
+                                    int32_t is_device, cmcg_pattern* out);
 /* Partitions a square pattern into n_sys independent diagonal blocks
  * (system i owns rows and columns [row_off[i], row_off[i+1])). Fails if an
  * entry couples two systems. No reference counterpart (the reference needs one
  * shared pattern per batch, cuMat/src/SparseProductEvaluation.h:113-114). */
 cmcg_status cmcg_pattern_set_systems(cmcg_pattern p, int64_t n_sys, const int64_t* row_off);
-/* rows, cols, nnz (stored entries incl. ELL padding), format, n_sys, width (ELL). */
+/* rows, cols, nnz (stored scalar entries incl. ELL padding), format (as
+ * created: CSR, ELLPACK, CSC or BSR), n_sys, width (ELL; BSR: block size). */
 cmcg_status cmcg_pattern_info(cmcg_pattern p, int32_t* rows, int32_t* cols, int64_t* nnz, int32_t* format,
                               int64_t* n_sys, int32_t* width);
-/* Copies the pattern's index arrays to host memory (row_ptr/col_idx, or the
+/* Copies the pattern's index arrays, as given at creation, to host memory
+ * (row_ptr/col_idx; CSC col_ptr/row_idx; BSR block row_ptr/col_idx; or the
  * column-major ELL indices in row_ptr_or_idx, col_idx unused). */
 cmcg_status cmcg_pattern_download(cmcg_pattern p, int32_t* row_ptr_or_idx, int32_t* col_idx);
 cmcg_status cmcg_pattern_destroy(cmcg_pattern p);
@@ -171,6 +196,25 @@ cmcg_status cmcg_matrix_destroy(cmcg_matrix m);
  * Rows without entries give 0. Device pointers. */
 cmcg_status cmcg_spmv(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t x_batches, void* y,
                       int32_t mode);
+
+/* y (mode)= A^T * x for every batch (no reference product: the reference's
+ * product kernels leave transposed operands as a TODO,
+ * SparseProductEvaluation.h:94). x: [x_batches][rows], y: [out_batches][cols].
+ * CSR-equivalent patterns (CSR, CSC, BSR) only: thread per column of A over
+ * the pattern's transpose (built once per pattern), values read through the
+ * transpose's entry map; no atomics, deterministic. */
+cmcg_status cmcg_spmv_transposed(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t x_batches, void* y,
+                                 int32_t mode);
+
+/* Dense <-> sparse on the pattern (reference: assignment of a sparse matrix
+ * to a dense one and of a dense expression to a sparse matrix, evaluated
+ * coefficient-wise on the pattern: SparseEvaluation.h:15-34, tests
+ * TestSparseMatrix.cu:10-384). dense: device, [batches][rows][cols] when
+ * row_major, else [batches][cols][rows], of the matrix dtype. to_dense writes
+ * zeros off the pattern; from_dense takes the dense values at the pattern's
+ * entries (a sparse view of the dense matrix). */
+cmcg_status cmcg_matrix_to_dense(cmcg_matrix A, void* dense, int32_t row_major);
+cmcg_status cmcg_matrix_from_dense(cmcg_matrix A, const void* dense, int32_t row_major);
 
 /* out[b] = sum_i x[b][i] * y[b][i] for b < out_batches (reference
  * MatrixBase::dot, cuMat/src/ReductionOpsPlugin.inl:279-298); a one-batch
@@ -269,6 +313,18 @@ cmcg_status cmcg_cg_system_stats(cmcg_solver s, int32_t* iters, double* err, int
  * (use the solver's matrix; it must then be F32 or F64). */
 cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix A_outer, const double* b, int32_t b_batches,
                                   double* x, double outer_tol, int32_t max_outer);
+
+/* BF16 inner values (no reference counterpart): rounding the Jacobi-scaled
+ * values to BF16 perturbs them by up to 2^-9 relative, which stops the
+ * refinement from contracting once that times the condition number nears 1.
+ * cmcg_cg_solve_refined therefore checks every system after a BF16 solve and
+ * solves the ones that did not converge again with FP32 values (those of
+ * A_outer, rounded to FP32 when it is FP64), keeping their results; this
+ * synchronises the context stream once per BF16 solve. Set
+ * CUMAT_CG_BF16_FALLBACK=0 before creating the solver to keep the BF16
+ * statuses. flags (may be NULL): per instance of the last solve, 1 where it
+ * was re-solved with FP32 values; count: how many. */
+cmcg_status cmcg_cg_fallbacks(cmcg_solver s, int32_t* flags, int64_t* count);
 
 /* Adjoint of x = A^{-1} b for a loss L(x) (no reference counterpart):
  * solves A^T lambda = gx with this solver (A symmetric, so A lambda = gx;

@@ -3,6 +3,8 @@
 //   tests/TestSparseMultOp.cu:70-519   CSR / ELLPACK products, batched matrix / vector
 //   tests/TestReductionOps4.cu:39-87   dot {49, 32}, squaredNorm {46, 130}, norm
 //   tests/TestConjugateGradient.cu     early outs, dense solves, batched dense solve
+//   tests/TestSparseMatrix.cu:53-101   CSC pattern, sparse -> dense
+//   tests/TestBlockedConjugateGradient.cu:244-275   blocked (3x3) Poisson CG
 // plus a sparse 2D Poisson CG against the bundled Eigen's iteration count and
 // an FP64-refined solve. Prints one line per case; the exit status is the
 // number of failed cases.
@@ -332,6 +334,54 @@ int main() {
         REQUIRE(cg2.error() < 1e-10);
         auto st = cg2.systemStats(1);
         REQUIRE(st.status[0] == CMCG_SOLVE_CONVERGED);
+    });
+    run("CSC sparse matrix to dense", [] {
+        // TestSparseMatrix.cu:53-101: 4 x 5, column pointers JA, row indices IA
+        SparsityPattern<CSC> p;
+        p.rows = 4;
+        p.cols = 5;
+        p.nnz = 9;
+        p.IA = SparsityPattern<CSC>::IndexVector::fromHost(std::vector<int>{0, 2, 0, 1, 1, 3, 2, 2, 3}, 9);
+        p.JA = SparsityPattern<CSC>::IndexVector::fromHost(std::vector<int>{0, 2, 4, 6, 7, 9}, 6);
+        p.assertValid();
+        SparseMatrix<float, 2, CSC> A(p);
+        std::vector<float> v{1, 5, 4, 2, 3, 9, 7, 8, 6, -1, -5, -4, -2, -3, -9, -7, -8, -6};
+        A.getData().copyFromHost(v.data());
+        auto d = host(A.toDense());
+        const double want[4][5] = {{1, 4, 0, 0, 0}, {0, 2, 3, 0, 0}, {5, 0, 0, 7, 8}, {0, 0, 9, 0, 6}};
+        for (int b = 0; b < 2; ++b)
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 5; ++c) REQUIRE(d[static_cast<size_t>(b * 20 + r * 5 + c)] == (b ? -1 : 1) * want[r][c]);
+        // the transposed product of the CSC matrix: A^T (1, 1, 1, 1) = column sums
+        VectorXf ones = VectorXf::fromHost(std::vector<float>{1, 1, 1, 1}, 4);
+        SparseMatrix<float, 1, CSC> A1(p);
+        A1.getData().copyFromHost(v.data());
+        REQUIRE(close_rel(host(A1.transposedProduct(ones)), {6, 6, 12, 7, 14}, 1e-6));
+    });
+    run("Blocked CG", [] {
+        // TestBlockedConjugateGradient.cu:244-275: 3 x 3 blocks of 3 x 3
+        // (row-major), b = (0.1, 0, 0 | 0, 0, 0 | 0, 0, -0.1), tol 1e-5, 30 iterations
+        SparsityPattern<CSR> blocks;
+        blocks.rows = blocks.cols = 3;
+        blocks.nnz = 7;
+        blocks.JA = SparsityPattern<CSR>::IndexVector::fromHost(std::vector<int>{0, 2, 5, 7}, 4);
+        blocks.IA = SparsityPattern<CSR>::IndexVector::fromHost(std::vector<int>{0, 1, 0, 1, 2, 1, 2}, 7);
+        const std::vector<float> D{2, -1, 0, -1, 2, -1, 0, -1, 2}, U{0, 0, 0, 0, 0, 0, -1, 0, 0},
+            L{0, 0, -1, 0, 0, 0, 0, 0, 0}, E{2, -1, 0, -1, 2, -1, 0, -1, 1};
+        std::vector<float> vals;
+        for (const auto* blk : {&D, &U, &L, &D, &U, &L, &E}) vals.insert(vals.end(), blk->begin(), blk->end());
+        BlockSparseMatrix<float, 3> mat(blocks);
+        mat.getData().copyFromHost(vals.data());
+        VectorXf b = VectorXf::fromHost(std::vector<float>{0.1f, 0, 0, 0, 0, 0, 0, 0, -0.1f}, 9);
+        ConjugateGradient<BlockSparseMatrix<float, 3>> cg(mat);
+        cg.setMaxIterations(30);
+        cg.setTolerance(1e-5);
+        VectorXf x = cg.solve(b);
+        REQUIRE(cg.error() < cg.tolerance());
+        REQUIRE(cg.iterations() < cg.maxIterations());
+        REQUIRE(cg.iterations() > 0);
+        // A x reproduces b
+        REQUIRE(close_rel(host(mat * x), {0.1, 0, 0, 0, 0, 0, 0, 0, -0.1}, 1e-4));
     });
     std::printf("%d failed\n", g_failed);
     return g_failed;

@@ -64,6 +64,19 @@ def kats() -> dict:
         "sparse_to_dense_csr": {"source": "tests/TestSparseMatrix.cu:10-50", **csr,
                                 "values_b1": [-1, -4, -2, -3, -5, -7, -8, -9, -6],
                                 "dense_b0": [[1, 4, 0, 0, 0], [0, 2, 3, 0, 0], [5, 0, 0, 7, 8], [0, 0, 9, 0, 6]]},
+        "sparse_to_dense_csc": {"source": "tests/TestSparseMatrix.cu:53-101", "rows": 4, "cols": 5,
+                                "JA": [0, 2, 4, 6, 7, 9], "IA": [0, 2, 0, 1, 1, 3, 2, 2, 3],
+                                "values_b0": [1, 5, 4, 2, 3, 9, 7, 8, 6],
+                                "values_b1": [-1, -5, -4, -2, -3, -9, -7, -8, -6],
+                                "dense_b0": [[1, 4, 0, 0, 0], [0, 2, 3, 0, 0], [5, 0, 0, 7, 8], [0, 0, 9, 0, 6]]},
+        "blocked_cg": {"source": "tests/TestBlockedConjugateGradient.cu:244-275 (3x3 blocks, row-major; the "
+                                 "reference's float4 rows carry a zero 4th component, left out here)",
+                       "block_rows": 3, "block_size": 3, "JA": [0, 2, 5, 7], "IA": [0, 1, 0, 1, 2, 1, 2],
+                       "blocks": [[[2, -1, 0], [-1, 2, -1], [0, -1, 2]], [[0, 0, 0], [0, 0, 0], [-1, 0, 0]],
+                                  [[0, 0, -1], [0, 0, 0], [0, 0, 0]], [[2, -1, 0], [-1, 2, -1], [0, -1, 2]],
+                                  [[0, 0, 0], [0, 0, 0], [-1, 0, 0]], [[0, 0, -1], [0, 0, 0], [0, 0, 0]],
+                                  [[2, -1, 0], [-1, 2, -1], [0, -1, 1]]],
+                       "b": [[0.1, 0, 0], [0, 0, 0], [0, 0, -0.1]], "tol": 1e-5, "max_iterations": 30},
         "dot": {"source": "tests/TestReductionOps4.cu:39-63", "x": [[1, 2, 6], [2, 1, 3]], "y": [[5, -2, 8]],
                 "out": [49, 32]},
         "squared_norm": {"source": "tests/TestReductionOps4.cu:65-87", "x": [[5, 2, 4, 1], [11, 0, 0, -3]],

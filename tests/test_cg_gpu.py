@@ -721,3 +721,37 @@ def test_grid_diagonal_layout_matches_sliced(cuda, monkeypatch, kind):
     assert s1["status"][0] == 0
     r = p3.b.astype(np.float64) - O.spmv_csr_f32_in_f64(p3.n, p3.n, p3.row_ptr, p3.col, p3.val, x1)[0]
     assert np.linalg.norm(r) / np.linalg.norm(p3.b.astype(np.float64)) < 1.5e-10
+
+
+def test_bf16_values_fall_back_to_fp32(cuda, monkeypatch):
+    # BF16 values round the Jacobi-scaled systems by up to 2^-9; on the larger,
+    # worse-conditioned systems of this batch the reliable updates stop
+    # contracting. Those systems are solved again with the FP32 values and
+    # reported per system; every system then meets the FP64 target.
+    m = cm()
+    bt = P.fv2d_batch(40, 16, 128, 0.5, 23)
+    p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
+    p.set_systems(bt.row_off)
+    Ai = m.SparseMatrix(p, dtype=torch.bfloat16).setData(bt.val)
+    Ao = m.SparseMatrix(p, dtype=torch.float32).setData(bt.val)
+    b64 = bt.b.astype(np.float64)
+    cg = m.ConjugateGradient(Ai).setTolerance(1e-4)
+    x = cg.solve_refined(torch.from_numpy(b64).to(cuda), outer=Ao, outer_tol=1e-10, max_outer=60).cpu().numpy()
+    st = cg.system_stats()
+    assert np.all(st["status"] == 0) and np.all(st["error"] < 1e-10)
+    r = b64 - O.spmv_csr_f32_in_f64(bt.n, bt.n, bt.row_ptr, bt.col, bt.val, x)[0]
+    for s in range(bt.n_sys):
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.linalg.norm(r[r0:r1]) / np.linalg.norm(b64[r0:r1]) < 1e-10
+    # the same solve without the fallback: exactly the re-solved systems end
+    # unconverged, the others are unchanged
+    monkeypatch.setenv("CUMAT_CG_BF16_FALLBACK", "0")
+    cg0 = m.ConjugateGradient(Ai).setTolerance(1e-4)
+    x0 = cg0.solve_refined(torch.from_numpy(b64).to(cuda), outer=Ao, outer_tol=1e-10, max_outer=60).cpu().numpy()
+    s0 = cg0.system_stats()
+    assert st["fallback"].sum() > 0
+    assert np.array_equal(s0["status"] != 0, st["fallback"] == 1)
+    assert s0["fallback"].sum() == 0
+    for s in np.nonzero(st["fallback"] == 0)[0]:
+        r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+        assert np.array_equal(x[r0:r1], x0[r0:r1])
