@@ -6,12 +6,12 @@ Importing fails if the library has not been built (no CPU fallback).
 """
 from . import _native
 from ._native import CuMatError, launch_count
-from .sparse import (CSR, ELLPACK, Context, SparseMatrix, SparsityPattern, dot, linear_combination, norm, sddmm,
-                     squaredNorm)
+from .sparse import (BSR, CSC, CSR, ELLPACK, Context, SparseMatrix, SparsityPattern, dot, linear_combination, norm,
+                     reduce, sddmm, set_log_callback, squaredNorm)
 from .solvers import ConjugateGradient, DiagonalPreconditioner, IdentityPreconditioner
 
 __all__ = [
-    "CSR", "ELLPACK", "Context", "SparseMatrix", "SparsityPattern", "dot", "linear_combination", "norm", "squaredNorm",
-    "sddmm",
+    "CSR", "CSC", "BSR", "ELLPACK", "Context", "SparseMatrix", "SparsityPattern", "dot", "linear_combination", "norm",
+    "squaredNorm", "sddmm", "reduce", "set_log_callback",
     "ConjugateGradient", "DiagonalPreconditioner", "IdentityPreconditioner", "CuMatError", "launch_count",
 ]

@@ -18,6 +18,8 @@ ASSIGN, ADD, SUB = 0, 1, 2
 SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_ZERO_RHS, SOLVE_BREAKDOWN, SOLVE_NON_FINITE = 0, 1, 2, 3, 4
 PATH_AUTO, PATH_PERSISTENT, PATH_GRID, PATH_PERSISTENT_GLOBAL = 0, 1, 2, 3
 REFINE_RELIABLE, REFINE_RESTART = 0, 1
+REDUCE_SUM, REDUCE_PROD, REDUCE_MIN, REDUCE_MAX = 0, 1, 2, 3
+AXIS_ROW, AXIS_COLUMN, AXIS_BATCH = 1, 2, 4
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "OUT_OF_MEMORY", 4: "NOT_SUPPORTED", 5: "INTERNAL"}
 
 _vp = C.c_void_p
@@ -58,6 +60,8 @@ SIGNATURES = {
     "cmcg_spmv": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32]),
     "cmcg_spmv_transposed": (_i32, [_vp, _i32, _vp, _i32, _vp, _i32]),
     "cmcg_matrix_to_dense": (_i32, [_vp, _vp, _i32]),
+    "cmcg_reduce": (_i32, [_vp, _i32, _i32, _i64, _i64, _i64, _i32, _vp, _vp]),
+    "cmcg_set_log_callback": (_i32, [_vp, _i32, _vp]),
     "cmcg_matrix_from_dense": (_i32, [_vp, _vp, _i32]),
     "cmcg_dot": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp, _i32, _vp]),
     "cmcg_squared_norm": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp]),

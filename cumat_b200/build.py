@@ -30,8 +30,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                   "-I" + str(ROOT / "include")]
 
-CU_SOURCES = ["runtime.cu", "spmv.cu", "sell.cu", "sparse_ops.cu", "cg.cu", "cg_mixed.cu", "cg_plain.cu", "cg_coop.cu",
-              "lincomb.cu"]
+CU_SOURCES = ["runtime.cu", "spmv.cu", "sell.cu", "sparse_ops.cu", "reduce.cu", "cg.cu", "cg_mixed.cu", "cg_plain.cu",
+              "cg_coop.cu", "lincomb.cu"]
 HEADERS = ["common.cuh", "objects.h", "spmv_dev.cuh", "cg_dev.cuh", "tma.cuh", "cg_smem.cuh", "cg_grid.cuh",
            "grid_sync.cuh", "cg_compact.cuh", "cg_plain.cuh"]
 

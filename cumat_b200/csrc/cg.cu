@@ -2351,6 +2351,9 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
     CMCG_TRY(ensure_sell_values(s->A));
     const bool smem_ok = (FMT == CMCG_CSR && compact_ok(s)) || (sizeof(VT) == 4 && s->use_smem);
     const int32_t path = choose_path(s, n_inst, smem_ok);
+    if (log_on(2))
+        log_msg(2, "solve: %d instances of up to %d rows, %s vectors, %s path", n_inst, s->max_sys_rows,
+                sizeof(VT) == 8 ? "FP64" : "FP32", path == CMCG_PATH_GRID ? "grid" : "persistent");
     const size_t vbytes = sizeof(VT) * static_cast<size_t>(p->rows) * ob;
     SolveArgs<VT, MT> a = base_args<VT, MT>(s, ob);
     a.dinv = static_cast<const VT*>(dinv);
@@ -2510,6 +2513,9 @@ cmcg_status refined_persistent(cmcg_solver s, cmcg_matrix Ao, const double* b, i
             CMCG_TRY(ensure_aux_stream(s));
             CMCG_CUDA(cudaEventRecord(s->ev_fork, ctx->stream));
         }
+        if (log_on(2))
+            log_msg(2, "refined solve: %d instances on %d CTA tier(s) [%d, %d, %d instances], %s layout", n_inst, nt,
+                    lo[1] - lo[0], lo[2] - lo[1], lo[3] - lo[2], nd ? "diagonal" : "sliced");
         for (int j = 0; j < nt; ++j) {
             const int t = tiers[j];
             // the last (smallest) tier runs on the caller's stream
@@ -2896,6 +2902,7 @@ cmcg_status cmcg_cg_set_refinement(cmcg_solver s, int32_t method, double delta) 
 }
 
 cmcg_status cmcg_cg_solve(cmcg_solver s, int32_t vdt, const void* b, int32_t b_batches, const void* guess, void* x) {
+    NvtxRange nvtx_("cmcg_cg_solve");
     CMCG_REQUIRE(s && b && x, "cmcg_cg_solve: NULL argument");
     CMCG_REQUIRE(b_batches >= 1, "cmcg_cg_solve: b_batches must be >= 1");
     CMCG_REQUIRE(s->A->batches == 1 || b_batches == 1 || b_batches == s->A->batches,
@@ -2913,6 +2920,7 @@ cmcg_status cmcg_cg_solve(cmcg_solver s, int32_t vdt, const void* b, int32_t b_b
 
 cmcg_status cmcg_cg_solve_host(cmcg_solver s, int32_t vdt, const void* b_host, int32_t b_batches, const void* guess_host,
                                void* x_host) {
+    NvtxRange nvtx_("cmcg_cg_solve_host");
     CMCG_REQUIRE(s && b_host && x_host, "cmcg_cg_solve_host: NULL argument");
     CMCG_REQUIRE(vdt == CMCG_F32 || vdt == CMCG_F64, "cmcg_cg_solve_host: vector dtype must be F32 or F64");
     CMCG_REQUIRE(b_batches >= 1, "cmcg_cg_solve_host: b_batches must be >= 1");
@@ -3063,6 +3071,8 @@ cmcg_status bf16_fallback(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_
     // the list upload must finish before the host vector goes away
     CMCG_CUDA(cudaStreamSynchronize(ctx->stream));
     for (int32_t i : list) s->fallback[i] = 1;
+    log_msg(1, "refined solve: %zu of %d systems did not converge with BF16 values and were solved with FP32 values",
+            list.size(), n);
     return CMCG_OK;
 }
 
@@ -3072,6 +3082,7 @@ extern "C" {
 
 cmcg_status cmcg_cg_solve_refined(cmcg_solver s, cmcg_matrix Ao, const double* b, int32_t b_batches, double* x,
                                   double outer_tol, int32_t max_outer) {
+    NvtxRange nvtx_("cmcg_cg_solve_refined");
     CMCG_REQUIRE(s && b && x, "cmcg_cg_solve_refined: NULL argument");
     if (!Ao) Ao = s->A;
     s->fallback.clear();
@@ -3145,6 +3156,7 @@ extern "C" {
 
 cmcg_status cmcg_cg_adjoint(cmcg_solver s, cmcg_matrix Ao, const double* x, const double* gx, int32_t batches, double* gb,
                             double* gA, double outer_tol, int32_t max_outer) {
+    NvtxRange nvtx_("cmcg_cg_adjoint");
     CMCG_REQUIRE(s && x && gx && gb, "cmcg_cg_adjoint: NULL argument");
     // A symmetric: A^T lambda = gx is A lambda = gx, solved by the same fused CG
     CMCG_TRY(cmcg_cg_solve_refined(s, Ao, gx, batches, gb, outer_tol, max_outer));

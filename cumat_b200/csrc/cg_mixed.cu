@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
     __shared__ float red[2 * (T / 32)];
     __shared__ double red64[2 * (T / 32)];
     __shared__ int slot;
+    __shared__ int guard[3];
     const int M = ND > 0 ? a.margin : 0;
     float* P = smf + M;
     float* R = smf + nmax + 2 * M;
@@ -205,8 +206,16 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
         else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
         else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
         const int64_t maxit = sys_max_iter(a.max_inner, n);
-        // progress guard (stall_len): forced replacements, stalls in a row
-        int it_rep = 0, cyc0 = 0, stalls = 0;
+        // progress guard (stall_len) in shared memory, so that the iteration
+        // loop keeps its registers: guard[0] = iteration that forces the next
+        // replacement, [1] = first cycle's length, [2] = stalls in a row;
+        // written by thread 0 inside a replacement, between barriers
+        if (tid == 0) {
+            guard[0] = kStallFirst;
+            guard[1] = 0;
+            guard[2] = 0;
+        }
+        __syncthreads();
         bool folded = true;
         // diagonal layout: alpha of the x increment not yet added to xh
         bool pend = false;
@@ -265,7 +274,7 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
             // replace the residual when it dropped by delta, or when it suggests
             // that the FP64 residual may have reached the target, or when the
             // cycle has run too long (progress guard)
-            if (rzn < d2 * rmax || rzn < goal || it - it_rep >= stall_len(updates, cyc0)) {
+            if (rzn < d2 * rmax || rzn < goal || it >= guard[0]) {
                 if (ND > 0 && pend) {
                     CMCG_DIA_SLOTS(nk, (dia_xinc<NK, T>(P, XH, tid, alpha_pend)))
                     pend = false;
@@ -296,9 +305,15 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
                 block_sum<double, 2>(t2, red64);
                 ++updates;
                 folded = true;
-                stalls = t2[0] > kStallRatio * rr64 ? stalls + 1 : 0;
-                if (updates == 1) cyc0 = it;
-                it_rep = it;
+                // (every thread has read guard[] for this iteration: block_sum synchronised)
+                const int stalls = t2[0] > kStallRatio * rr64 ? guard[2] + 1 : 0;
+                const int cyc0 = updates == 1 ? it : guard[1];
+                __syncthreads();
+                if (tid == 0) {
+                    guard[0] = it + stall_len(updates, cyc0);
+                    guard[1] = cyc0;
+                    guard[2] = stalls;
+                }
                 rr64 = t2[0];
                 rzn = static_cast<float>(t2[1]);
                 rmax = rzn;

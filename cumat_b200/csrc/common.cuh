@@ -3,6 +3,7 @@
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <cstdio>
@@ -39,6 +40,20 @@ cmcg_status cuda_fail(cudaError_t e, const char* what, const char* file, int lin
         cmcg_status s_ = (expr);                                                 \
         if (s_ != CMCG_OK) return s_;                                            \
     } while (0)
+
+// Log hook (cmcg_set_log_callback / CUMAT_LOG): level 0 = error, 1 = info,
+// 2 = detail. log_on tells whether a message of that level goes anywhere, so
+// callers skip formatting otherwise.
+bool log_on(int level);
+void log_msg(int level, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+
+// NVTX range over an entry point (a no-op unless a tool listens)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Number of kernel launches issued by this library on the current host thread
 // (a test hook in the spirit of the reference's CUMAT_PROFILING counters,

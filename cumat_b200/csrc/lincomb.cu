@@ -158,6 +158,7 @@ using namespace cmcg;
 extern "C" cmcg_status cmcg_lincomb(cmcg_ctx ctx, int32_t dtype, int64_t n, int32_t n_terms, const double* coeffs,
                                     const void* const* vectors, const int32_t* v_batches, void* out,
                                     int32_t out_batches, int32_t mode) {
+    NvtxRange nvtx_("cmcg_lincomb");
     CMCG_REQUIRE(ctx && coeffs && vectors && v_batches && out, "cmcg_lincomb: NULL argument");
     CMCG_REQUIRE(dtype == CMCG_F32 || dtype == CMCG_F64, "cmcg_lincomb: dtype must be F32 or F64");
     CMCG_REQUIRE(n_terms >= 1 && n_terms <= kMaxTerms, "cmcg_lincomb: 1 to 16 terms");

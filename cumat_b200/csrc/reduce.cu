@@ -51,8 +51,8 @@ const char* const kKernName[K_COUNT] = {"thread", "warp", "block", "split"};
 
 struct View {
     int64_t K1, O1, K2, O2;
-    int64_t outputs() const { return O1 * O2; }
-    int64_t length() const { return K1 * K2; }
+    __host__ __device__ int64_t outputs() const { return O1 * O2; }
+    __host__ __device__ int64_t length() const { return K1 * K2; }
 };
 
 template <typename T, int OP>
@@ -360,6 +360,7 @@ cmcg_status reduce_t(cmcg_ctx ctx, const View& v, const void* in_, void* out_) {
         red_choices()[key] = pick;
         red_cache_store(key, pick);
     }
+    log_msg(1, "reduction %s: %s kernel timed fastest (%.3f ms for 3 calls)", key.c_str(), kKernName[pick], best);
     // the last candidate's result is in out; rerun the pick if it was another one
     return pick == cand[nc - 1] ? CMCG_OK : launch_kern<T, OP>(ctx, pick, v, in, out);
 }
@@ -384,6 +385,7 @@ extern "C" {
 
 cmcg_status cmcg_reduce(cmcg_ctx ctx, int32_t dtype, int32_t op, int64_t rows, int64_t cols, int64_t batches,
                         int32_t axes, const void* in, void* out) {
+    NvtxRange nvtx_("cmcg_reduce");
     CMCG_REQUIRE(ctx && in && out, "cmcg_reduce: NULL argument");
     CMCG_REQUIRE(rows > 0 && cols > 0 && batches > 0, "cmcg_reduce: sizes must be positive");
     CMCG_REQUIRE((axes & ~7) == 0, "cmcg_reduce: axes is a mask of CMCG_AXIS_ROW | COLUMN | BATCH");

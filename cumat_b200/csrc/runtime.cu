@@ -7,8 +7,13 @@
 // shared pointers, and patterns are validated on the host when created (the
 // reference only asserts sizes, SparseMatrixBase.h:112-119).
 
+#include <atomic>
 #include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -21,10 +26,46 @@ thread_local std::string g_last_error;
 thread_local int64_t g_launches = 0;
 }  // namespace
 
-void set_error(const std::string& msg) { g_last_error = msg; }
+// ---- log hook ---------------------------------------------------------------------
+namespace {
+std::mutex g_log_mu;
+std::atomic<cmcg_log_fn> g_log_cb{nullptr};
+std::atomic<int> g_log_level{-1};
+void* g_log_user = nullptr;
+// CUMAT_LOG=<level>: messages up to that level go to stderr when no callback is set
+int env_log_level() {
+    static const int lv = [] {
+        const char* e = std::getenv("CUMAT_LOG");
+        return e ? std::atoi(e) : -1;
+    }();
+    return lv;
+}
+}  // namespace
+
+bool log_on(int level) {
+    return g_log_cb.load() ? level <= g_log_level.load() : level <= env_log_level();
+}
+
+void log_msg(int level, const char* fmt, ...) {
+    if (!log_on(level)) return;
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    std::lock_guard<std::mutex> lk(g_log_mu);
+    if (cmcg_log_fn cb = g_log_cb.load()) cb(level, buf, g_log_user);
+    else std::fprintf(stderr, "[cumat_b200:%d] %s\n", level, buf);
+}
+
+void set_error(const std::string& msg) {
+    g_last_error = msg;
+    log_msg(0, "%s", msg.c_str());
+}
 
 cmcg_status fail(cmcg_status code, const std::string& msg) {
     g_last_error = msg;
+    log_msg(0, "%s", msg.c_str());
     return code;
 }
 
@@ -32,6 +73,7 @@ cmcg_status cuda_fail(cudaError_t e, const char* what, const char* file, int lin
     const char* base = std::strrchr(file, '/');
     g_last_error = std::string("CUDA error '") + cudaGetErrorString(e) + "' in " + what + " (" +
                    (base ? base + 1 : file) + ":" + std::to_string(line) + ")";
+    log_msg(0, "%s", g_last_error.c_str());
     return e == cudaErrorMemoryAllocation ? CMCG_ERR_OUT_OF_MEMORY : CMCG_ERR_CUDA;
 }
 
@@ -301,6 +343,14 @@ static cmcg_status upload_default_systems(cmcg_pattern p) {
     const int32_t h[2] = {0, p->rows};
     CMCG_CUDA(cudaMemcpyAsync(p->d_row_off, h, sizeof(h), cudaMemcpyHostToDevice, p->ctx->stream));
     CMCG_CUDA(cudaStreamSynchronize(p->ctx->stream));
+    return CMCG_OK;
+}
+
+cmcg_status cmcg_set_log_callback(cmcg_log_fn callback, int32_t max_level, void* user) {
+    std::lock_guard<std::mutex> lk(g_log_mu);
+    g_log_user = user;
+    g_log_level.store(max_level);
+    g_log_cb.store(callback);
     return CMCG_OK;
 }
 

@@ -367,6 +367,7 @@ cmcg_status cmcg_pattern_create_bsr(cmcg_ctx ctx, int32_t block_rows, int32_t bl
 
 cmcg_status cmcg_spmv_transposed(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t x_batches, void* y,
                                  int32_t mode) {
+    NvtxRange nvtx_("cmcg_spmv_transposed");
     CMCG_REQUIRE(A && x && y, "cmcg_spmv_transposed: NULL argument");
     CMCG_REQUIRE(A->pat->format == CMCG_CSR, "cmcg_spmv_transposed: CSR, CSC or BSR patterns only");
     CMCG_REQUIRE(x_batches >= 1 && (A->batches == 1 || x_batches == 1 || x_batches == A->batches),

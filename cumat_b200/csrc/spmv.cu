@@ -803,6 +803,8 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     if (p->format == CMCG_CSR) {
         const int vec = csr_vec_variant(p);
         if (vec >= 0) {
+            log_msg(1, "product: skewed rows (%d rows, %lld entries), %d lanes per row", p->rows,
+                    static_cast<long long>(p->nnz), 4 << (vec - 3));
             choice = static_cast<int8_t>(vec);
             return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, vec);
         }
@@ -847,6 +849,7 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     if (rc != CMCG_OK) return rc;
     choice = static_cast<int8_t>(pick);
     tune_store(key, pick);
+    log_msg(1, "product %s: variant %d timed fastest (%.3f ms for 3 calls)", key.c_str(), pick, best);
     // the last candidate's output is in y; rerun the pick if it was another one
     return pick == cands[1] ? CMCG_OK : launch_spmv_variant<MT, VT>(A, x, xb, y, mode, pick);
 }
@@ -904,6 +907,7 @@ using namespace cmcg;
 extern "C" {
 
 cmcg_status cmcg_spmv(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t x_batches, void* y, int32_t mode) {
+    NvtxRange nvtx_("cmcg_spmv");
     CMCG_REQUIRE(A && x && y, "cmcg_spmv: NULL argument");
     CMCG_REQUIRE(x_batches >= 1, "cmcg_spmv: x_batches must be >= 1");
     CMCG_REQUIRE(A->batches == 1 || x_batches == 1 || A->batches == x_batches,
@@ -915,6 +919,7 @@ cmcg_status cmcg_spmv(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t x
 
 cmcg_status cmcg_dot(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb,
                      void* out) {
+    NvtxRange nvtx_("cmcg_dot");
     CMCG_REQUIRE(ctx && x && y && out, "cmcg_dot: NULL argument");
     CMCG_REQUIRE(n >= 0 && xb >= 1 && yb >= 1, "cmcg_dot: bad size");
     CMCG_REQUIRE(xb == 1 || yb == 1 || xb == yb, "cmcg_dot: batch counts must match or be 1");
@@ -924,6 +929,7 @@ cmcg_status cmcg_dot(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int3
 }
 
 cmcg_status cmcg_squared_norm(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t batches, void* out) {
+    NvtxRange nvtx_("cmcg_squared_norm");
     return cmcg_dot(ctx, dtype, n, x, batches, x, batches, out);
 }
 
@@ -996,6 +1002,7 @@ extern "C" {
 
 cmcg_status cmcg_dot_noalloc(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t xb, const void* y,
                              int32_t yb, void* out) {
+    NvtxRange nvtx_("cmcg_dot_noalloc");
     CMCG_REQUIRE(ctx && x && y && out, "cmcg_dot_noalloc: NULL argument");
     CMCG_REQUIRE(n >= 0 && xb >= 1 && yb >= 1, "cmcg_dot_noalloc: bad size");
     CMCG_REQUIRE(xb == 1 || yb == 1 || xb == yb, "cmcg_dot_noalloc: batch counts must match or be 1");
@@ -1012,6 +1019,7 @@ cmcg_status cmcg_dot_noalloc(cmcg_ctx ctx, int32_t dtype, int64_t n, const void*
 
 cmcg_status cmcg_sddmm(cmcg_matrix M, int32_t vec_dtype, double alpha, const void* u, int32_t ub, const void* v,
                        int32_t vb, void* out, int32_t ob) {
+    NvtxRange nvtx_("cmcg_sddmm");
     CMCG_REQUIRE(M && u && v && out, "cmcg_sddmm: NULL argument");
     CMCG_REQUIRE(ub >= 1 && vb >= 1 && ob >= 1, "cmcg_sddmm: batch counts must be >= 1");
     CMCG_REQUIRE((ub == 1 || ub == ob) && (vb == 1 || vb == ob), "cmcg_sddmm: batch counts must match or be 1");

@@ -407,3 +407,44 @@ def sddmm(A: SparseMatrix, u: torch.Tensor, v: torch.Tensor, alpha: float = 1.0)
     N.call("cmcg_sddmm", A.handle, _TORCH_DT[u.dtype], float(alpha), _vp(u.contiguous()), ub, _vp(v.contiguous()), vb,
            _vp(out), ob)
     return out
+
+
+_REDUCE_OPS = {"sum": N.REDUCE_SUM, "prod": N.REDUCE_PROD, "min": N.REDUCE_MIN, "max": N.REDUCE_MAX}
+_AXES = {"rows": N.AXIS_ROW, "cols": N.AXIS_COLUMN, "batches": N.AXIS_BATCH}
+
+
+def reduce(x: torch.Tensor, op: str = "sum", axes=("rows",)) -> torch.Tensor:
+    """Reduction of a dense batched matrix along any set of axes, like the
+    reference's ``sum<ReductionAxis::Row | ...>()`` / ``prod`` / ``minCoeff`` /
+    ``maxCoeff``. ``x`` is (batches, cols, rows) in memory order (rows fastest,
+    the reference's ColumnMajor; a 2-D tensor is one batch); ``axes`` names the
+    reduced ones. Returns the kept axes in the same order, reduced axes kept
+    with size 1."""
+    if x.dim() == 2:
+        x = x.unsqueeze(0)
+    B, Cc, R = x.shape
+    mask = 0
+    for a in axes:
+        mask |= _AXES[a]
+    out = torch.empty((1 if mask & N.AXIS_BATCH else B, 1 if mask & N.AXIS_COLUMN else Cc,
+                       1 if mask & N.AXIS_ROW else R), dtype=x.dtype, device=x.device)
+    N.call("cmcg_reduce", Context.current().handle, _TORCH_DT[x.dtype], _REDUCE_OPS[op], R, Cc, B, mask,
+           _vp(x.contiguous()), _vp(out))
+    return out
+
+
+_log_keep = []
+
+
+def set_log_callback(fn, max_level: int = 1) -> None:
+    """Routes the library's log messages (level 0 errors, 1 decisions such as
+    tuned kernels and FP32 fallbacks, 2 details of every solve) to
+    ``fn(level, message)``; ``None`` removes the callback."""
+    if fn is None:
+        N.call("cmcg_set_log_callback", None, 0, None)
+        _log_keep.clear()
+        return
+    proto = C.CFUNCTYPE(None, C.c_int32, C.c_char_p, C.c_void_p)
+    cb = proto(lambda level, msg, user: fn(int(level), msg.decode(errors="replace")))
+    _log_keep[:] = [cb]
+    N.call("cmcg_set_log_callback", C.cast(cb, C.c_void_p), int(max_level), None)

@@ -113,6 +113,18 @@ cmcg_status cmcg_device_free(cmcg_ctx ctx, void* p);
 cmcg_status cmcg_memcpy(cmcg_ctx ctx, void* dst, const void* src, int64_t bytes, int32_t kind);
 cmcg_status cmcg_memset_zero(cmcg_ctx ctx, void* dst, int64_t bytes);
 cmcg_status cmcg_ctx_stream(cmcg_ctx ctx, void** stream);
+/* Log hook (no reference counterpart; the reference has no logging): the
+ * library reports what it decided and what went wrong (the kernel a product
+ * or reduction tuned to, the execution path and CTA tiers of a solve, systems
+ * re-solved with FP32 values, failures with their message) through
+ * callback(level, message, user) with level 0 = error, 1 = info, 2 = detail,
+ * for every message at or below max_level. NULL removes the callback.
+ * CUMAT_LOG=<level> in the environment logs to stderr instead when no
+ * callback is set. Solves, products and reductions are also marked as NVTX
+ * ranges ("cmcg_cg_solve", ...) for Nsight timelines. */
+typedef void (*cmcg_log_fn)(int32_t level, const char* message, void* user);
+cmcg_status cmcg_set_log_callback(cmcg_log_fn callback, int32_t max_level, void* user);
+
 /* Synchronises and returns (then clears) the context's device error bits:
  * bit 0 = a bulk-copy (mbarrier) wait ran out, bit 1 = a grid-barrier wait of
  * the cooperative solver ran out. Every device-side wait is bounded (no
@@ -238,6 +250,22 @@ cmcg_status cmcg_squared_norm(cmcg_ctx ctx, int32_t dtype, int64_t n, const void
  * other threads) race and must be serialised by the caller. */
 cmcg_status cmcg_dot_noalloc(cmcg_ctx ctx, int32_t dtype, int64_t n, const void* x, int32_t x_batches, const void* y,
                              int32_t y_batches, void* out);
+
+/* Reduction of a dense batched matrix along any set of axes (reference: the
+ * sum / prod / minCoeff / maxCoeff reductions over rows, columns and batches,
+ * cuMat/src/ReductionOps.h, ReductionOpsPlugin.inl, with the algorithm
+ * selection of ReductionAlgorithmSelection.h:40-112). in: device,
+ * [batches][cols][rows] (rows fastest, the reference's ColumnMajor), dtype F32
+ * or F64; axes: a mask of CMCG_AXIS_ROW | CMCG_AXIS_COLUMN | CMCG_AXIS_BATCH
+ * (0 copies); out: device, the kept axes in the same order. The kernel
+ * (thread, warp or CTA per output, or outputs split over several CTAs) is
+ * picked per shape by timing on first use and kept in memory and in the
+ * tuning cache file; each kernel combines in a fixed order, so results are
+ * deterministic for a given choice (MIN / MAX for any). */
+enum { CMCG_REDUCE_SUM = 0, CMCG_REDUCE_PROD = 1, CMCG_REDUCE_MIN = 2, CMCG_REDUCE_MAX = 3 };
+enum { CMCG_AXIS_ROW = 1, CMCG_AXIS_COLUMN = 2, CMCG_AXIS_BATCH = 4 };
+cmcg_status cmcg_reduce(cmcg_ctx ctx, int32_t dtype, int32_t op, int64_t rows, int64_t cols, int64_t batches,
+                        int32_t axes, const void* in, void* out);
 
 /* out (mode)= sum_t coeffs[t] * v_t over n_terms <= 16 vectors, for every
  * batch, in one streaming pass (reference: the cwise evaluation of

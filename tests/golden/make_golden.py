@@ -77,6 +77,22 @@ def kats() -> dict:
                                   [[0, 0, 0], [0, 0, 0], [-1, 0, 0]], [[0, 0, -1], [0, 0, 0], [0, 0, 0]],
                                   [[2, -1, 0], [-1, 2, -1], [0, -1, 1]]],
                        "b": [[0.1, 0, 0], [0, 0, 0], [0, 0, -0.1]], "tol": 1e-5, "max_iterations": 30},
+        "reduce_axes": {"source": "tests/TestReductionOps2.cu:13-158 (sum), TestReductionOps3.cu:70-125 (min, max "
+                                  "over all); data[batch][row][col]; 'row' sums over the row index",
+                        "data": [[[5, 2, 4, 1], [8, 5, 6, 2], [-5, 0, 3, -9]],
+                                 [[11, 0, 0, 3], [-7, -2, -4, 1], [9, 4, 7, -7]]],
+                        "sum": {"none": [[[5, 2, 4, 1], [8, 5, 6, 2], [-5, 0, 3, -9]],
+                                         [[11, 0, 0, 3], [-7, -2, -4, 1], [9, 4, 7, -7]]],
+                                "column": [[[12], [21], [-11]], [[14], [-12], [13]]],
+                                "row": [[[8, 7, 13, -6]], [[13, 2, 3, -3]]],
+                                "batch": [[[16, 2, 4, 4], [1, 3, 2, 3], [4, 4, 10, -16]]],
+                                "row+column": [[[22]], [[15]]],
+                                "column+batch": [[[26], [9], [2]]],
+                                "row+batch": [[[21, 9, 16, -9]]],
+                                "row+column+batch": [[[37]]]},
+                        "min_all": -9, "max_all": 11},
+        "reduce_prod": {"source": "tests/TestReductionOps3.cu:42-68",
+                        "data": [[[1, 2], [1, 1], [-5, 1]], [[2, 1], [-3, -2], [2, 1]]], "prod_all": -240},
         "dot": {"source": "tests/TestReductionOps4.cu:39-63", "x": [[1, 2, 6], [2, 1, 3]], "y": [[5, -2, 8]],
                 "out": [49, 32]},
         "squared_norm": {"source": "tests/TestReductionOps4.cu:65-87", "x": [[5, 2, 4, 1], [11, 0, 0, -3]],

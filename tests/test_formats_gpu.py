@@ -152,9 +152,11 @@ def test_kat_blocked_cg(cuda):
 
 
 def _block_poisson(g, B, seed):
-    """2D Poisson on a g x g grid of B-vector unknowns coupled through SPD
-    blocks: diagonal blocks 4 I + C (C a random symmetric coupling with
-    |C| < 1), off-diagonal blocks -I; SPD."""
+    """2D Poisson on a g x g grid of B-vector unknowns coupled inside each
+    cell: diagonal blocks 5 I + C (C random symmetric, entries in [-0.1,
+    0.1], so its eigenvalues exceed -0.1 B >= -0.4), off-diagonal blocks -I:
+    the Laplacian (eigenvalues > 0) plus a block diagonal with eigenvalues
+    above 0.6, so SPD."""
     rng = np.random.default_rng(seed)
     n = g * g
     brp, bci, blocks = [0], [], []
@@ -166,8 +168,8 @@ def _block_poisson(g, B, seed):
                 nb.append((x + dx) * g + (y + dy))
         for c in sorted(nb):
             if c == r:
-                C = rng.uniform(-0.2, 0.2, (B, B))
-                blocks.append(4 * np.eye(B) + (C + C.T) / 2)
+                C = rng.uniform(-0.1, 0.1, (B, B))
+                blocks.append(5 * np.eye(B) + (C + C.T) / 2)
             else:
                 blocks.append(-np.eye(B))
             bci.append(c)
