@@ -440,6 +440,34 @@ def cg_config2(cm, torch, dev, stream, hbm_peak):
             "gbs_model": round(gbs, 1), "frac_model": round(gbs / hbm_peak, 3)}
 
 
+def cg_poisson10000(cm, torch, dev, stream, hbm_peak):
+    """The grid path's iteration on the 10000^2 Poisson matrix (10^8 rows, FP32,
+    Jacobi; every vector 400 MB, far above L2): the per-iteration time is the
+    difference of two solves capped at 40 and 10 iterations, over 30. The
+    diagonal-layout iteration streams 72 B per row: product + p.q (5 values,
+    p, q: 28 B), x / r update + |r|^2 + r.z (x, p, r, q, 1/diag read, x, r
+    written: 28 B), p update (r, p, 1/diag read, p written: 16 B)."""
+    from cumat_b200 import problems as P
+    pr = P.poisson2d(10000, 1)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    b = torch.from_numpy(pr.b).to(dev)
+    x = torch.empty_like(b)
+    del pr
+    t = {}
+    for k in (10, 40):
+        cg = cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(k).set_path(2)
+        t[k] = _ev_time(torch, stream, lambda: cg.solve(b, out=x), 2)
+        its = cg.iterations()
+        del cg
+    us = (t[40] - t[10]) * 1e3 / 30
+    byt = 72.0 * A.rows
+    out = {"rows": A.rows, "us_per_iter": round(us, 2), "gbs_model": round(byt / us / 1e3, 1),
+           "frac_model": round(byt / us / 1e3 / hbm_peak, 3), "iterations_checked": int(its)}
+    del A, b, x
+    torch.cuda.empty_cache()
+    return out
+
+
 def precision_c4(cm, torch, dev, stream, reps=2):
     """The precision configuration: 3D 7-point finite-volume system on a 256^3
     grid (kappa = exp(N(0, 1)), seed 3, values exact in FP32), solved to a
@@ -576,17 +604,56 @@ def run_ours(args):
               "converged": int((st_sl["status"] == 0).sum()), "max_error": float(st_sl["error"].max())}
     del cg_sl
 
-    # end to end through the public API with pinned host buffers
+    # end to end through the public API with pinned host buffers: every step
+    # copies its right-hand sides in and its solutions out; the copies run on
+    # a copy stream with two device buffers each, so step k + 1's upload and
+    # step k - 1's download overlap step k's solve (as a stream of batches
+    # would run in an application)
     hb = torch.from_numpy(bt.b.astype(np.float64)).pin_memory()
-    hx = torch.empty(bt.n, dtype=torch.float64).pin_memory()
-    db = torch.empty_like(b64)
+    hx = [torch.empty(bt.n, dtype=torch.float64).pin_memory() for _ in range(2)]
+    db = [torch.empty_like(b64) for _ in range(2)]
+    dx = [torch.empty_like(b64) for _ in range(2)]
+    copy = torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_done = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
 
-    def e2e_step():
-        db.copy_(hb, non_blocking=True)
-        cg.solve_refined(db, outer=A32, outer_tol=OUTER_TOL, max_outer=MAX_OUTER, out=x64)
-        hx.copy_(x64, non_blocking=True)
+    def e2e_run(steps):
+        with torch.cuda.stream(copy):
+            db[0].copy_(hb, non_blocking=True)
+            ev_in[0].record(copy)
+        for i in range(steps):
+            j = i % 2
+            if i + 1 < steps:
+                with torch.cuda.stream(copy):
+                    if i >= 1:
+                        copy.wait_event(ev_done[1 - j])   # the solve that read db[1 - j]
+                    db[1 - j].copy_(hb, non_blocking=True)
+                    ev_in[1 - j].record(copy)
+            stream.wait_event(ev_in[j])
+            if i >= 2:
+                stream.wait_event(ev_out[j])              # dx[j]'s previous download
+            cg.solve_refined(db[j], outer=A32, outer_tol=OUTER_TOL, max_outer=MAX_OUTER, out=dx[j])
+            ev_done[j].record(stream)
+            with torch.cuda.stream(copy):
+                copy.wait_event(ev_done[j])
+                hx[j].copy_(dx[j], non_blocking=True)
+                ev_out[j].record(copy)
+        stream.wait_stream(copy)
 
-    ms_e2e = time_device(e2e_step, args.steps, 1, stream, world)
+    e2e_run(2)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    copy.wait_stream(stream)   # the first upload starts inside the timed region
+    e2e_run(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_e2e = max_over_ranks(world, e0.elapsed_time(e1) / args.steps)
+    assert np.array_equal(hx[(args.steps - 1) % 2].numpy(), x64.cpu().numpy()), "end-to-end result differs"
 
     extra = {}
     if rank == 0 and world == 1 and not args.no_spmv:
@@ -597,6 +664,7 @@ def run_ours(args):
         extra["reference_suite"] = reference_suite(cm, torch, dev, stream, hbm_peak)
     if rank == 0 and world == 1 and not args.no_configs:
         extra["cg_poisson1024"] = cg_config2(cm, torch, dev, stream, hbm_peak)
+        extra["cg_poisson10000"] = cg_poisson10000(cm, torch, dev, stream, hbm_peak)
         extra["precision_c4"] = precision_c4(cm, torch, dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -649,6 +717,9 @@ def run_ours(args):
         if "cg_poisson1024" in extra:
             c2 = extra["cg_poisson1024"]
             hl.update(c2_iters=c2["iterations"], c2_ms=c2["ms"], c2_us_per_iter=c2["us_per_iter"])
+        if "cg_poisson10000" in extra:
+            hl.update(cg10000_us_per_iter=extra["cg_poisson10000"]["us_per_iter"],
+                      cg10000_frac=extra["cg_poisson10000"]["frac_model"])
         if "precision_c4" in extra:
             c4 = extra["precision_c4"]
             hl.update(c4_f32_ms=c4["mixed_f32"]["ms"], c4_bf16_ms=c4["mixed_bf16"]["ms"], c4_fp64_ms=c4["fp64"]["ms"],
@@ -790,6 +861,8 @@ def run_profile_case(case: str):
                 sampled outer product on n = 64 Mi entries (k_dot, k_lincomb,
                 k_sddmm_csr on the 8192^2 Poisson pattern)
     spmv_big    CSR and ELLPACK products on the 8192^2 Poisson matrix (3 each)
+    cg10000     three grid-path Jacobi-CG iterations on the 10000^2 Poisson
+                matrix (FP32, diagonal layout: the fused product + p.q kernel)
     """
     import torch
 
@@ -809,6 +882,12 @@ def run_profile_case(case: str):
         cgm = cm.ConjugateGradient(A32).setTolerance(1e-4).setMaxIterations(20).set_path(2)
         cgm.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=3)
         out.update(rows=p3.n, nnz=p3.nnz)
+    elif case == "cg10000":
+        pr = P.poisson2d(10000, 1)
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+        b = torch.from_numpy(pr.b).to(dev)
+        cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(3).set_path(2).solve(b)
+        out.update(rows=pr.n, nnz=pr.nnz)
     elif case == "plain_dia":
         bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED)
         k = int(bt.row_off[512])
@@ -868,7 +947,7 @@ def main():
                     help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "
                          "mixed and FP64 solvers on the first 512 systems of the batch")
     ap.add_argument("--profile-case", default=None,
-                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big)")
+                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big, cg10000)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

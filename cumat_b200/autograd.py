@@ -35,7 +35,14 @@ class SparseSolveOp:
         self.max_outer = max_outer
 
     def set_values(self, values: torch.Tensor) -> None:
+        """values: (nnz,) or (batches, nnz); a new batch count rebuilds the
+        matrices and the solver on the same pattern."""
         v = values.detach().to(torch.float64).contiguous()
+        batches = 1 if v.dim() == 1 else v.shape[0]
+        if batches != self.A64.batches:
+            self.A32 = SparseMatrix(self.pattern, dtype=torch.float32, batches=batches)
+            self.A64 = SparseMatrix(self.pattern, dtype=torch.float64, batches=batches)
+            self.cg = ConjugateGradient(self.A32, DiagonalPreconditioner)
         self.A64.setData(v)
         self.A32.setData(v)
 

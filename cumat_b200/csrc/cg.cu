@@ -1360,7 +1360,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
                 atomicSub(a.active, 1);
             } else if (rzn < d2 * static_cast<float>(a.st.rmax[g.inst]) || rzn < static_cast<float>(a.st.goal[g.inst]) ||
                        it >= sys_max_iter(a.max_iter, n) ||
-                       it - a.st.rep_it[g.inst] >= stall_len(a.st.outer[g.inst], a.st.cyc0[g.inst])) {
+                       it - a.st.rep_it[g.inst] >= stall_len(a.st.outer[g.inst], a.st.cyc0[g.inst], m.delta)) {
                 a.st.flag[g.inst] = 1;   // fold and replace in this iteration
             } else if (!(rzn > 0.0f)) {
                 a.st.status[g.inst] = CMCG_SOLVE_BREAKDOWN;

@@ -11,7 +11,13 @@
 //   barrier: convergence, beta (last CTA to arrive)
 // Forming p_k inside the product removes the separate p update pass and its
 // barrier; the owner and every gatherer evaluate p_k(j) with the same
-// expression, so they agree bit for bit. The last CTA to reach a barrier adds
+// expression, so they agree bit for bit. When a CTA's rows lie in one system
+// and all their column indices in a window [c0, c1) that fits the CTA's
+// shared memory (stencils: the rows plus a halo as wide as the largest
+// offset), phase 1 first forms p_k over the whole window with coalesced
+// loads into shared memory and the product gathers from there: three
+// coalesced vector reads per window entry instead of three L2 gathers per
+// matrix entry, with the same expression and therefore the same values. The last CTA to reach a barrier adds
 // the phase's per-segment partials of every instance in a fixed order and
 // writes the scalars (alpha, beta, statuses, running count) before releasing
 // the others, so every CTA sees the same values and leaves the loop in the
@@ -29,6 +35,19 @@
 
 namespace cmcg {
 namespace {
+
+template <typename VT>
+struct WindowX {     // gathers from the shared-memory window [c0, c0 + width)
+    const VT* w;
+    int c0, width;
+    // every stored entry's column lies in the window; a padding slot of the
+    // sliced layout (value 0) may name a column outside it and reads an
+    // entry of the window instead
+    __device__ __forceinline__ VT operator()(int c) const { return w[min(max(c - c0, 0), width - 1)]; }
+};
+
+// entries of p_k the window of one CTA may hold (dynamic shared memory)
+constexpr int kCoopWindowBytes = 192 * 1024;
 
 template <typename VT>
 struct CoherentX {   // gathers of a vector that other CTAs of the launch write
@@ -91,9 +110,12 @@ struct SegCache {
 
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a, CoopArgs<VT> c) {
+    extern __shared__ __align__(16) unsigned char coop_smem[];
+    VT* const win = reinterpret_cast<VT*>(coop_smem);
     __shared__ VT red[2 * (kCoopThreads / 32)];
     __shared__ SegCache segs[kCoopMaxSegs];
     __shared__ int nseg_s;
+    __shared__ int win_lo, win_hi, win_sys;
     VT* const parts2[2] = {a.part1, a.part2};
     VT* const parts1[1] = {a.part1};
     const VT tol = static_cast<VT>(a.tol);
@@ -108,6 +130,40 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
         segs[threadIdx.x] = SegCache{g.s, seg, g.sr0, g.r0, g.r1, a.sys_seg0[g.s]};
     }
     __syncthreads();
+    // the column window of this CTA's rows (CSR patterns whose CTA rows lie in
+    // one system); win_sys < 0: gather from global memory
+    if (threadIdx.x == 0) {
+        // the window holds the CTA's own rows (whose p_k the product emits)
+        // and every column its rows reference
+        win_lo = nseg > 0 ? segs[0].r0 : 0;
+        win_hi = nseg > 0 ? segs[nseg - 1].r1 - 1 : -1;
+        win_sys = (FMT == CMCG_CSR && nseg > 0 && nseg == a.cta_seg0[blockIdx.x + 1] - a.cta_seg0[blockIdx.x])
+                      ? segs[0].s : -1;
+        for (int k = 1; k < nseg; ++k)
+            if (segs[k].s != win_sys) win_sys = -1;
+    }
+    __syncthreads();
+    if (FMT == CMCG_CSR && win_sys >= 0) {
+        int lo = INT32_MAX, hi = -1;
+        for (int k = 0; k < nseg; ++k)
+            for (int e = __ldg(a.m.rp + segs[k].r0) + threadIdx.x; e < __ldg(a.m.rp + segs[k].r1); e += kCoopThreads) {
+                const int cidx = __ldg(a.m.ci + e);
+                lo = min(lo, cidx);
+                hi = max(hi, cidx);
+            }
+        atomicMin(&win_lo, lo);
+        atomicMax(&win_hi, hi);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int sr0 = a.row_off[win_sys], send = a.row_off[win_sys + 1];
+            const bool fits = win_hi >= win_lo && win_lo >= sr0 && win_hi < send &&
+                              static_cast<int64_t>(win_hi - win_lo + 1) * static_cast<int64_t>(sizeof(VT)) <= kCoopWindowBytes;
+            if (!fits) win_sys = -1;
+        }
+        __syncthreads();
+    }
+    const bool use_win = win_sys >= 0;
+    const int wlo = win_lo, whi = win_hi + 1;
 
 // loop over this CTA's (batch, segment) pairs: b_, g (SegCache), inst, pidx, vo
 #define CMCG_COOP_SEGMENTS                                                        \
@@ -212,6 +268,42 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
     VT* pcur = c.p_alt;
     for (int32_t loop = 0; *reinterpret_cast<volatile int32_t*>(a.active) > 0 && loop < a.loop_cap; ++loop) {
         // phase 1: p_k = z + beta p_{k-1}; q = A p_k; partial p_k.q
+        if (use_win) {
+            // one system: stage p_k over the window, then the product
+            for (int b_ = 0; b_ < a.ob; ++b_) {
+                const int inst = b_ * a.n_sys + win_sys;
+                const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+                const VT beta = ld_cg_scalar<VT>(a.st.beta + inst);
+                const bool running = ld_status(a.st.status + inst) == ST_RUNNING;
+                const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+                const VT* rv = a.r + vo;
+                const VT* pp = pprev + vo;
+                if (running) {
+                    for (int j = wlo + threadIdx.x; j < whi; j += kCoopThreads)
+                        win[j - wlo] = p_next(dinv ? __ldg(dinv + j) : VT(1), __ldcg(rv + j), __ldcg(pp + j), beta);
+                }
+                __syncthreads();
+                for (int k_ = 0; k_ < nseg; ++k_) {
+                    const SegCache g = segs[k_];
+                    const int pidx = b_ * a.n_seg + g.seg;
+                    VT acc[1] = {VT(0)};
+                    if (running) {
+                        VT* pc = pcur + vo;
+                        VT* q = a.q + vo;
+                        const auto A = inst_matrix<MT, FMT>(a.m, b_);
+                        cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, WindowX<VT>{win, wlo, whi - wlo},
+                                          [&](int row, VT v) {
+                                              const VT pk = win[row - wlo];
+                                              pc[row] = pk;
+                                              q[row] = v;
+                                              acc[0] += pk * v;
+                                          });
+                    }
+                    block_sum<VT, 1>(acc, red);
+                    if (threadIdx.x == 0) a.part1[pidx] = acc[0];
+                }
+            }
+        } else {
         CMCG_COOP_SEGMENTS {
             const VT beta = ld_cg_scalar<VT>(a.st.beta + inst);
             const int32_t st = ld_status(a.st.status + inst);
@@ -233,6 +325,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
             }
             block_sum<VT, 1>(acc, red);
             if (threadIdx.x == 0) a.part1[pidx] = acc[0];
+        }
         }
         if (!grid_barrier(c.sync, c.err, c.lim, epoch, [&] {
                 int32_t running = 0;
@@ -315,7 +408,9 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
 
 template <typename VT, typename MT, int FMT>
 cmcg_status coop_cg_occupancy(int* ctas_per_sm) {
-    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_coop_cg<VT, MT, FMT>, kCoopThreads, 0));
+    CMCG_CUDA(cudaFuncSetAttribute(k_coop_cg<VT, MT, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoopWindowBytes));
+    CMCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_coop_cg<VT, MT, FMT>, kCoopThreads,
+                                                            kCoopWindowBytes));
     return CMCG_OK;
 }
 
@@ -332,7 +427,7 @@ cmcg_status coop_cg_launch(const SolveArgs<VT, MT>& a, void* sync, int32_t* err,
     CoopArgs<VT> c{static_cast<GridSync*>(sync), err, n_inst, p_alt, lim};
     void* params[] = {&args, &c};
     CMCG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_coop_cg<VT, MT, FMT>), grid, kCoopThreads,
-                                          params, 0, st));
+                                          params, kCoopWindowBytes, st));
     return CMCG_OK;
 }
 

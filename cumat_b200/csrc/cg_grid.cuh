@@ -91,20 +91,23 @@ struct InstState {
 // system's conditioning (BF16 at a condition number of ~1e6) make the inner
 // recursion stagnate or diverge, and its residual may then never drop far
 // enough to trigger a replacement. A replacement is therefore also forced
-// after kStallFirst iterations in the first cycle, and later after 4 times the
+// after kStallFirst iterations in the first cycle (see below), and later after 4 times the
 // first cycle's length plus kStallPad, kept within [kStallMin, kStallFirst]. A
 // replacement whose true residual norm fell by less than 10 % is a stall;
 // kStallMax stalls in a row stop the system with CMCG_SOLVE_BREAKDOWN. (A
 // healthy FP32 cycle at condition 1e8 still cuts the residual by more than
 // half in kStallFirst iterations.)
+// With a coarse replacement threshold (delta >= 0.05, the BF16 default, whose
+// cycles are short) the first cycle is forced after kStallMin iterations.
 constexpr int kStallFirst = 4096;
 constexpr int kStallMin = 1024;
 constexpr int kStallPad = 256;
 constexpr int kStallMax = 3;
 constexpr double kStallRatio = 0.81;   // |r|^2 ratio of a 10 % norm drop
-__host__ __device__ __forceinline__ int stall_len(int replacements, int cyc0) {
+__host__ __device__ __forceinline__ int stall_len(int replacements, int cyc0, float delta) {
     const int l = 4 * cyc0 + kStallPad;
-    return replacements == 0 ? kStallFirst : (l < kStallMin ? kStallMin : (l > kStallFirst ? kStallFirst : l));
+    if (replacements == 0) return delta >= 0.05f ? kStallMin : kStallFirst;
+    return l < kStallMin ? kStallMin : (l > kStallFirst ? kStallFirst : l);
 }
 
 template <typename VT, typename MT>

@@ -2,6 +2,8 @@
 // diagonal layout (one 1024-thread CTA per system instance, reliable updates).
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "cg_compact.cuh"
 #include "objects.h"
 
@@ -206,12 +208,15 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
         else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
         else if (!(rz > 0.0f)) status = CMCG_SOLVE_BREAKDOWN;
         const int64_t maxit = sys_max_iter(a.max_inner, n);
-        // progress guard (stall_len) in shared memory, so that the iteration
-        // loop keeps its registers: guard[0] = iteration that forces the next
-        // replacement, [1] = first cycle's length, [2] = stalls in a row;
-        // written by thread 0 inside a replacement, between barriers
-        if (tid == 0) {
-            guard[0] = kStallFirst;
+        // progress guard (stall_len), for BF16 inner values (FP32 values keep
+        // the unguarded loop; their cycles stall only past condition ~1e7), in
+        // shared memory, so that the iteration loop keeps its registers:
+        // guard[0] = iteration that forces the next replacement, [1] = first
+        // cycle's length, [2] = stalls in a row; written by thread 0 inside a
+        // replacement, between barriers
+        constexpr bool kGuard = std::is_same<MI, __nv_bfloat16>::value;
+        if (kGuard && tid == 0) {
+            guard[0] = stall_len(0, 0, a.delta);
             guard[1] = 0;
             guard[2] = 0;
         }
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
             // replace the residual when it dropped by delta, or when it suggests
             // that the FP64 residual may have reached the target, or when the
             // cycle has run too long (progress guard)
-            if (rzn < d2 * rmax || rzn < goal || it >= guard[0]) {
+            if (rzn < d2 * rmax || rzn < goal || (kGuard && it >= guard[0])) {
                 if (ND > 0 && pend) {
                     CMCG_DIA_SLOTS(nk, (dia_xinc<NK, T>(P, XH, tid, alpha_pend)))
                     pend = false;
@@ -306,13 +311,16 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
                 ++updates;
                 folded = true;
                 // (every thread has read guard[] for this iteration: block_sum synchronised)
-                const int stalls = t2[0] > kStallRatio * rr64 ? guard[2] + 1 : 0;
-                const int cyc0 = updates == 1 ? it : guard[1];
-                __syncthreads();
-                if (tid == 0) {
-                    guard[0] = it + stall_len(updates, cyc0);
-                    guard[1] = cyc0;
-                    guard[2] = stalls;
+                int stalls = 0;
+                if constexpr (kGuard) {
+                    stalls = t2[0] > kStallRatio * rr64 ? guard[2] + 1 : 0;
+                    const int cyc0 = updates == 1 ? it : guard[1];
+                    __syncthreads();
+                    if (tid == 0) {
+                        guard[0] = it + stall_len(updates, cyc0, a.delta);
+                        guard[1] = cyc0;
+                        guard[2] = stalls;
+                    }
                 }
                 rr64 = t2[0];
                 rzn = static_cast<float>(t2[1]);
@@ -320,7 +328,7 @@ __global__ void __launch_bounds__(T, kDiaBlockRows / T) k_mixed_fast(MixArgs<MI,
                 goal = static_cast<float>(thr / rr64) * rmax;
                 if (!finite_(rr64)) { status = CMCG_SOLVE_NON_FINITE; break; }
                 if (rr64 < thr) { status = CMCG_SOLVE_CONVERGED; break; }
-                if (stalls >= kStallMax) { status = CMCG_SOLVE_BREAKDOWN; break; }
+                if (kGuard && stalls >= kStallMax) { status = CMCG_SOLVE_BREAKDOWN; break; }
             }
             if (!(rzn > 0.0f)) { status = CMCG_SOLVE_BREAKDOWN; break; }
             const float beta = rzn / rz;

@@ -149,3 +149,40 @@ def test_adjoint_config5_shape_vs_sparse_fd(cuda):
             E = sp.csr_matrix(([h], ([r], [ci[kk]])), shape=(n, n)).tocsc()
             fd = (L(spl.spsolve(A + E, bs)) - L(spl.spsolve(A - E, bs))) / (2 * h)
             assert abs(fd - gA[k0 + kk]) <= 1e-6 * gscale
+
+
+def test_autograd_broadcast_and_interleaved_forwards(cuda):
+    # batched values with a one-batch b: the gradient of b sums over the
+    # batches and has b's shape; two forwards on the same op before the first
+    # backward: each backward uses its own forward's values
+    from cumat_b200.autograd import SparseSolveOp, sparse_solve
+    bt = P.fv2d_batch(2, 6, 8, 0.5, 9, with_xstar=True)
+    op = SparseSolveOp(bt.n, bt.row_ptr, bt.col, bt.row_off)
+    v0 = bt.val.astype(np.float64)
+    vals = torch.from_numpy(np.stack([v0, 1.5 * v0])).to(cuda).requires_grad_(True)
+    b = torch.from_numpy(bt.b.astype(np.float64)).to(cuda).requires_grad_(True)
+    x = sparse_solve(vals, b, op)
+    assert x.shape == (2, bt.n)
+    (0.5 * (x ** 2).sum()).backward()
+    assert b.grad.shape == b.shape and vals.grad.shape == vals.shape
+    # per batch: dL/db_k = A_k^{-T} x_k, summed over the batches
+    gb = np.zeros(bt.n)
+    for k, scale in enumerate((1.0, 1.5)):
+        for s in range(bt.n_sys):
+            r0, r1 = bt.row_off[s], bt.row_off[s + 1]
+            A, _, _ = _dense(bt, s)
+            xk = np.linalg.solve(scale * A, bt.b[r0:r1].astype(np.float64))
+            gb[r0:r1] += np.linalg.solve(scale * A.T, xk)
+    assert np.allclose(b.grad.cpu().numpy(), gb, rtol=1e-8, atol=1e-12)
+    # interleaved forwards
+    va = torch.from_numpy(v0).to(cuda).requires_grad_(True)
+    vb = torch.from_numpy(2.0 * v0).to(cuda).requires_grad_(True)
+    bb = torch.from_numpy(bt.b.astype(np.float64)).to(cuda)
+    xa = sparse_solve(va, bb, op)
+    xb = sparse_solve(vb, bb, op)
+    (0.5 * (xa ** 2).sum()).backward()
+    (0.5 * (xb ** 2).sum()).backward()
+    # A x = b with A scaled by 2: x halves, dL/dA = -lambda x^T with lambda = A^-T x
+    # scales by 1/8; the two gradients keep that ratio only if each backward
+    # used its own forward's values
+    assert np.allclose(vb.grad.cpu().numpy(), va.grad.cpu().numpy() / 8.0, rtol=1e-7, atol=1e-14)
