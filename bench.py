@@ -435,9 +435,29 @@ def cg_config2(cm, torch, dev, stream, hbm_peak):
     it = cg.iterations()
     per_iter = pr.nnz * 8 + (pr.n + 1) * 4 + 13 * pr.n * 4
     gbs = per_iter * it / (ms / 1e3) / 1e9
-    return {"ms": round(ms, 3), "iterations": int(it), "error": cg.error(),
-            "iters_per_s": round(it / (ms / 1e3), 1), "us_per_iter": round(ms * 1e3 / it, 2),
-            "gbs_model": round(gbs, 1), "frac_model": round(gbs / hbm_peak, 3)}
+    out = {"ms": round(ms, 3), "iterations": int(it), "error": cg.error(),
+           "iters_per_s": round(it / (ms / 1e3), 1), "us_per_iter": round(ms * 1e3 / it, 2),
+           "gbs_model": round(gbs, 1), "frac_model": round(gbs / hbm_peak, 3)}
+    # the other grid-path loop on the same system: the cooperative one-launch
+    # solve (one CTA per SM, p staged per CTA in shared memory), which the
+    # solver picks for systems up to 2^19 rows (CUMAT_CG_COOP=2 forces it)
+    old = os.environ.get("CUMAT_CG_COOP")
+    os.environ["CUMAT_CG_COOP"] = "2"
+    try:
+        cgc = cm.ConjugateGradient(A).setTolerance(1e-6).setMaxIterations(4000)
+    finally:
+        if old is None:
+            del os.environ["CUMAT_CG_COOP"]
+        else:
+            os.environ["CUMAT_CG_COOP"] = old
+    before = cm.launch_count()
+    cgc.solve(b, out=x)
+    launches = cm.launch_count() - before
+    msc = _ev_time(torch, stream, lambda: cgc.solve(b, out=x), 3)
+    itc = cgc.iterations()
+    out["cooperative"] = {"ms": round(msc, 3), "iterations": int(itc), "error": cgc.error(),
+                          "us_per_iter": round(msc * 1e3 / itc, 2), "launches_per_solve": int(launches)}
+    return out
 
 
 def cg_poisson10000(cm, torch, dev, stream, hbm_peak):
@@ -852,7 +872,7 @@ def run_profile_case(case: str):
     """Small single-purpose workloads for one-kernel ncu captures (each well
     above L2 in its streamed data, a few GB on the device at most):
 
-    grid3d      the 128^3 3D system (kappa = exp(N(0, 1)), seed 3) on the grid
+    grid3d      the 160^3 3D system (kappa = exp(N(0, 1)), seed 3) on the grid
                 path: plain FP64 Jacobi-CG and the mixed FP32 / FP64 solve,
                 each capped at 20 inner iterations (k_grid_*, k_gmix_*)
     plain_dia   plain FP64 batched CG of the first 512 systems of the batch
@@ -862,7 +882,14 @@ def run_profile_case(case: str):
                 k_sddmm_csr on the 8192^2 Poisson pattern)
     spmv_big    CSR and ELLPACK products on the 8192^2 Poisson matrix (3 each)
     cg10000     three grid-path Jacobi-CG iterations on the 10000^2 Poisson
-                matrix (FP32, diagonal layout: the fused product + p.q kernel)
+                matrix (FP32, diagonal layout: the fused product + p.q kernel;
+                about 10 GB on the device: launch lists only)
+    cg4096      the same on the 4096^2 Poisson matrix (16.8 M rows, 1.2 GB
+                streamed per iteration), for full captures
+    c4          the 256^3 precision system: 12 plain FP64 Jacobi-CG iterations
+                and 12 inner iterations of the mixed FP32 / FP64 solve (one
+                launch per kernel under CUMAT_CG_GRAPH=0: the per-kernel share
+                of an iteration in a launch list)
     """
     import torch
 
@@ -872,7 +899,7 @@ def run_profile_case(case: str):
     dev = torch.device("cuda", 0)
     out = {"profile_case": case}
     if case == "grid3d":
-        p3 = P.fv3d(128, 1.0, 3)
+        p3 = P.fv3d(160, 1.0, 3)
         pat = cm.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
         A64 = cm.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
         A32 = cm.SparseMatrix(pat, dtype=torch.float32).setData(p3.val)
@@ -882,8 +909,19 @@ def run_profile_case(case: str):
         cgm = cm.ConjugateGradient(A32).setTolerance(1e-4).setMaxIterations(20).set_path(2)
         cgm.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=3)
         out.update(rows=p3.n, nnz=p3.nnz)
-    elif case == "cg10000":
-        pr = P.poisson2d(10000, 1)
+    elif case == "c4":
+        p3 = P.fv3d(256, 1.0, 3)
+        pat = cm.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+        A64 = cm.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
+        A32 = cm.SparseMatrix(pat, dtype=torch.float32).setData(p3.val)
+        b64 = torch.from_numpy(p3.b.astype(np.float64)).to(dev)
+        out.update(rows=p3.n, nnz=p3.nnz)
+        del p3
+        cm.ConjugateGradient(A64).setTolerance(1e-10).setMaxIterations(12).set_path(2).solve(b64)
+        cgm = cm.ConjugateGradient(A32).setTolerance(1e-4).setMaxIterations(12).set_path(2)
+        cgm.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=3)
+    elif case in ("cg10000", "cg4096"):
+        pr = P.poisson2d(10000 if case == "cg10000" else 4096, 1)
         A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
         b = torch.from_numpy(pr.b).to(dev)
         cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(3).set_path(2).solve(b)
@@ -947,7 +985,7 @@ def main():
                     help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "
                          "mixed and FP64 solvers on the first 512 systems of the batch")
     ap.add_argument("--profile-case", default=None,
-                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big, cg10000)")
+                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big, cg10000, cg4096, c4)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -856,6 +856,47 @@ __global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __r
 // Diagonal-layout products of the grid path (stencil-shaped CSR patterns)
 // ---------------------------------------------------------------------------
 
+// The four values of a diagonal for four consecutive rows, loaded as streaming
+// data (ld.global.cs: evict-first in L1 and L2). A grid-path product reads each
+// value once per iteration while the p entries it gathers at offsets of up to
+// a grid plane are read again by later rows; evicting the values first keeps
+// those p entries in L2 on systems whose vectors exceed it.
+__device__ __forceinline__ void load_stream(Vals4<float>& w, const float* p) {
+    const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+    w.v[0] = t.x; w.v[1] = t.y; w.v[2] = t.z; w.v[3] = t.w;
+}
+__device__ __forceinline__ void load_stream(Vals4<double>& w, const double* p) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+    w.v[0] = a.x; w.v[1] = a.y; w.v[2] = b.x; w.v[3] = b.y;
+}
+__device__ __forceinline__ void load_stream(Vals4<__nv_bfloat16>& w, const __nv_bfloat16* p) {
+    const uint2 t = __ldcs(reinterpret_cast<const uint2*>(p));
+    const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&t.x);
+    const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&t.y);
+    w.v[0] = a.x; w.v[1] = a.y; w.v[2] = b.x; w.v[3] = b.y;
+}
+
+// p[c .. c + 3] with each index clamped into [lo, hi]: one or two 16-byte loads
+// where the four entries lie inside and start on a 16-byte boundary, else four
+// clamped scalar loads (the same entries either way).
+template <typename VT>
+__device__ __forceinline__ void p_quad(const VT* __restrict__ p, int c, int lo, int hi, VT (&o)[4]) {
+    if (c >= lo && c + 3 <= hi && (reinterpret_cast<uintptr_t>(p + c) & 15) == 0) {
+        if constexpr (sizeof(VT) == 4) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(p + c));
+            o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+        } else {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(p + c));
+            const double2 b = __ldg(reinterpret_cast<const double2*>(p + c) + 1);
+            o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) o[q] = __ldg(p + min(max(c + q, lo), hi));
+    }
+}
+
 // q[i] = sum_d v_d[i] p[i + off_d] for the rows [r0, r1) of one system (global
 // rows sr0 .. send - 1, r0 - sr0 a multiple of 4; v points at the system's
 // first value), diagonals in ascending offset order, the row's CSR order, with
@@ -864,30 +905,57 @@ __global__ void k_scale_sell(const int32_t* __restrict__ col, const int64_t* __r
 // r0 + 4 t + 3, then r0 + 4 (t + kTile) ..., the rows the sliced path gives
 // it, and emits them in the same order, so partial sums over the emitted
 // rows match too; the values of a diagonal for its four rows are one 16-byte
-// (8-byte for BF16) load. p indices are clamped into the system, where a zero
-// value (or, past the system's end, a row that is not emitted) meets them.
+// (8-byte for BF16) streaming load. p indices are clamped into the system,
+// where a zero value (or, past the system's end, a row that is not emitted)
+// meets them. The gathers: a thread loads its own four p entries (offset 0)
+// as one quad; offsets -1 and +1 take three of them and one entry from the
+// neighbouring lane (a scalar load at the warp's edges); other offsets load a
+// quad each. The entries are the clamped ones in every case, so the sums do
+// not depend on how they were loaded.
 // UNIT: the middle diagonal is offset 0 with every value 1 and is not loaded.
 // emit(global row, value).
 template <typename VT, typename MT, int ND, bool UNIT, typename F>
 __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int (&off)[ND], int sr0, int send, int r0,
                                              int r1, const VT* __restrict__ p, F&& emit) {
-    for (int ib = r0 + 4 * threadIdx.x; ib < r1; ib += 4 * kTile) {
+    const int lane = threadIdx.x & 31;
+    // the loop bound is the same for the whole CTA, so every lane takes part
+    // in the shuffles
+    for (int base = r0; base < r1; base += 4 * kTile) {
+        const int ib = base + 4 * threadIdx.x;
+        VT own[4];
+        p_quad(p, ib, sr0, send - 1, own);   // (ib >= sr0: only the upper clamp acts)
+        const VT from_prev = __shfl_up_sync(FULL, own[3], 1);     // p[ib - 1] of lane - 1's quad
+        const VT from_next = __shfl_down_sync(FULL, own[0], 1);   // p[ib + 4] of lane + 1's quad
+        if (ib >= r1) continue;
         const int li = ib - sr0;
         const MT* vr = v + (static_cast<int64_t>(li / kDiaBlockRows) * ND * kDiaBlockRows) + li % kDiaBlockRows;
         VT acc[4] = {VT(0), VT(0), VT(0), VT(0)};
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
+            const int o = off[d];
+            VT pv[4];
+            if (o == 0) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pv[q] = own[q];
+            } else if (o == -1) {
+                // lane >= 1: lane - 1's quad starts at ib - 4 >= r0, so its last
+                // entry is p[ib - 1] itself
+                pv[0] = lane ? from_prev : __ldg(p + max(ib - 1, sr0));
+                pv[1] = own[0]; pv[2] = own[1]; pv[3] = own[2];
+            } else if (o == 1) {
+                pv[0] = own[1]; pv[1] = own[2]; pv[2] = own[3];
+                pv[3] = lane != 31 ? from_next : __ldg(p + min(ib + 4, send - 1));
+            } else {
+                p_quad(p, ib + o, sr0, send - 1, pv);
+            }
             if (UNIT && d == ND / 2) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(VT(1), p[min(ib + q, send - 1)], acc[q]);
+                for (int q = 0; q < 4; ++q) acc[q] = fma(VT(1), pv[q], acc[q]);
             } else {
                 Vals4<MT> w;
-                w.load(vr + d * kDiaBlockRows);
+                load_stream(w, vr + d * kDiaBlockRows);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int c = min(max(ib + q + off[d], sr0), send - 1);
-                    acc[q] = fma(mval<VT>(w.v[q]), p[c], acc[q]);
-                }
+                for (int q = 0; q < 4; ++q) acc[q] = fma(mval<VT>(w.v[q]), pv[q], acc[q]);
             }
         }
 #pragma unroll
@@ -924,7 +992,7 @@ __global__ void k_dia_gather(const int32_t* __restrict__ pos, int64_t nnz, const
 
 // init A: x = guess or 0, r = b - A x, |b|^2, |r|^2 -> status
 template <typename VT, typename MT, int FMT>
-__global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
     CMCG_FOR_SEGMENTS(a) {
@@ -977,7 +1045,7 @@ __global__ void __launch_bounds__(kTile) k_grid_init(SolveArgs<VT, MT> a) {
 
 // init B: zero x of zero-rhs systems; p = M^-1 r and r.z of running systems
 template <typename VT, typename MT, int FMT>
-__global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
     CMCG_FOR_SEGMENTS(a) {
@@ -1020,7 +1088,7 @@ __global__ void __launch_bounds__(kTile) k_grid_init2(SolveArgs<VT, MT> a) {
 // iteration kernel 1: q = A p, p.q -> alpha (ND > 0: the values in the
 // pattern's diagonal layout, ND diagonals per system)
 template <typename VT, typename MT, int FMT, int ND = 0>
-__global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
     __shared__ VT red[kTile / 32];
     __shared__ bool last_s;
     CMCG_FOR_SEGMENTS(a) {
@@ -1031,7 +1099,7 @@ __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
         VT* q = a.q + vo;
         VT acc[1] = {VT(0)};
         const auto emit = [&](int row, VT v) {
-            q[row] = v;
+            __stcs(q + row, v);   // read once, by the update kernel
             acc[0] += p[row] * v;
         };
         if constexpr (ND > 0) {
@@ -1064,7 +1132,7 @@ __global__ void __launch_bounds__(kTile) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
 
 // iteration kernel 2: x += alpha p, r -= alpha q, |r|^2, r.z -> convergence, beta
 template <typename VT, typename MT, int FMT>
-__global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_update(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
     __shared__ bool last_s;
     CMCG_FOR_SEGMENTS(a) {
@@ -1140,7 +1208,7 @@ __global__ void __launch_bounds__(kTile) k_grid_update(SolveArgs<VT, MT> a) {
 
 // iteration kernel 3: p = M^-1 r + beta p
 template <typename VT, typename MT, int FMT>
-__global__ void __launch_bounds__(kTile) k_grid_pupdate(SolveArgs<VT, MT> a) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_pupdate(SolveArgs<VT, MT> a) {
     CMCG_FOR_SEGMENTS(a) {
         const SegInfo g = seg_info(a, b_, seg_);
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
@@ -1198,7 +1266,7 @@ struct GMixArgs {
 };
 
 template <typename MI, typename MO>
-__global__ void __launch_bounds__(kTile) k_gmix_init(GMixArgs<MI, MO> m) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_init(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     __shared__ double red[2 * (kTile / 32)];
     __shared__ bool last_s;
@@ -1260,7 +1328,7 @@ __device__ __forceinline__ bool gmix_tail_status(int32_t st) {
 // pattern's diagonal layout, the unit middle diagonal not loaded where the
 // system's flag says so)
 template <typename MI, typename MO, int ND = 0>
-__global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_spmv(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     __shared__ float red[kTile / 32];
     __shared__ bool last_s;
@@ -1272,7 +1340,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
         float* q = a.q + vo;
         float acc[1] = {0.0f};
         const auto emit = [&](int row, float v) {
-            q[row] = v;
+            __stcs(q + row, v);   // read once, by the update kernel
             acc[0] += p[row] * v;
         };
         if constexpr (ND > 0) {
@@ -1307,7 +1375,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_spmv(GMixArgs<MI, MO> m) {
 
 // xh += alpha p, r -= alpha q, |r|^2 -> replacement decision or beta
 template <typename MI, typename MO>
-__global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_update(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     __shared__ float red[kTile / 32];
     __shared__ bool last_s;
@@ -1375,7 +1443,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_update(GMixArgs<MI, MO> m) {
 
 // x += S xh where a replacement is due (TAIL: where the solve stopped unfolded)
 template <typename MI, typename MO, bool TAIL>
-__global__ void __launch_bounds__(kTile) k_gmix_fold(GMixArgs<MI, MO> m) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_fold(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     CMCG_FOR_SEGMENTS(a) {
         const SegInfo g = seg_info(a, b_, seg_);
@@ -1394,7 +1462,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_fold(GMixArgs<MI, MO> m) {
 // r = S (b - A x) in FP64 where a replacement is due -> convergence, beta
 // (TAIL: only the final |b - A x|^2 of the instances folded by the tail)
 template <typename MI, typename MO, bool TAIL>
-__global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_residual(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     __shared__ double red[2 * (kTile / 32)];
     __shared__ bool last_s;
@@ -1457,7 +1525,7 @@ __global__ void __launch_bounds__(kTile) k_gmix_residual(GMixArgs<MI, MO> m) {
 
 // p = r + beta p
 template <typename MI, typename MO>
-__global__ void __launch_bounds__(kTile) k_gmix_pupdate(GMixArgs<MI, MO> m) {
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_pupdate(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     CMCG_FOR_SEGMENTS(a) {
         const SegInfo g = seg_info(a, b_, seg_);
@@ -1494,6 +1562,30 @@ __global__ void k_finalize(InstState st, int32_t n_inst) {
     int32_t s = st.status[i];
     if (s == ST_RUNNING) { s = CMCG_SOLVE_MAX_ITER; st.status[i] = s; }
     st.err[i] = (s == CMCG_SOLVE_ZERO_RHS) ? 0.0 : sqrt(st.rr[i] / st.bb[i]);
+}
+
+// The grid path's iteration loop without a graph: `body` launches one
+// iteration's kernels on `st`; the count of running instances is read back
+// every kHostLoopPoll iterations and the loop ends at 0 or after cap - 1
+// iterations, as the graph's WHILE node does (k_grid_cond). Iterations run
+// after the last instance finished change nothing: the kernels skip finished
+// instances.
+constexpr int32_t kHostLoopPoll = 16;
+template <typename F>
+cmcg_status host_loop(cudaStream_t st, const int32_t* active, int32_t cap, int per_iter, F&& body) {
+    for (int32_t l = 1;; ++l) {
+        body();
+        count_launch(per_iter);
+        CMCG_CHECK_LAUNCH();
+        if (l >= cap) break;
+        if (l % kHostLoopPoll == 0) {
+            int32_t running = 0;
+            CMCG_CUDA(cudaMemcpyAsync(&running, active, sizeof(running), cudaMemcpyDeviceToHost, st));
+            CMCG_CUDA(cudaStreamSynchronize(st));
+            if (running <= 0) break;
+        }
+    }
+    return CMCG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1557,7 +1649,14 @@ struct cmcg_solver_s {
     bool use_smem = true;     // shared-memory-resident kernels where the systems fit
     bool inner_solve = false; // set while the solver runs the inner solves of a refinement
     bool fast_kernels = true; // compact-layout kernels where available (CUMAT_CG_FAST=0 disables)
-    bool coop = true;         // cooperative one-launch grid solve where it applies (CUMAT_CG_COOP=0 disables)
+    // cooperative one-launch grid solve: 0 never, 1 where it applies (systems up
+    // to kCoopMaxRows rows), 2 also for larger systems (CUMAT_CG_COOP)
+    int coop = 1;
+    // grid path iteration loop: true = one CUDA graph with a device-side WHILE
+    // node; false = the same kernels launched from the host, polling the count
+    // of running instances (CUMAT_CG_GRAPH=0; kernel profilers do not replay
+    // kernels inside conditional graph nodes)
+    bool graph_loop = true;
     int64_t systems_version = -1;  // pattern systems the plan was built for
     // plan
     int32_t n_sys = 0, max_sys_rows = 0, n_tiles = 0;
@@ -2233,6 +2332,20 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     count_launch(2);
     CMCG_CHECK_LAUNCH();
 
+    if (!s->graph_loop) {
+        return host_loop(st, a.active, a.loop_cap, 3, [&] {
+            if constexpr (FMT == CMCG_CSR) {
+                if (nd == 5) k_grid_spmv_pq<VT, MT, FMT, 5><<<grid, kTile, 0, st>>>(a);
+                else if (nd == 7) k_grid_spmv_pq<VT, MT, FMT, 7><<<grid, kTile, 0, st>>>(a);
+                else k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+            } else {
+                k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+            }
+            k_grid_update<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+            k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+        });
+    }
+
     // graph with a WHILE node over the three iteration kernels; rebuilt when any
     // kernel argument changes
     std::vector<char> key(sizeof(a) + sizeof(int) * 2);
@@ -2297,11 +2410,15 @@ cmcg_status run_coop(cmcg_solver s, SolveArgs<VT, MT>& a, VT* p_alt, bool* done)
     if (!s->coop || n_inst > kCoopMaxInst || s->coop_ctas < 1 || s->coop_max_segs > kCoopMaxSegs) return CMCG_OK;
     // systems large enough to hide the graph's per-kernel launches run faster
     // on the graph kernels (more threads per SM in flight)
-    if (s->max_sys_rows > kCoopMaxRows) return CMCG_OK;
+    if (s->max_sys_rows > kCoopMaxRows && s->coop < 2) return CMCG_OK;
     int coop_attr = 0, occ = 0;
     CMCG_CUDA(cudaDeviceGetAttribute(&coop_attr, cudaDevAttrCooperativeLaunch, ctx->device));
     CMCG_TRY((coop_cg_occupancy<VT, MT, FMT>(&occ)));
-    if (!coop_attr || occ * ctx->sm_count < s->coop_ctas) return CMCG_OK;
+    if (!coop_attr || occ * ctx->sm_count < s->coop_ctas) {
+        if (log_on(1))
+            log_msg(1, "cooperative solve not launched: %d CTAs per SM resident, %d CTAs needed", occ, s->coop_ctas);
+        return CMCG_OK;
+    }
     // the cooperative launch has its own segment plan (one CTA per SM)
     SolveArgs<VT, MT> c = a;
     c.n_seg = s->coop_n_seg;
@@ -2732,49 +2849,61 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     k_gmix_init<MI, MO><<<grid, kTile, 0, st>>>(m);
     count_launch();
     CMCG_CHECK_LAUNCH();
-    std::vector<char> key(sizeof(m) + sizeof(int) * 2);
-    {
-        GMixArgs<MI, MO> k = m;
-        k.g.cond = 0;
-        std::memcpy(key.data(), &k, sizeof(k));
-        const int ids[2] = {DT<MI>::id, DT<MO>::id};
-        std::memcpy(key.data() + sizeof(k), ids, sizeof(ids));
+    if (!s->graph_loop) {
+        CMCG_TRY(host_loop(st, m.g.active, m.g.loop_cap, 5, [&] {
+            if (nd == 5) k_gmix_spmv<MI, MO, 5><<<grid, kTile, 0, st>>>(m);
+            else if (nd == 7) k_gmix_spmv<MI, MO, 7><<<grid, kTile, 0, st>>>(m);
+            else k_gmix_spmv<MI, MO><<<grid, kTile, 0, st>>>(m);
+            k_gmix_update<MI, MO><<<grid, kTile, 0, st>>>(m);
+            k_gmix_fold<MI, MO, false><<<grid, kTile, 0, st>>>(m);
+            k_gmix_residual<MI, MO, false><<<grid, kTile, 0, st>>>(m);
+            k_gmix_pupdate<MI, MO><<<grid, kTile, 0, st>>>(m);
+        }));
+    } else {
+        std::vector<char> key(sizeof(m) + sizeof(int) * 2);
+        {
+            GMixArgs<MI, MO> k = m;
+            k.g.cond = 0;
+            std::memcpy(key.data(), &k, sizeof(k));
+            const int ids[2] = {DT<MI>::id, DT<MO>::id};
+            std::memcpy(key.data() + sizeof(k), ids, sizeof(ids));
+        }
+        if (!s->gexec_mix || key != s->gkey_mix) {
+            if (s->gexec_mix) { cudaGraphExecDestroy(s->gexec_mix); s->gexec_mix = nullptr; }
+            if (s->graph_mix) { cudaGraphDestroy(s->graph_mix); s->graph_mix = nullptr; }
+            cudaGraph_t g;
+            CMCG_CUDA(cudaGraphCreate(&g, 0));
+            s->graph_mix = g;
+            cudaGraphConditionalHandle h;
+            CMCG_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            CMCG_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            m.g.cond = h;
+            if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
+            cudaStream_t cs = ctx->capture_stream;
+            CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            if (nd == 5) k_gmix_spmv<MI, MO, 5><<<grid, kTile, 0, cs>>>(m);
+            else if (nd == 7) k_gmix_spmv<MI, MO, 7><<<grid, kTile, 0, cs>>>(m);
+            else k_gmix_spmv<MI, MO><<<grid, kTile, 0, cs>>>(m);
+            k_gmix_update<MI, MO><<<grid, kTile, 0, cs>>>(m);
+            k_gmix_fold<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
+            k_gmix_residual<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
+            k_gmix_pupdate<MI, MO><<<grid, kTile, 0, cs>>>(m);
+            k_grid_cond<<<1, 1, 0, cs>>>(m.g.active, m.g.loops, m.g.loop_cap, h);
+            cudaGraph_t captured = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+            if (ce != cudaSuccess) return cuda_fail(ce, "capture of the mixed CG iteration", __FILE__, __LINE__);
+            CMCG_CUDA(cudaGraphInstantiate(&s->gexec_mix, g, 0));
+            s->gkey_mix = key;
+        }
+        CMCG_CUDA(cudaGraphLaunch(s->gexec_mix, st));
     }
-    if (!s->gexec_mix || key != s->gkey_mix) {
-        if (s->gexec_mix) { cudaGraphExecDestroy(s->gexec_mix); s->gexec_mix = nullptr; }
-        if (s->graph_mix) { cudaGraphDestroy(s->graph_mix); s->graph_mix = nullptr; }
-        cudaGraph_t g;
-        CMCG_CUDA(cudaGraphCreate(&g, 0));
-        s->graph_mix = g;
-        cudaGraphConditionalHandle h;
-        CMCG_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        CMCG_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        m.g.cond = h;
-        if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
-        cudaStream_t cs = ctx->capture_stream;
-        CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        if (nd == 5) k_gmix_spmv<MI, MO, 5><<<grid, kTile, 0, cs>>>(m);
-        else if (nd == 7) k_gmix_spmv<MI, MO, 7><<<grid, kTile, 0, cs>>>(m);
-        else k_gmix_spmv<MI, MO><<<grid, kTile, 0, cs>>>(m);
-        k_gmix_update<MI, MO><<<grid, kTile, 0, cs>>>(m);
-        k_gmix_fold<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
-        k_gmix_residual<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
-        k_gmix_pupdate<MI, MO><<<grid, kTile, 0, cs>>>(m);
-        k_grid_cond<<<1, 1, 0, cs>>>(m.g.active, m.g.loops, m.g.loop_cap, h);
-        cudaGraph_t captured = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(cs, &captured);
-        if (ce != cudaSuccess) return cuda_fail(ce, "capture of the mixed CG iteration", __FILE__, __LINE__);
-        CMCG_CUDA(cudaGraphInstantiate(&s->gexec_mix, g, 0));
-        s->gkey_mix = key;
-    }
-    CMCG_CUDA(cudaGraphLaunch(s->gexec_mix, st));
     k_gmix_fold<MI, MO, true><<<grid, kTile, 0, st>>>(m);
     k_gmix_residual<MI, MO, true><<<grid, kTile, 0, st>>>(m);
     k_finalize<<<(n_inst + 255) / 256, 256, 0, st>>>(s->st, n_inst);
@@ -2813,7 +2942,8 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     if (const char* e = std::getenv("CUMAT_CG_FAST")) s->fast_kernels = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_DIA")) s->dia_kernels = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_SMALL")) s->mix_small = std::atoi(e) != 0;
-    if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::atoi(e) != 0;
+    if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::max(0, std::min(2, std::atoi(e)));
+    if (const char* e = std::getenv("CUMAT_CG_GRAPH")) s->graph_loop = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_BF16_FALLBACK")) s->bf16_fallback = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);
     if (st == CMCG_OK) st = dev_alloc(reinterpret_cast<void**>(&s->counters), 64);

@@ -40,9 +40,11 @@ constexpr int kSpmvThreads = 256;
 
 // Stand-alone product kernels: 0 = row-unrolled CSR / four-rows-per-thread
 // ELLPACK, 1 = warp row-block CSR / thread-per-row ELLPACK, 2 = bulk-staged
-// CSR / four-rows-per-thread ELLPACK. CUMAT_SPMV_VARIANT forces one (a
-// comparison knob, read at each product); unset, each pattern picks by timing on
-// its first product (see launch_spmv).
+// CSR / four-rows-per-thread ELLPACK, 3 .. 6 = CSR with 4 .. 32 lanes per row,
+// 7 = CSR with four rows per thread and 16-byte chunks, 8 = CSR with
+// warp-staged entries. CUMAT_SPMV_VARIANT forces one (a comparison knob, read
+// at each product); unset, each pattern picks by timing on its first product
+// (see launch_spmv).
 int spmv_variant() {
     const char* e = std::getenv("CUMAT_SPMV_VARIANT");
     return e ? std::atoi(e) : -1;
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_rows(const int32_t* _
             }
 #pragma unroll
             for (int u = 0; u < kCsrUnroll; ++u)
-                if (c[u] >= 0) acc += mval<VT>(w[u]) * __ldg(xv + c[u]);
+                if (c[u] >= 0) acc = fma(mval<VT>(w[u]), __ldg(xv + c[u]), acc);
         }
         assign_out<MODE>(y + it, acc);
     }
@@ -180,6 +182,109 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_vec(const int32_t* __
 #pragma unroll
         for (int o = V / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
         if (sub == 0 && it < items) assign_out<MODE>(y + it, acc);
+    }
+}
+
+// ---- CSR, four consecutive rows per thread, 16-byte chunks ------------------------
+//
+// The four rows r .. r + 3 of a thread (r a multiple of 4) own one contiguous
+// entry range [rp[r], rp[r + 4]); the thread reads it in 4-entry chunks
+// aligned to 16 bytes (one int4 of column indices and one 16-byte load of
+// values, 8-byte for BF16; the padded index and value arrays keep the last
+// chunk in bounds), so neighbouring threads read neighbouring chunks and a
+// warp's loads are whole lines, as in the ELLPACK kernel. Each entry is added
+// to its row's sum in entry order, the same sums as thread per row.
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr4(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                            const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                            const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                            VT* __restrict__ y, int32_t rows, int32_t ob) {
+    const int64_t quads = (static_cast<int64_t>(rows) + 3) / 4;
+    const int64_t items = quads * ob;
+    for (int64_t it = static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x; it < items;
+         it += static_cast<int64_t>(gridDim.x) * kSpmvThreads) {
+        const int b = static_cast<int>(it / quads);
+        const int r = static_cast<int>(it - static_cast<int64_t>(b) * quads) * 4;
+        const MT* v = vals + (mb == 1 ? 0 : b * vstride);
+        const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        // row pointers of the four rows (padded with copies of nnz past the end)
+        const int4 bp = __ldg(reinterpret_cast<const int4*>(rp + r));
+        const int b4 = __ldg(rp + r + 4);
+        VT a0 = VT(0), a1 = VT(0), a2 = VT(0), a3 = VT(0);
+#pragma unroll 2
+        for (int k = bp.x & ~3; k < b4; k += 4) {
+            const int4 c = __ldg(reinterpret_cast<const int4*>(ci + k));
+            Vals4<MT> w;
+            w.load(v + k);
+            const int cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int kk = k + u;
+                if (kk < bp.x || kk >= b4) continue;
+                const VT t = mval<VT>(w.v[u]);
+                if (kk < bp.y) a0 += t * __ldg(xv + cc[u]);
+                else if (kk < bp.z) a1 += t * __ldg(xv + cc[u]);
+                else if (kk < bp.w) a2 += t * __ldg(xv + cc[u]);
+                else a3 += t * __ldg(xv + cc[u]);
+            }
+        }
+        VT* yv = y + static_cast<int64_t>(b) * rows + r;
+        if (r < rows) assign_out<MODE>(yv, a0);
+        if (r + 1 < rows) assign_out<MODE>(yv + 1, a1);
+        if (r + 2 < rows) assign_out<MODE>(yv + 2, a2);
+        if (r + 3 < rows) assign_out<MODE>(yv + 3, a3);
+    }
+}
+
+// ---- CSR, warp-staged entries ----------------------------------------------------
+//
+// A warp takes 32 consecutive rows, whose entries form one contiguous range. It
+// reads the range in rounds of kCsrStage entries with coalesced loads (lane l
+// takes entries l, l + 32, ...), converting each value to the vector type and
+// gathering its x into shared memory; lane l then adds up the staged entries
+// of row l in entry order with fused multiply-adds, which is the
+// thread-per-row kernel's sum bit for bit. Rows longer than a round carry
+// their sum into the next one.
+
+constexpr int kCsrStage = 256;   // entries per warp and round
+
+template <typename MT, typename VT, int MODE>
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_warp(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                                const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                                const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                                VT* __restrict__ y, int32_t rows, int32_t ob) {
+    __shared__ VT sw[kSpmvThreads / 32][kCsrStage];
+    __shared__ VT sx[kSpmvThreads / 32][kCsrStage];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t groups = (static_cast<int64_t>(rows) + 31) / 32;
+    const int64_t items = groups * ob;
+    const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * kSpmvThreads) >> 5;
+    // the loop bound is the warp's (uniform), so every lane reaches the
+    // shuffles and __syncwarp
+    for (int64_t w = (static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x) >> 5; w < items; w += nwarps) {
+        const int b = static_cast<int>(w / groups);
+        const int r0 = static_cast<int>(w - static_cast<int64_t>(b) * groups) * 32;
+        const int r = r0 + lane;
+        const MT* v = vals + (mb == 1 ? 0 : b * vstride);
+        const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+        const int a = r < rows ? __ldg(rp + r) : 0;
+        const int e = r < rows ? __ldg(rp + r + 1) : 0;
+        const int g0 = __shfl_sync(FULL, a, 0);
+        const int g1 = __shfl_sync(FULL, e, min(32, rows - r0) - 1);
+        VT acc = VT(0);
+        for (int cs = g0; cs < g1; cs += kCsrStage) {
+            const int ce = min(cs + kCsrStage, g1);
+            for (int k = cs + lane; k < ce; k += 32) {
+                sw[wib][k - cs] = mval<VT>(v[k]);
+                sx[wib][k - cs] = __ldg(xv + __ldg(ci + k));
+            }
+            __syncwarp();
+            const int lo = max(a, cs), hi = min(e, ce);
+            for (int k = lo; k < hi; ++k) acc = fma(sw[wib][k - cs], sx[wib][k - cs], acc);
+            __syncwarp();
+        }
+        if (r < rows) assign_out<MODE>(y + static_cast<int64_t>(b) * rows + r, acc);
     }
 }
 
@@ -518,6 +623,36 @@ cmcg_status launch_spmv_variant(cmcg_matrix A, const void* x, int32_t xb, void* 
         CMCG_CHECK_LAUNCH();
         return CMCG_OK;
     }
+    if (p->format == CMCG_CSR && variant == 7) {
+        const int64_t threads = (static_cast<int64_t>(p->rows) + 3) / 4 * ob;
+        const int needed = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
+#define CMCG_LAUNCH_CSR4(M)                                                                                    \
+    k_spmv_csr4<MT, VT, M><<<resident_grid(k_spmv_csr4<MT, VT, M>, needed, ctx->sm_count), kSpmvThreads, 0,      \
+                             ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride, A->batches, xv, p->cols, xb, yv, \
+                                            p->rows, ob)
+        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR4(CMCG_ASSIGN);
+        else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR4(CMCG_ADD);
+        else CMCG_LAUNCH_CSR4(CMCG_SUB);
+#undef CMCG_LAUNCH_CSR4
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        return CMCG_OK;
+    }
+    if (p->format == CMCG_CSR && variant == 8) {
+        const int64_t warps = (static_cast<int64_t>(p->rows) + 31) / 32 * ob;
+        const int needed = static_cast<int>(std::min<int64_t>((warps + kSpmvThreads / 32 - 1) / (kSpmvThreads / 32), max_blocks));
+#define CMCG_LAUNCH_CSR_WARP(M)                                                                                       \
+    k_spmv_csr_warp<MT, VT, M><<<resident_grid(k_spmv_csr_warp<MT, VT, M>, needed, ctx->sm_count), kSpmvThreads, 0,     \
+                                 ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride, A->batches, xv, p->cols, xb, yv, \
+                                                p->rows, ob)
+        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR_WARP(CMCG_ASSIGN);
+        else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR_WARP(CMCG_ADD);
+        else CMCG_LAUNCH_CSR_WARP(CMCG_SUB);
+#undef CMCG_LAUNCH_CSR_WARP
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+        return CMCG_OK;
+    }
     if (p->format == CMCG_CSR && variant == 0) {
         const int64_t threads = static_cast<int64_t>(p->rows) * ob;
         const int needed = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
@@ -585,10 +720,26 @@ __global__ void __launch_bounds__(kRedThreads) k_dot(int64_t n, const VT* __rest
     const int b = blockIdx.y;
     const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * n);
     const VT* yv = y + (yb == 1 ? 0 : static_cast<int64_t>(b) * n);
+    // four grid strides per pass: eight independent loads in flight per thread,
+    // summed into four accumulators that are added in a fixed order
     VT acc[1] = {VT(0)};
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kRedThreads + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * kRedThreads)
-        acc[0] += __ldg(xv + i) * __ldg(yv + i);
+    VT a4[4] = {VT(0), VT(0), VT(0), VT(0)};
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kRedThreads;
+    int64_t i = static_cast<int64_t>(blockIdx.x) * kRedThreads + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+        VT xs[4], ys[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            xs[j] = __ldg(xv + i + j * stride);
+            ys[j] = __ldg(yv + i + j * stride);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a4[j] += xs[j] * ys[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        if (i + j * stride < n) a4[j] += __ldg(xv + i + j * stride) * __ldg(yv + i + j * stride);
+    acc[0] = (a4[0] + a4[1]) + (a4[2] + a4[3]);
     block_sum<VT, 1>(acc, red);
     if (threadIdx.x == 0) {
         partial[static_cast<int64_t>(b) * gridDim.x + blockIdx.x] = acc[0];
@@ -609,11 +760,19 @@ __global__ void __launch_bounds__(kRedThreads) k_dot(int64_t n, const VT* __rest
     }
 }
 
+// CTAs per batch of the dot product: one per 4 x 256 x 4 entries (four
+// passes of four loads per thread), at most 8 per SM over all batches (a full
+// SM of 256-thread CTAs), at most `cap`
+int dot_grid(cmcg_ctx ctx, int64_t n, int32_t ob, int cap) {
+    const int64_t want = std::max<int64_t>(1, (n + kRedThreads * 16 - 1) / (kRedThreads * 16));
+    const int most = std::max(1, std::min(cap, (ctx->sm_count * 8) / std::max(1, ob) + 1));
+    return static_cast<int>(std::min<int64_t>(want, most));
+}
+
 template <typename VT>
 cmcg_status launch_dot(cmcg_ctx ctx, int64_t n, const void* x, int32_t xb, const void* y, int32_t yb, void* out,
                        int32_t ob) {
-    const int64_t want = std::max<int64_t>(1, (n + kRedThreads * 4 - 1) / (kRedThreads * 4));
-    const int gx = static_cast<int>(std::min<int64_t>(want, std::max(1, (ctx->sm_count * 4) / std::max(1, ob) + 1)));
+    const int gx = dot_grid(ctx, n, ob, INT32_MAX);
     CMCG_TRY(ensure_buffer(&ctx->red_partial, &ctx->red_partial_bytes, static_cast<size_t>(gx) * ob * sizeof(VT)));
     if (ctx->red_ticket_count < static_cast<size_t>(ob)) {
         dev_free(ctx->red_ticket);
@@ -634,37 +793,90 @@ cmcg_status launch_dot(cmcg_ctx ctx, int64_t n, const void* x, int32_t xb, const
 
 // ---- sampled outer product on the pattern -----------------------------------------
 
+// Sampled outer product on a CSR pattern, out_k = alpha * u[row(k)] * v[col(k)]
+// for every stored entry k. A CTA takes 1024 rows at a time (four per thread)
+// and walks their entries in windows of 2048: the thread of each non-empty
+// row marks the row's first entry in the window, an inclusive max-scan over
+// the window (threads scan 8 consecutive slots, then across the CTA) gives
+// every entry its row, and the entries are then read and written in order
+// (coalesced), each column index loaded once for all value batches. The work
+// per entry is a few instructions whatever the row lengths (a long row only
+// spans more windows). Slot k of the window sits at k + k / 32 in shared
+// memory, so that the scan's strided accesses hit 32 different banks.
+constexpr int kSdThreads = 256, kSdRowsPer = 4, kSdRows = kSdThreads * kSdRowsPer, kSdPer = 8,
+              kSdWin = kSdThreads * kSdPer;
+
+__device__ __forceinline__ int sd_slot(int k) { return k + (k >> 5); }
+
 template <typename VT>
-__global__ void k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, int32_t rows, int32_t cols,
-                            int64_t vstride, VT alpha, const VT* __restrict__ u, int32_t ub, const VT* __restrict__ v,
-                            int32_t vb, VT* __restrict__ out, int32_t ob) {
-    // warp per 32-row block: lane-parallel over the block's contiguous entries,
-    // row of an entry found by a short search over the block's row bounds
-    __shared__ int32_t bounds[8][33];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nblk = (rows + 31) >> 5;
-    const int64_t items = static_cast<int64_t>(nblk) * ob;
-    for (int64_t it = static_cast<int64_t>(blockIdx.x) * 8 + warp; it < items; it += static_cast<int64_t>(gridDim.x) * 8) {
-        const int b = static_cast<int>(it / nblk);
-        const int r0 = static_cast<int>(it - static_cast<int64_t>(b) * nblk) * 32;
-        const int nr = min(32, rows - r0);
-        // nr + 1 bounds (up to 33): lane j loads bound j, lane 0 also the last one
-        if (lane < nr) bounds[warp][lane] = __ldg(rp + r0 + lane);
-        if (lane == 0) bounds[warp][nr] = __ldg(rp + r0 + nr);
-        __syncwarp();
-        const int lo = bounds[warp][0], hi = bounds[warp][nr];
-        const VT* ub_ = u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows);
-        const VT* vb_ = v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols);
-        VT* ob_ = out + static_cast<int64_t>(b) * vstride;
-        for (int k = lo + lane; k < hi; k += 32) {
-            int a = 0, e = nr;  // find row j with bounds[j] <= k < bounds[j+1]
-            while (e - a > 1) {
-                const int m = (a + e) >> 1;
-                if (bounds[warp][m] <= k) a = m; else e = m;
-            }
-            ob_[k] = alpha * ub_[r0 + a] * vb_[__ldg(ci + k)];
+__global__ void __launch_bounds__(kSdThreads) k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                          int32_t rows, int32_t cols, int64_t vstride, VT alpha,
+                                                          const VT* __restrict__ u, int32_t ub,
+                                                          const VT* __restrict__ v, int32_t vb,
+                                                          VT* __restrict__ out, int32_t ob) {
+    __shared__ int32_t owner[kSdWin + kSdWin / 32];
+    __shared__ int32_t wmax[kSdThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int ntile = (rows + kSdRows - 1) / kSdRows;
+    for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int r0 = tile * kSdRows;
+        const int nr = min(kSdRows, rows - r0);
+        int my_lo[kSdRowsPer], my_hi[kSdRowsPer];
+#pragma unroll
+        for (int m = 0; m < kSdRowsPer; ++m) {   // rows r0 + t + 256 m (coalesced bounds)
+            const int lr = t + m * kSdThreads;
+            my_lo[m] = lr < nr ? __ldg(rp + r0 + lr) : 0;
+            my_hi[m] = lr < nr ? __ldg(rp + r0 + lr + 1) : 0;
         }
-        __syncwarp();
+        const int lo = __ldg(rp + r0), hi = __ldg(rp + r0 + nr);
+        int carry = -1;   // the row (in the tile) owning the window's first entry
+        for (int w0 = lo; w0 < hi; w0 += kSdWin) {
+            const int wn = min(kSdWin, hi - w0);
+#pragma unroll
+            for (int j = 0; j < kSdPer; ++j) owner[sd_slot(j * kSdThreads + t)] = -1;
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < kSdRowsPer; ++m)
+                if (my_hi[m] > my_lo[m] && my_lo[m] >= w0 && my_lo[m] < w0 + wn)
+                    owner[sd_slot(my_lo[m] - w0)] = t + m * kSdThreads;
+            __syncthreads();
+            int mark[kSdPer];
+            int m = -1;
+#pragma unroll
+            for (int j = 0; j < kSdPer; ++j) {
+                mark[j] = owner[sd_slot(t * kSdPer + j)];
+                m = max(m, mark[j]);
+            }
+            int wm = m;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, wm, o);
+                if (lane >= o) wm = max(wm, y);
+            }
+            if (lane == 31) wmax[warp] = wm;
+            const int ex = __shfl_up_sync(0xffffffffu, wm, 1);
+            __syncthreads();
+            int pre = max(carry, lane == 0 ? -1 : ex);
+            for (int w = 0; w < warp; ++w) pre = max(pre, wmax[w]);
+#pragma unroll
+            for (int j = 0; j < kSdPer; ++j) {
+                pre = max(pre, mark[j]);
+                owner[sd_slot(t * kSdPer + j)] = pre;
+            }
+            __syncthreads();
+            for (int j = t; j < wn; j += kSdThreads) {
+                const int64_t k = static_cast<int64_t>(w0) + j;
+                const int row = r0 + owner[sd_slot(j)];
+                const int c = __ldg(ci + k);
+                for (int b = 0; b < ob; ++b) {
+                    const VT uu = __ldg(u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows) + row);
+                    const VT vv = __ldg(v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols) + c);
+                    out[static_cast<int64_t>(b) * vstride + k] = alpha * uu * vv;
+                }
+            }
+            carry = owner[sd_slot(kSdWin - 1)];   // (read only when the window was full)
+            __syncthreads();
+        }
     }
 }
 
@@ -694,9 +906,9 @@ cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub,
     cmcg_pattern p = M->pat;
     cmcg_ctx ctx = p->ctx;
     if (p->format == CMCG_CSR) {
-        const int64_t warps = static_cast<int64_t>((p->rows + 31) / 32) * ob;
-        const int blocks = static_cast<int>(std::min<int64_t>((warps + 7) / 8, ctx->sm_count * 8));
-        k_sddmm_csr<VT><<<blocks, 256, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, p->rows, p->cols, p->nnz,
+        const int64_t tiles = (static_cast<int64_t>(p->rows) + kSdRows - 1) / kSdRows;
+        const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, ctx->sm_count * 8)));
+        k_sddmm_csr<VT><<<blocks, kSdThreads, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, p->rows, p->cols, p->nnz,
                                                          static_cast<VT>(alpha), static_cast<const VT*>(u), ub,
                                                          static_cast<const VT*>(v), vb, static_cast<VT*>(out), ob);
     } else {
@@ -811,7 +1023,7 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     }
     const std::string key = tune_key(p, DT<MT>::id, DT<VT>::id);
     const int cached = tune_lookup(key);
-    if (cached == 0 || cached == 1 || cached == 2) {
+    if (cached == 0 || cached == 1 || cached == 2 || ((cached == 7 || cached == 8) && p->format == CMCG_CSR)) {
         choice = static_cast<int8_t>(cached);
         return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, cached);
     }
@@ -819,7 +1031,15 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (mode != CMCG_ASSIGN || cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
         return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, 0);
-    const int cands[2] = {0, p->format == CMCG_CSR ? 2 : 1};
+    // CSR: thread per row, warp-staged entries, four rows per thread with
+    // 16-byte chunks, bulk-staged tiles (the last candidate's output stays in
+    // y); ELLPACK: four rows per thread, thread per row
+    int cands[4] = {0, 8, 7, 2};
+    int nc = 4;
+    if (p->format != CMCG_CSR) {
+        cands[1] = 1;
+        nc = 2;
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CMCG_CUDA(cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -829,7 +1049,8 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     float best = 0.0f;
     int pick = cands[0];
     cmcg_status rc = CMCG_OK;
-    for (int c : cands) {
+    for (int j = 0; j < nc; ++j) {
+        const int c = cands[j];
         if ((rc = launch_spmv_variant<MT, VT>(A, x, xb, y, mode, c)) != CMCG_OK) break;
         cudaEventRecord(e0, st);
         for (int r = 0; r < 3 && rc == CMCG_OK; ++r) rc = launch_spmv_variant<MT, VT>(A, x, xb, y, mode, c);
@@ -851,7 +1072,7 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     tune_store(key, pick);
     log_msg(1, "product %s: variant %d timed fastest (%.3f ms for 3 calls)", key.c_str(), pick, best);
     // the last candidate's output is in y; rerun the pick if it was another one
-    return pick == cands[1] ? CMCG_OK : launch_spmv_variant<MT, VT>(A, x, xb, y, mode, pick);
+    return pick == cands[nc - 1] ? CMCG_OK : launch_spmv_variant<MT, VT>(A, x, xb, y, mode, pick);
 }
 
 cmcg_status spmv_dispatch(cmcg_matrix A, int32_t vec_dtype, const void* x, int32_t xb, void* y, int32_t mode) {
@@ -983,9 +1204,7 @@ cmcg_status launch_dot_noalloc(cmcg_ctx ctx, int64_t n, const void* x, int32_t x
     CMCG_TRY(dot_scratch_address(ctx->device, &base));
     VT* partial = static_cast<VT*>(base);
     unsigned* ticket = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(base) + kNoAllocMaxPartials * sizeof(double));
-    const int64_t want = std::max<int64_t>(1, (n + kRedThreads * 4 - 1) / (kRedThreads * 4));
-    const int cap = std::max(1, std::min(kNoAllocMaxPartials / ob, (ctx->sm_count * 4) / std::max(1, ob) + 1));
-    const int gx = static_cast<int>(std::min<int64_t>(want, cap));
+    const int gx = dot_grid(ctx, n, ob, std::max(1, kNoAllocMaxPartials / ob));
     // the tickets must start at zero; every call clears them (no allocation)
     CMCG_CUDA(cudaMemsetAsync(ticket, 0, ob * sizeof(unsigned), ctx->stream));
     dim3 grid(gx, ob);

@@ -723,6 +723,75 @@ def test_grid_diagonal_layout_matches_sliced(cuda, monkeypatch, kind):
     assert np.linalg.norm(r) / np.linalg.norm(p3.b.astype(np.float64)) < 1.5e-10
 
 
+@pytest.mark.parametrize("kind", ["fp64", "mixed_f32"])
+@pytest.mark.parametrize("cap", [-1, 21])
+def test_host_loop_matches_graph_loop(cuda, monkeypatch, kind, cap):
+    # CUMAT_CG_GRAPH=0 launches the grid path's iteration kernels from the host
+    # (reading the count of running instances back every 16 iterations)
+    # instead of through the graph's WHILE node: the same kernels on the same
+    # data, so the same bits, iteration counts and statuses, with or without
+    # an iteration cap
+    m = cm()
+    monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    p3 = P.fv3d(24, 1.0, 7)
+    pat = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    A64 = m.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
+    A32 = m.SparseMatrix(pat, dtype=torch.float32).setData(p3.val)
+    b64 = torch.from_numpy(p3.b.astype(np.float64)).to(cuda)
+
+    def run():
+        if kind == "fp64":
+            cg = m.ConjugateGradient(A64).setTolerance(1e-10).setMaxIterations(cap).set_path(2)
+            x = cg.solve(b64)
+        else:
+            cg = m.ConjugateGradient(A32).setTolerance(1e-4).setMaxIterations(cap).set_path(2)
+            x = cg.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=60)
+        return x.cpu().numpy(), cg.system_stats()
+
+    x1, s1 = run()
+    monkeypatch.setenv("CUMAT_CG_GRAPH", "0")
+    before = m.launch_count()
+    x0, s0 = run()
+    host_launches = m.launch_count() - before
+    assert np.array_equal(s1["iterations"], s0["iterations"]) and np.array_equal(s1["status"], s0["status"])
+    assert np.array_equal(x1, x0, equal_nan=True)
+    # one launch per kernel per iteration (the graph counts as one)
+    assert host_launches >= 3 * int(s0["iterations"].max())
+    if cap < 0:
+        assert s1["status"][0] == 0
+    elif kind == "fp64":
+        assert s1["status"][0] == m._native.SOLVE_MAX_ITER and int(s1["iterations"][0]) == cap
+
+
+def test_cooperative_solve_forced_on_large_system(cuda, monkeypatch):
+    # systems above 2^19 rows take the graph loop unless CUMAT_CG_COOP=2; the
+    # cooperative launch stages each CTA's window of p (its rows plus the
+    # columns they reach) in shared memory and must agree with the graph loop
+    m = cm()
+    pr = P.poisson2d(760, 1)
+    assert pr.n > (1 << 19)
+    A = _matrix(pr)
+    b = torch.from_numpy(pr.b).to(cuda)
+    monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    cg0 = m.ConjugateGradient(A).setTolerance(1e-6).set_path(2)
+    x0 = cg0.solve(b).cpu().numpy()
+    monkeypatch.setenv("CUMAT_CG_COOP", "2")
+    cg2 = m.ConjugateGradient(A).setTolerance(1e-6).set_path(2)
+    cg2.solve(b)
+    before = m.launch_count()
+    x2 = cg2.solve(b).cpu().numpy()
+    assert m.launch_count() - before == 2      # the cooperative solve + the finaliser
+    s0, s2 = cg0.system_stats(), cg2.system_stats()
+    assert s0["status"][0] == 0 and s2["status"][0] == 0
+    assert abs(int(s2["iterations"][0]) - int(s0["iterations"][0])) <= 2
+    assert np.linalg.norm(x2 - x0) / np.linalg.norm(x0) < 1e-4
+    r = pr.b.astype(np.float64) - O.spmv_csr_f32_in_f64(pr.n, pr.n, pr.row_ptr, pr.col, pr.val, x2)[0]
+    # the FP32 recursion drifts from the true residual by about eps_f32 *
+    # cond(A) times the size of the updates (1.9e-4 measured at 1024^2)
+    assert np.linalg.norm(r) / np.linalg.norm(pr.b.astype(np.float64)) < 1e-3
+    assert m.Context.current().device_errors() == 0
+
+
 def test_bf16_values_fall_back_to_fp32(cuda, monkeypatch):
     # BF16 values round the Jacobi-scaled systems by up to 2^-9; on the larger,
     # worse-conditioned systems of this batch the reliable updates stop

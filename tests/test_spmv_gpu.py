@@ -295,9 +295,43 @@ def test_tuning_cache_records_the_choice(cuda, monkeypatch, tmp_path):
     y0 = (A * x).cpu().numpy()
     lines = cache.read_text().split("\n")
     key = f"|csr|0|0|{pr.n}|{pr.nnz}|0 "
-    assert any(key in (l + " ") and l.split()[-1] in ("0", "2") for l in lines if l), lines
+    assert any(key in (l + " ") and l.split()[-1] in ("0", "2", "7", "8") for l in lines if l), lines
     B = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
     before = cm.launch_count()
     y1 = (B * x).cpu().numpy()
     assert cm.launch_count() - before == 1
     assert np.array_equal(y0, y1)
+
+
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64, torch.bfloat16])
+@pytest.mark.parametrize("variant,max_len", [("7", 12), ("8", 12), ("8", 700)])
+def test_row_order_kernels_equal_thread_per_row(cuda, monkeypatch, dt, variant, max_len):
+    # the 16-byte-chunk kernel (variant 7) and the warp-staged kernel (variant
+    # 8) add every row in entry order with fused multiply-adds, so they equal
+    # thread per row (variant 0) bit for bit: random rows of 0..max_len
+    # entries (empty rows, a row count that is not a multiple of 4 or 32, and
+    # with max_len 700 rows that span several staging rounds of 256 entries),
+    # two batches of values and vectors, all assignment modes
+    cm = _cm()
+    rng = np.random.default_rng(17 + max_len)
+    n = 5003 if max_len < 100 else 701
+    lens = rng.integers(0, max_len + 1, n)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    col = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) for k in lens]).astype(np.int32)
+    vals = rng.uniform(-1.0, 1.0, (2, col.size))
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(n, n, rp, col), dtype=dt, batches=2).setData(vals)
+    vdt = torch.float64 if dt == torch.float64 else torch.float32
+    X = torch.from_numpy(rng.uniform(-1.0, 1.0, (2, n))).to(device=cuda, dtype=vdt)
+    out = {}
+    for v in ("0", variant):
+        monkeypatch.setenv("CUMAT_SPMV_VARIANT", v)
+        res = [A.product(X).cpu().numpy()]
+        for mode in (cm._native.ADD, cm._native.SUB):
+            y = torch.ones((2, n), dtype=vdt, device=cuda)
+            A.product(X, out=y, mode=mode)
+            res.append(y.cpu().numpy())
+        out[v] = res
+    for a, b in zip(out["0"], out[variant]):
+        assert np.array_equal(a, b)
+    assert np.all(out[variant][0][:, lens == 0] == 0)
