@@ -913,7 +913,7 @@ __device__ __forceinline__ void p_quad(const VT* __restrict__ p, int c, int lo, 
 // quad each. The entries are the clamped ones in every case, so the sums do
 // not depend on how they were loaded.
 // UNIT: the middle diagonal is offset 0 with every value 1 and is not loaded.
-// emit(global row, value).
+// emit(global row, value, p[row]).
 template <typename VT, typename MT, int ND, bool UNIT, typename F>
 __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int (&off)[ND], int sr0, int send, int r0,
                                              int r1, const VT* __restrict__ p, F&& emit) {
@@ -929,6 +929,18 @@ __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int
         if (ib >= r1) continue;
         const int li = ib - sr0;
         const MT* vr = v + (static_cast<int64_t>(li / kDiaBlockRows) * ND * kDiaBlockRows) + li % kDiaBlockRows;
+        // The value loads (the streamed bytes) of all diagonals are issued
+        // before the first use, so that one diagonal's DRAM latency does not
+        // follow another's behind the offset branches below; 8-byte values
+        // keep the per-diagonal order (ND quads of them would not fit the
+        // 64-register budget of four CTAs per SM).
+        constexpr bool kHoist = sizeof(MT) <= 4;
+        Vals4<MT> w[kHoist ? ND : 1];
+        if constexpr (kHoist) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d)
+                if (!(UNIT && d == ND / 2)) load_stream(w[d], vr + d * kDiaBlockRows);
+        }
         VT acc[4] = {VT(0), VT(0), VT(0), VT(0)};
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
@@ -952,15 +964,16 @@ __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc[q] = fma(VT(1), pv[q], acc[q]);
             } else {
-                Vals4<MT> w;
-                load_stream(w, vr + d * kDiaBlockRows);
+                Vals4<MT> wd;
+                if constexpr (kHoist) wd = w[d];
+                else load_stream(wd, vr + d * kDiaBlockRows);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] = fma(mval<VT>(w.v[q]), pv[q], acc[q]);
+                for (int q = 0; q < 4; ++q) acc[q] = fma(mval<VT>(wd.v[q]), pv[q], acc[q]);
             }
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-            if (ib + q < r1) emit(ib + q, acc[q]);
+            if (ib + q < r1) emit(ib + q, acc[q], own[q]);
     }
 }
 
@@ -1105,7 +1118,10 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_spmv_pq(SolveArg
         if constexpr (ND > 0) {
             int off[ND];
             const MT* v = dia_system<MT, ND>(a.dia, b_, g.s, off);
-            dia_rows_seg<VT, MT, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit);
+            dia_rows_seg<VT, MT, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, [&](int row, VT qv, VT prow) {
+                __stcs(q + row, qv);
+                acc[0] += prow * qv;
+            });
         } else {
             const auto A = inst_matrix<MT, FMT>(a.m, b_);
             cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, emit);
@@ -1347,8 +1363,12 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_spmv(GMixArgs<MI
             int off[ND];
             const MI* v = dia_system<MI, ND>(a.dia, b_, g.s, off);
             const bool unit = a.dia.unit && __ldg(a.dia.unit + (a.dia.mb == 1 ? 0 : b_ * a.n_sys) + g.s);
-            if (unit) dia_rows_seg<float, MI, ND, true>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit);
-            else dia_rows_seg<float, MI, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit);
+            const auto emit3 = [&](int row, float qv, float prow) {
+                __stcs(q + row, qv);
+                acc[0] += prow * qv;
+            };
+            if (unit) dia_rows_seg<float, MI, ND, true>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit3);
+            else dia_rows_seg<float, MI, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit3);
         } else {
             const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
             cta_rows4_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, emit);
@@ -1371,6 +1391,28 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_spmv(GMixArgs<MI
             }
         }
     }
+}
+
+// Condition probe of BF16 inner values (grid path). CG's residual contracts
+// at least as fast as its bound for the scaled system's condition number
+// kappa, so the rate rho observed over the first kCondProbe iterations gives
+// a lower estimate kappa >= ((1 + rho) / (1 - rho))^2. Refinement through an
+// inner system rounded to BF16 (unit roundoff 2^-8) needs kappa * 2^-8 well
+// below 1; above kBf16CondLimit the instance stops with BREAKDOWN, and the
+// FP32 fallback solves it, instead of the progress guard's thousands of
+// iterations later. ratio = |r_k|^2 / |r_0|^2 of the first cycle.
+constexpr int32_t kCondProbe = 64;
+constexpr float kBf16CondLimit = 256.0f;
+// The same decision at every replacement: the inner recursion claimed |r|^2
+// down by delta^2 since the last one, the true FP64 residual is down by about
+// (delta + u kappa)^2; a true ratio above kBf16Lag delta^2 means the BF16
+// rounding term dominates, and the cycles to come will crawl.
+constexpr double kBf16Lag = 10.0;
+__device__ __forceinline__ bool bf16_condition_ok(float ratio, int32_t k) {
+    if (!(ratio < 1.0f)) return false;   // no contraction at all (or NaN)
+    const float rho = powf(ratio, 0.5f / static_cast<float>(k));
+    const float s = (1.0f + rho) / (1.0f - rho);
+    return s * s <= kBf16CondLimit;
 }
 
 // xh += alpha p, r -= alpha q, |r|^2 -> replacement decision or beta
@@ -1425,6 +1467,10 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_update(GMixArgs<
             const int n = g.send - g.sr0;
             if (!finite_(rzn)) {
                 a.st.status[g.inst] = CMCG_SOLVE_NON_FINITE;
+                atomicSub(a.active, 1);
+            } else if (std::is_same<MI, __nv_bfloat16>::value && it == kCondProbe && a.st.outer[g.inst] == 0 &&
+                       !bf16_condition_ok(rzn / static_cast<float>(a.st.rmax[g.inst]), it)) {
+                a.st.status[g.inst] = CMCG_SOLVE_BREAKDOWN;
                 atomicSub(a.active, 1);
             } else if (rzn < d2 * static_cast<float>(a.st.rmax[g.inst]) || rzn < static_cast<float>(a.st.goal[g.inst]) ||
                        it >= sys_max_iter(a.max_iter, n) ||
@@ -1498,7 +1544,8 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_residual(GMixArg
             const int32_t outer = a.st.outer[g.inst] + 1;
             a.st.outer[g.inst] = outer;
             // progress guard: the true residual against the last replacement's
-            const int32_t stall = rr64 > kStallRatio * a.st.rr[g.inst] ? a.st.stall[g.inst] + 1 : 0;
+            const double rr_prev = a.st.rr[g.inst];
+            const int32_t stall = rr64 > kStallRatio * rr_prev ? a.st.stall[g.inst] + 1 : 0;
             a.st.stall[g.inst] = stall;
             if (outer == 1) a.st.cyc0[g.inst] = a.st.it[g.inst];
             a.st.rep_it[g.inst] = a.st.it[g.inst];
@@ -1508,8 +1555,11 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_residual(GMixArg
             a.st.flag[g.inst] = 0;
             const int n = g.send - g.sr0;
             int32_t status = ST_RUNNING;
+            const double d2 = static_cast<double>(m.delta) * m.delta;
             if (!finite_(rr64)) status = CMCG_SOLVE_NON_FINITE;
             else if (rr64 < thr) status = CMCG_SOLVE_CONVERGED;
+            else if (std::is_same<MI, __nv_bfloat16>::value && rr64 > kBf16Lag * d2 * rr_prev)
+                status = CMCG_SOLVE_BREAKDOWN;   // BF16 values too coarse for this system
             else if (a.st.it[g.inst] >= sys_max_iter(a.max_iter, n) || outer >= m.max_updates) status = CMCG_SOLVE_MAX_ITER;
             else if (!(rzn > 0.0f) || stall >= kStallMax) status = CMCG_SOLVE_BREAKDOWN;
             if (status != ST_RUNNING) {

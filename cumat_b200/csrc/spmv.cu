@@ -794,88 +794,29 @@ cmcg_status launch_dot(cmcg_ctx ctx, int64_t n, const void* x, int32_t xb, const
 // ---- sampled outer product on the pattern -----------------------------------------
 
 // Sampled outer product on a CSR pattern, out_k = alpha * u[row(k)] * v[col(k)]
-// for every stored entry k. A CTA takes 1024 rows at a time (four per thread)
-// and walks their entries in windows of 2048: the thread of each non-empty
-// row marks the row's first entry in the window, an inclusive max-scan over
-// the window (threads scan 8 consecutive slots, then across the CTA) gives
-// every entry its row, and the entries are then read and written in order
-// (coalesced), each column index loaded once for all value batches. The work
-// per entry is a few instructions whatever the row lengths (a long row only
-// spans more windows). Slot k of the window sits at k + k / 32 in shared
-// memory, so that the scan's strided accesses hit 32 different banks.
-constexpr int kSdThreads = 256, kSdRowsPer = 4, kSdRows = kSdThreads * kSdRowsPer, kSdPer = 8,
-              kSdWin = kSdThreads * kSdPer;
-
-__device__ __forceinline__ int sd_slot(int k) { return k + (k >> 5); }
-
+// for every stored entry k: thread per row, as the row-unrolled product, with
+// kCsrUnroll column indices loaded before the first gather and reused for all
+// value batches; each product is (alpha * u) * v, the reference's order.
 template <typename VT>
-__global__ void __launch_bounds__(kSdThreads) k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                          int32_t rows, int32_t cols, int64_t vstride, VT alpha,
-                                                          const VT* __restrict__ u, int32_t ub,
-                                                          const VT* __restrict__ v, int32_t vb,
-                                                          VT* __restrict__ out, int32_t ob) {
-    __shared__ int32_t owner[kSdWin + kSdWin / 32];
-    __shared__ int32_t wmax[kSdThreads / 32];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int ntile = (rows + kSdRows - 1) / kSdRows;
-    for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
-        const int r0 = tile * kSdRows;
-        const int nr = min(kSdRows, rows - r0);
-        int my_lo[kSdRowsPer], my_hi[kSdRowsPer];
+__global__ void __launch_bounds__(kSpmvThreads) k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                            int32_t rows, int32_t cols, int64_t vstride, VT alpha,
+                                                            const VT* __restrict__ u, int32_t ub,
+                                                            const VT* __restrict__ v, int32_t vb,
+                                                            VT* __restrict__ out, int32_t ob) {
+    for (int r = blockIdx.x * kSpmvThreads + threadIdx.x; r < rows; r += gridDim.x * kSpmvThreads) {
+        const int e = __ldg(rp + r + 1);
+        for (int k = __ldg(rp + r); k < e; k += kCsrUnroll) {
+            int c[kCsrUnroll];
 #pragma unroll
-        for (int m = 0; m < kSdRowsPer; ++m) {   // rows r0 + t + 256 m (coalesced bounds)
-            const int lr = t + m * kSdThreads;
-            my_lo[m] = lr < nr ? __ldg(rp + r0 + lr) : 0;
-            my_hi[m] = lr < nr ? __ldg(rp + r0 + lr + 1) : 0;
-        }
-        const int lo = __ldg(rp + r0), hi = __ldg(rp + r0 + nr);
-        int carry = -1;   // the row (in the tile) owning the window's first entry
-        for (int w0 = lo; w0 < hi; w0 += kSdWin) {
-            const int wn = min(kSdWin, hi - w0);
+            for (int q = 0; q < kCsrUnroll; ++q) c[q] = k + q < e ? __ldg(ci + k + q) : -1;
+            for (int b = 0; b < ob; ++b) {
+                const VT au = alpha * __ldg(u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows) + r);
+                const VT* vv = v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols);
+                VT* o = out + static_cast<int64_t>(b) * vstride + k;
 #pragma unroll
-            for (int j = 0; j < kSdPer; ++j) owner[sd_slot(j * kSdThreads + t)] = -1;
-            __syncthreads();
-#pragma unroll
-            for (int m = 0; m < kSdRowsPer; ++m)
-                if (my_hi[m] > my_lo[m] && my_lo[m] >= w0 && my_lo[m] < w0 + wn)
-                    owner[sd_slot(my_lo[m] - w0)] = t + m * kSdThreads;
-            __syncthreads();
-            int mark[kSdPer];
-            int m = -1;
-#pragma unroll
-            for (int j = 0; j < kSdPer; ++j) {
-                mark[j] = owner[sd_slot(t * kSdPer + j)];
-                m = max(m, mark[j]);
+                for (int q = 0; q < kCsrUnroll; ++q)
+                    if (c[q] >= 0) o[q] = au * __ldg(vv + c[q]);
             }
-            int wm = m;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, wm, o);
-                if (lane >= o) wm = max(wm, y);
-            }
-            if (lane == 31) wmax[warp] = wm;
-            const int ex = __shfl_up_sync(0xffffffffu, wm, 1);
-            __syncthreads();
-            int pre = max(carry, lane == 0 ? -1 : ex);
-            for (int w = 0; w < warp; ++w) pre = max(pre, wmax[w]);
-#pragma unroll
-            for (int j = 0; j < kSdPer; ++j) {
-                pre = max(pre, mark[j]);
-                owner[sd_slot(t * kSdPer + j)] = pre;
-            }
-            __syncthreads();
-            for (int j = t; j < wn; j += kSdThreads) {
-                const int64_t k = static_cast<int64_t>(w0) + j;
-                const int row = r0 + owner[sd_slot(j)];
-                const int c = __ldg(ci + k);
-                for (int b = 0; b < ob; ++b) {
-                    const VT uu = __ldg(u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows) + row);
-                    const VT vv = __ldg(v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols) + c);
-                    out[static_cast<int64_t>(b) * vstride + k] = alpha * uu * vv;
-                }
-            }
-            carry = owner[sd_slot(kSdWin - 1)];   // (read only when the window was full)
-            __syncthreads();
         }
     }
 }
@@ -906,9 +847,9 @@ cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub,
     cmcg_pattern p = M->pat;
     cmcg_ctx ctx = p->ctx;
     if (p->format == CMCG_CSR) {
-        const int64_t tiles = (static_cast<int64_t>(p->rows) + kSdRows - 1) / kSdRows;
-        const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, ctx->sm_count * 8)));
-        k_sddmm_csr<VT><<<blocks, kSdThreads, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, p->rows, p->cols, p->nnz,
+        const int64_t need = (static_cast<int64_t>(p->rows) + kSpmvThreads - 1) / kSpmvThreads;
+        const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, ctx->sm_count * 8)));
+        k_sddmm_csr<VT><<<blocks, kSpmvThreads, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, p->rows, p->cols, p->nnz,
                                                          static_cast<VT>(alpha), static_cast<const VT*>(u), ub,
                                                          static_cast<const VT*>(v), vb, static_cast<VT*>(out), ob);
     } else {

@@ -145,6 +145,52 @@ def test_config4_64_mixed_to_1e10(cuda, fv3d64, inner):
     _check_truth(pr, x, 1e-7)
 
 
+def test_bf16_condition_probe_on_the_grid_path(cuda, fv3d64, monkeypatch):
+    """BF16 inner values on the grid path: every replacement compares the
+    true FP64 residual with the inner recursion's claim (delta^2 = 0.01 of
+    |r|^2 since the last replacement). On the 64^3 system the true residual
+    falls behind by more than 10x after a few cycles (left alone, BF16 needs
+    about 44,000 inner iterations and 49 replacements where FP32 needs a few
+    hundred), so the BF16 solve stops with BREAKDOWN and the FP32 fallback
+    solves the system to 1e-10; on a well-conditioned system (the same matrix
+    plus twice its diagonal: scaled eigenvalues in [2/3, 4/3] roughly) BF16
+    values carry the refinement to 1e-10 without a fallback."""
+    if "c4_64_idx" not in SG:
+        pytest.skip("64^3 fixture not generated")
+    m = cm()
+    pr = fv3d64
+    pat = m.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)
+    A32 = m.SparseMatrix(pat, dtype=torch.float32).setData(pr.val)
+    Ab = m.SparseMatrix(pat, dtype=torch.bfloat16).setData(pr.val)
+    b = torch.from_numpy(pr.b.astype(np.float64)).to(cuda)
+    monkeypatch.setenv("CUMAT_CG_BF16_FALLBACK", "0")
+    cg0 = m.ConjugateGradient(Ab).setTolerance(1e-4)
+    cg0.solve_refined(b, outer=A32, outer_tol=1e-10, max_outer=60)
+    s0 = cg0.system_stats()
+    # (measured: BREAKDOWN after 7 replacements and 2607 inner iterations, at
+    # a true relative residual of 6.7e-6)
+    assert s0["status"][0] == m._native.SOLVE_BREAKDOWN and int(s0["outer"][0]) <= 12, s0
+    assert int(s0["iterations"][0]) <= 6000, s0
+    monkeypatch.setenv("CUMAT_CG_BF16_FALLBACK", "1")
+    cg1 = m.ConjugateGradient(Ab).setTolerance(1e-4)
+    x = cg1.solve_refined(b, outer=A32, outer_tol=1e-10, max_outer=60).cpu().numpy()
+    s1 = cg1.system_stats()
+    assert s1["status"][0] == 0 and s1["fallback"][0] == 1
+    assert _rel_res(pr, x) < 1e-10
+    # well conditioned: A + 2 diag(A), values exact in FP32
+    rows = np.repeat(np.arange(pr.n), np.diff(pr.row_ptr))
+    on = pr.col == rows
+    val = pr.val.copy()
+    val[on] *= 3.0
+    A2 = m.SparseMatrix(pat, dtype=torch.float32).setData(val)
+    cg2 = m.ConjugateGradient(m.SparseMatrix(pat, dtype=torch.bfloat16).setData(val)).setTolerance(1e-4)
+    x2 = cg2.solve_refined(b, outer=A2, outer_tol=1e-10, max_outer=60).cpu().numpy()
+    s2 = cg2.system_stats()
+    assert s2["status"][0] == 0 and s2["fallback"][0] == 0, s2
+    r = pr.b.astype(np.float64) - O.spmv_csr_f32_in_f64(pr.n, pr.n, pr.row_ptr, pr.col, val, x2)[0]
+    assert np.linalg.norm(r) / np.linalg.norm(pr.b.astype(np.float64)) < 1e-10
+
+
 def test_config4_64_fp64_matches_eigen(cuda, fv3d64):
     """Plain FP64 Jacobi-CG to 1e-10: iteration count within +-2 of Eigen's
     FP64 ConjugateGradient, true residual < 1e-10 (up to the FP64 recurrence
