@@ -31,9 +31,9 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--ex
                   "-I" + str(ROOT / "include")]
 
 CU_SOURCES = ["runtime.cu", "spmv.cu", "sell.cu", "sparse_ops.cu", "reduce.cu", "cg.cu", "cg_mixed.cu", "cg_plain.cu",
-              "cg_coop.cu", "lincomb.cu"]
+              "cg_coop.cu", "cg_cluster.cu", "lincomb.cu"]
 HEADERS = ["common.cuh", "objects.h", "spmv_dev.cuh", "cg_dev.cuh", "tma.cuh", "cg_smem.cuh", "cg_grid.cuh",
-           "grid_sync.cuh", "cg_compact.cuh", "cg_plain.cuh"]
+           "grid_sync.cuh", "cg_compact.cuh", "cg_plain.cuh", "cg_cluster.cuh"]
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

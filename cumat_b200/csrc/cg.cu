@@ -30,6 +30,7 @@
 
 #include <type_traits>
 
+#include "cg_cluster.cuh"
 #include "cg_compact.cuh"
 #include "cg_dev.cuh"
 #include "cg_smem.cuh"
@@ -1702,6 +1703,8 @@ struct cmcg_solver_s {
     // cooperative one-launch grid solve: 0 never, 1 where it applies (systems up
     // to kCoopMaxRows rows), 2 also for larger systems (CUMAT_CG_COOP)
     int coop = 1;
+    // cluster solve of the grid path where it applies (CUMAT_CG_CLUSTER=0 disables)
+    bool cluster = true;
     // grid path iteration loop: true = one CUDA graph with a device-side WHILE
     // node; false = the same kernels launched from the host, polling the count
     // of running instances (CUMAT_CG_GRAPH=0; kernel profilers do not replay
@@ -2449,6 +2452,38 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     return CMCG_OK;
 }
 
+// One thread-block cluster per instance (cg_cluster.cu), when every system
+// is larger than one CTA solves (kClusterMinRows) yet its p, q and r fit the
+// shared memory of at most kClusterMaxCtas CTAs, and all instances' clusters
+// can be resident at once. *done = false leaves the solve to the cooperative
+// launch or the graph loop.
+constexpr int32_t kClusterMinRows = 16384;
+template <typename VT, typename MT, int FMT>
+cmcg_status run_cluster(cmcg_solver s, SolveArgs<VT, MT>& a, bool* done) {
+    *done = false;
+    cmcg_ctx ctx = s->A->pat->ctx;
+    const int n_inst = a.n_sys * a.ob;
+    if (!s->cluster || s->max_sys_rows <= kClusterMinRows) return CMCG_OK;
+    int optin = 0;
+    CMCG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    int ctas = 0;
+    // (2 KB of the CTA's shared memory hold the reduction scratch)
+    const int lg = cluster_rows_log2(s->max_sys_rows, sizeof(VT), static_cast<size_t>(std::max(0, optin - 2048)), &ctas);
+    if (lg == 0 || ctas < 2) return CMCG_OK;
+    bool launched = false;
+    CMCG_TRY((cluster_cg_launch<VT, MT, FMT>(a, n_inst, ctas, lg, n_inst, ctx->stream, &launched)));
+    if (!launched) {
+        if (log_on(1))
+            log_msg(1, "cluster solve not launched: %d clusters of %d CTAs cannot be resident at once", n_inst, ctas);
+        return CMCG_OK;
+    }
+    if (log_on(2)) log_msg(2, "cluster solve: %d clusters of %d CTAs x %d rows", n_inst, ctas, 1 << lg);
+    count_launch();
+    CMCG_CHECK_LAUNCH();
+    *done = true;
+    return CMCG_OK;
+}
+
 // One cooperative launch for the whole grid-path solve, when the instances are
 // few (the closing sums run in one CTA per barrier) and the segment plan's
 // CTAs can all be resident. *done = false leaves the solve to the graph path.
@@ -2540,7 +2575,8 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
         a.r = w; a.p = w + nv; a.q = w + 2 * nv; a.x = w + 3 * nv;
         a.b = b; a.b_b = b_b; a.guess = guess; a.g_b = ob;
         bool done = false;
-        CMCG_TRY((run_coop<VT, MT, FMT>(s, a, w + 4 * nv, &done)));
+        CMCG_TRY((run_cluster<VT, MT, FMT>(s, a, &done)));
+        if (!done) CMCG_TRY((run_coop<VT, MT, FMT>(s, a, w + 4 * nv, &done)));
         if (!done) CMCG_TRY((run_grid<VT, MT, FMT>(s, a)));
         const int fb = (n_inst + 255) / 256;
         k_finalize<<<fb, 256, 0, ctx->stream>>>(s->st, n_inst);
@@ -2993,6 +3029,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     if (const char* e = std::getenv("CUMAT_CG_DIA")) s->dia_kernels = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_SMALL")) s->mix_small = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::max(0, std::min(2, std::atoi(e)));
+    if (const char* e = std::getenv("CUMAT_CG_CLUSTER")) s->cluster = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_GRAPH")) s->graph_loop = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_BF16_FALLBACK")) s->bf16_fallback = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);

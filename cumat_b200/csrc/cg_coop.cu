@@ -80,6 +80,7 @@ struct CoopArgs {
     int32_t n_inst;
     VT* p_alt;   // second p buffer, [batch][rows]
     BarrierLimits lim;
+    int32_t window;   // stage p_k over each CTA's column window (else form it inside the gathers)
 };
 
 // Totals of NV partial arrays over the segments of instance `inst` (whole CTA,
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(kCoopThreads, 1) k_coop_cg(SolveArgs<VT, MT> a
         }
         __syncthreads();
     }
-    const bool use_win = win_sys >= 0;
+    const bool use_win = c.window && win_sys >= 0;
     const int wlo = win_lo, whi = win_hi + 1;
 
 // loop over this CTA's (batch, segment) pairs: b_, g (SegCache), inst, pidx, vo
@@ -424,7 +425,10 @@ cmcg_status coop_cg_launch(const SolveArgs<VT, MT>& a, void* sync, int32_t* err,
     BarrierLimits lim{kGridBarrierSpins, 0u};
     if (const char* e = std::getenv("CUMAT_TEST_GRID_SPINS")) lim.spins = std::max(1LL, std::atoll(e));
     if (const char* e = std::getenv("CUMAT_TEST_GRID_EXTRA")) lim.extra = static_cast<unsigned>(std::max(0, std::atoi(e)));
-    CoopArgs<VT> c{static_cast<GridSync*>(sync), err, n_inst, p_alt, lim};
+    // CUMAT_CG_COOP_WINDOW=0 forms p_k inside the gathers instead of staging it
+    int32_t window = 1;
+    if (const char* e = std::getenv("CUMAT_CG_COOP_WINDOW")) window = std::atoi(e) != 0;
+    CoopArgs<VT> c{static_cast<GridSync*>(sync), err, n_inst, p_alt, lim, window};
     void* params[] = {&args, &c};
     CMCG_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_coop_cg<VT, MT, FMT>), grid, kCoopThreads,
                                           params, kCoopWindowBytes, st));

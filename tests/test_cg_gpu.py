@@ -493,6 +493,7 @@ def test_cooperative_grid_solve_matches_graph_path(cuda, monkeypatch, dtype):
     # grid solve (four CTAs per SM) differ only in how the partial sums are
     # grouped
     m = cm()
+    monkeypatch.setenv("CUMAT_CG_CLUSTER", "0")   # (the cluster solve would take this size)
     pr = P.poisson2d(160, 3)
     A = _matrix(pr, dtype=dtype)
     b = torch.from_numpy(pr.b.astype(np.float64 if dtype == torch.float64 else np.float32)).to(cuda)
@@ -518,9 +519,10 @@ def test_cooperative_grid_solve_matches_graph_path(cuda, monkeypatch, dtype):
     assert m.Context.current().device_errors() == 0
 
 
-def test_cooperative_grid_solve_batched_instances(cuda):
+def test_cooperative_grid_solve_batched_instances(cuda, monkeypatch):
     # 3 value batches x 2 systems = 6 instances in one cooperative launch
     m = cm()
+    monkeypatch.setenv("CUMAT_CG_CLUSTER", "0")   # (the cluster solve would take these sizes)
     bt = P.fv2d_batch(2, 150, 170, 0.5, 17)
     p = m.SparsityPattern.csr(bt.n, bt.n, bt.row_ptr, bt.col)
     p.set_systems(bt.row_off)
@@ -695,6 +697,7 @@ def test_grid_diagonal_layout_matches_sliced(cuda, monkeypatch, kind):
     # the same order as the sliced layout, so both runs agree bit for bit
     m = cm()
     monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    monkeypatch.setenv("CUMAT_CG_CLUSTER", "0")
     p3 = P.fv3d(32, 1.0, 5)
     pat = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
     A64 = m.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
