@@ -447,7 +447,7 @@ def cg_config2(cm, torch, dev, stream, hbm_peak):
            "gbs_model": round(gbs, 1), "frac_model": round(gbs / hbm_peak, 3)}
     # the other grid-path loop on the same system: the cooperative one-launch
     # solve (one CTA per SM, p staged per CTA in shared memory), which the
-    # solver picks for systems up to 2^19 rows (CUMAT_CG_COOP=2 forces it)
+    # solver picks for systems up to 2^15 rows (CUMAT_CG_COOP=2 forces it)
     old = os.environ.get("CUMAT_CG_COOP")
     os.environ["CUMAT_CG_COOP"] = "2"
     try:
@@ -893,6 +893,8 @@ def run_profile_case(case: str):
                 about 10 GB on the device: launch lists only)
     cg4096      the same on the 4096^2 Poisson matrix (16.8 M rows, 1.2 GB
                 streamed per iteration), for full captures
+    cluster200  the 200^2 Poisson matrix (40,000 rows), FP32 Jacobi-CG capped at
+                50 iterations: the cluster solve (k_cluster_cg, one launch)
     c4          the 256^3 precision system: 12 plain FP64 Jacobi-CG iterations
                 and 12 inner iterations of the mixed FP32 / FP64 solve (one
                 launch per kernel under CUMAT_CG_GRAPH=0: the per-kernel share
@@ -927,6 +929,12 @@ def run_profile_case(case: str):
         cm.ConjugateGradient(A64).setTolerance(1e-10).setMaxIterations(12).set_path(2).solve(b64)
         cgm = cm.ConjugateGradient(A32).setTolerance(1e-4).setMaxIterations(12).set_path(2)
         cgm.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=3)
+    elif case == "cluster200":
+        pr = P.poisson2d(200, 1)
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+        b = torch.from_numpy(pr.b).to(dev)
+        cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(50).solve(b)
+        out.update(rows=pr.n, nnz=pr.nnz)
     elif case in ("cg10000", "cg4096"):
         pr = P.poisson2d(10000 if case == "cg10000" else 4096, 1)
         A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
@@ -992,7 +1000,7 @@ def main():
                     help="run the small profiling case once (no JSON line): SpMV on the 1024^2 Poisson matrix and the "
                          "mixed and FP64 solvers on the first 512 systems of the batch")
     ap.add_argument("--profile-case", default=None,
-                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big, cg10000, cg4096, c4)")
+                    help="run one small single-purpose workload for ncu (grid3d, plain_dia, vectors, spmv_big, cg10000, cg4096, c4, cluster200)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

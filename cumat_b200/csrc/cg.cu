@@ -2470,14 +2470,31 @@ cmcg_status run_cluster(cmcg_solver s, SolveArgs<VT, MT>& a, bool* done) {
     // (2 KB of the CTA's shared memory hold the reduction scratch)
     const int lg = cluster_rows_log2(s->max_sys_rows, sizeof(VT), static_cast<size_t>(std::max(0, optin - 2048)), &ctas);
     if (lg == 0 || ctas < 2) return CMCG_OK;
+    // stencil-shaped CSR patterns: the product reads the diagonal layout
+    SolveArgs<VT, MT> c = a;
+    int nd = 0;
+    c.dia = DiaArgs<MT>{};
+    if (FMT == CMCG_CSR) {
+        bool dia = false;
+        CMCG_TRY(ensure_dia_plain(s, &dia));
+        if (dia) {
+            const DiaPlan& D = s->A->pat->dia;
+            nd = D.max_nd;
+            c.dia = DiaArgs<MT>{static_cast<const MT*>(s->dia_plain), s->dia_plain_stride, D.d_sys_base, D.d_sys_off,
+                                nullptr, s->A->batches};
+        }
+    }
+    if (nd != 5 && nd != 7) nd = 0;
     bool launched = false;
-    CMCG_TRY((cluster_cg_launch<VT, MT, FMT>(a, n_inst, ctas, lg, n_inst, ctx->stream, &launched)));
+    CMCG_TRY((cluster_cg_launch<VT, MT, FMT>(c, n_inst, ctas, lg, nd, n_inst, ctx->stream, &launched)));
     if (!launched) {
         if (log_on(1))
             log_msg(1, "cluster solve not launched: %d clusters of %d CTAs cannot be resident at once", n_inst, ctas);
         return CMCG_OK;
     }
-    if (log_on(2)) log_msg(2, "cluster solve: %d clusters of %d CTAs x %d rows", n_inst, ctas, 1 << lg);
+    if (log_on(2))
+        log_msg(2, "cluster solve: %d clusters of %d CTAs x %d rows, %s layout", n_inst, ctas, 1 << lg,
+                nd ? "diagonal" : "sliced");
     count_launch();
     CMCG_CHECK_LAUNCH();
     *done = true;

@@ -3,9 +3,11 @@
 // threads on B200) are solved by one cluster each, without grid barriers.
 //
 // CTA k of a cluster owns the 2^lg rows [k 2^lg, (k + 1) 2^lg) of its system
-// and keeps their p, q and r in its shared memory; x, b and the inverse
-// diagonal stay in global memory. The product gathers p from the CTA that
-// owns each column through distributed shared memory (the column's owner is a
+// and keeps their p, q, r, x and inverse diagonal in its shared memory (x is
+// written back at the end). The product reads the values from global memory
+// (L2) in the pattern's diagonal layout for stencil patterns (no column
+// indices), else in the sliced layout, and gathers p from the CTA that owns
+// each column through distributed shared memory (the column's owner is a
 // shift of its local row). A scalar (p.q, |r|^2, r.z) is summed per CTA, each
 // CTA writes its partial into every CTA's shared memory, and after one cluster
 // barrier every CTA adds the partials in rank order, so all CTAs hold the same
@@ -19,6 +21,7 @@
 
 #include "cg_cluster.cuh"
 #include "cg_dev.cuh"
+#include "objects.h"
 
 namespace cmcg {
 namespace {
@@ -78,18 +81,49 @@ __device__ __forceinline__ void cluster_rows(const InstMatrix<MT, FMT>& A, int s
     }
 }
 
+// The same over the diagonal layout (ND diagonals per system, ascending
+// offsets, the row's CSR order): the values of both rows are loaded before
+// the first gather; a column index is clamped into the system, where a zero
+// value meets it.
+template <typename VT, typename MT, int ND, typename XF, typename F>
+__device__ __forceinline__ void cluster_dia_rows(const MT* __restrict__ v, const int (&off)[ND], int r0, int n, int lo,
+                                                 int cnt, const XF& xf, F&& f) {
+    const int T = blockDim.x;
+    for (int ib = threadIdx.x; ib < cnt; ib += 2 * T) {
+        const bool ok1 = ib + T < cnt;
+        const int ii[2] = {lo + ib, ok1 ? lo + ib + T : lo + ib};
+        MT w[2][ND];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const MT* vr = v + static_cast<int64_t>(ii[k] / kDiaBlockRows) * ND * kDiaBlockRows + ii[k] % kDiaBlockRows;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) w[k][d] = vr[d * kDiaBlockRows];
+        }
+        VT acc[2] = {VT(0), VT(0)};
+#pragma unroll
+        for (int d = 0; d < ND; ++d)
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+                acc[k] = fma(mval<VT>(w[k][d]), xf(r0 + min(max(ii[k] + off[d], 0), n - 1)), acc[k]);
+        f(r0 + ii[0], acc[0]);
+        if (ok1) f(r0 + ii[1], acc[1]);
+    }
+}
+
 struct ClusterArgs {
     int32_t ctas;   // CTAs per cluster
     int32_t lg;     // log2 of the rows per CTA
 };
 
-template <typename VT, typename MT, int FMT>
+template <typename VT, typename MT, int FMT, int ND>
 __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT, MT> a, ClusterArgs c) {
     extern __shared__ __align__(16) unsigned char cl_smem[];
     const int R = 1 << c.lg;
     VT* const p = reinterpret_cast<VT*>(cl_smem);
     VT* const q = p + R;
     VT* const r = q + R;
+    VT* const x = r + R;
+    VT* const dv = x + R;   // inverse diagonal (Jacobi)
     __shared__ VT red[2 * (kClusterThreads / 32)];
     // partial sums written by the cluster's CTAs: A for p.q and r.z, B for
     // |b|^2, |r|^2 and r.z (each reuse of a buffer is a barrier after its reads)
@@ -99,8 +133,6 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT,
     const int rank = static_cast<int>(cl.block_rank());
     const int ctas = c.ctas;
     const int inst = blockIdx.x / ctas;
-    const int n_inst = a.n_sys * a.ob;
-    if (inst >= n_inst) return;   // (the grid holds exactly n_inst clusters)
     const int bi = inst / a.n_sys, s = inst - bi * a.n_sys;
     const int r0 = a.row_off[s], n = a.row_off[s + 1] - r0;
     const int lo = rank << c.lg;
@@ -108,41 +140,55 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT,
     const int T = blockDim.x, tid = threadIdx.x;
     const int64_t vo = static_cast<int64_t>(bi) * a.rows;
     const auto A = inst_matrix<MT, FMT>(a.m, bi);
+    int off[ND > 0 ? ND : 1];
+    const MT* dvals = nullptr;
+    if constexpr (ND > 0) {
+#pragma unroll
+        for (int j = 0; j < ND; ++j) off[j] = __ldg(a.dia.off + s * kDiaMax + j);
+        dvals = a.dia.vals + (a.dia.mb == 1 ? 0 : static_cast<int64_t>(bi) * a.dia.vstride) + __ldg(a.dia.base + s);
+    }
+    // q_i = (A y)_i for the CTA's rows, f(global row, value)
+    const auto product = [&](const auto& xf, auto&& f) {
+        if constexpr (ND > 0) cluster_dia_rows<VT, MT, ND>(dvals, off, r0, n, lo, cnt, xf, f);
+        else cluster_rows<VT>(A, s, r0, lo, cnt, xf, f);
+    };
     const VT* bv = a.b + (a.b_b == 1 ? 0 : vo);
     const VT* g = a.guess ? a.guess + (a.g_b == 1 ? 0 : vo) : nullptr;
     const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
-    VT* x = a.x + vo;
+    const bool jacobi = dinv != nullptr;
     const VT tol = static_cast<VT>(a.tol);
     const int64_t maxit = sys_max_iter(a.max_iter, n);
 
     // r = b - A x0 (x0 = guess or 0); |b|^2, |r|^2
     VT acc[2] = {VT(0), VT(0)};
     if (g) {
-        cluster_rows<VT>(A, s, r0, lo, cnt, GlobalX<VT>{g}, [&](int row, VT v) {
+        product(GlobalX<VT>{g}, [&](int row, VT v) {
+            const int li = row - r0 - lo;
             const VT b_i = bv[row];
             const VT ri = b_i - v;
-            r[row - r0 - lo] = ri;
-            x[row] = g[row];
+            r[li] = ri;
+            x[li] = g[row];
             acc[0] += b_i * b_i;
             acc[1] += ri * ri;
         });
     } else {
         for (int li = tid; li < cnt; li += T) {
-            const int row = r0 + lo + li;
-            const VT b_i = bv[row];
+            const VT b_i = bv[r0 + lo + li];
             r[li] = b_i;
-            x[row] = VT(0);
+            x[li] = VT(0);
             acc[0] += b_i * b_i;
         }
     }
-    cluster_sum<VT, 2>(acc, red, partB, rank, ctas);
+    if (jacobi)
+        for (int li = tid; li < cnt; li += T) dv[li] = dinv[r0 + lo + li];
+    cluster_sum<VT, 2>(acc, red, partB, rank, ctas);   // (its barriers also order the shared stores above)
     const VT bb = acc[0];
     VT rr = g ? acc[1] : bb;
     const VT thr = tol * tol * bb;
     int32_t status = ST_RUNNING;
     int32_t it = 0;
     if ((a.abs_zero_test && bb < tol * tol) || bb == VT(0)) {
-        for (int li = tid; li < cnt; li += T) x[r0 + lo + li] = VT(0);
+        for (int li = tid; li < cnt; li += T) x[li] = VT(0);
         status = CMCG_SOLVE_ZERO_RHS;
     } else if (!finite_(rr) || !finite_(bb)) {
         status = CMCG_SOLVE_NON_FINITE;
@@ -152,7 +198,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT,
         VT rzv[1] = {VT(0)};
         for (int li = tid; li < cnt; li += T) {
             const VT ri = r[li];
-            const VT zi = dinv ? dinv[r0 + lo + li] * ri : ri;
+            const VT zi = jacobi ? dv[li] * ri : ri;
             p[li] = zi;
             rzv[0] += ri * zi;
         }
@@ -164,7 +210,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT,
             if (it >= maxit) { status = CMCG_SOLVE_MAX_ITER; break; }
             cl.sync();   // p of every CTA written
             VT pq[1] = {VT(0)};
-            cluster_rows<VT>(A, s, r0, lo, cnt, ClusterP<VT>{p, r0, c.lg, rank}, [&](int row, VT v) {
+            product(ClusterP<VT>{p, r0, c.lg, rank}, [&](int row, VT v) {
                 const int li = row - r0 - lo;
                 q[li] = v;
                 pq[0] += p[li] * v;
@@ -175,11 +221,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT,
             if (!(pq[0] > VT(0))) { status = CMCG_SOLVE_BREAKDOWN; break; }
             VT s2[2] = {VT(0), VT(0)};
             for (int li = tid; li < cnt; li += T) {
-                const int row = r0 + lo + li;
-                x[row] += alpha * p[li];
+                x[li] += alpha * p[li];
                 const VT ri = r[li] - alpha * q[li];
                 r[li] = ri;
-                const VT zi = dinv ? dinv[row] * ri : ri;
+                const VT zi = jacobi ? dv[li] * ri : ri;
                 s2[0] += ri * ri;
                 s2[1] += ri * zi;
             }
@@ -193,12 +238,14 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_cg(SolveArgs<VT,
             rz = rzn;
             for (int li = tid; li < cnt; li += T) {
                 const VT ri = r[li];
-                const VT zi = dinv ? dinv[r0 + lo + li] * ri : ri;
+                const VT zi = jacobi ? dv[li] * ri : ri;
                 p[li] = zi + beta * p[li];
             }
             ++it;
         }
     }
+    VT* xg = a.x + vo;
+    for (int li = tid; li < cnt; li += T) xg[r0 + lo + li] = x[li];
     if (rank == 0 && tid == 0) {
         a.st.it[inst] = it;
         a.st.status[inst] = status;
@@ -217,7 +264,7 @@ int cluster_rows_log2(int64_t max_rows, size_t elem_bytes, size_t smem_limit, in
         const int64_t R = int64_t(1) << lg;
         const int64_t c = (max_rows + R - 1) / R;
         if (c > kClusterMaxCtas) continue;
-        if (3 * static_cast<size_t>(R) * elem_bytes > smem_limit) return 0;
+        if (kClusterVectors * static_cast<size_t>(R) * elem_bytes > smem_limit) return 0;
         *ctas = static_cast<int>(std::max<int64_t>(c, 1));
         return lg;
     }
@@ -225,11 +272,12 @@ int cluster_rows_log2(int64_t max_rows, size_t elem_bytes, size_t smem_limit, in
 }
 
 template <typename VT, typename MT, int FMT>
-cmcg_status cluster_cg_launch(const SolveArgs<VT, MT>& a, int n_inst, int ctas, int rows_log2, int min_resident,
+cmcg_status cluster_cg_launch(const SolveArgs<VT, MT>& a, int n_inst, int ctas, int rows_log2, int nd, int min_resident,
                               cudaStream_t st, bool* launched) {
     *launched = false;
-    const auto kern = k_cluster_cg<VT, MT, FMT>;
-    const size_t smem = 3 * sizeof(VT) * (size_t(1) << rows_log2);
+    const auto kern = nd == 5 ? k_cluster_cg<VT, MT, FMT, 5> : nd == 7 ? k_cluster_cg<VT, MT, FMT, 7>
+                                                                        : k_cluster_cg<VT, MT, FMT, 0>;
+    const size_t smem = kClusterVectors * sizeof(VT) * (size_t(1) << rows_log2);
     CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     cudaLaunchConfig_t cfg = {};
@@ -257,8 +305,8 @@ cmcg_status cluster_cg_launch(const SolveArgs<VT, MT>& a, int n_inst, int ctas, 
 }
 
 #define CMCG_CLUSTER_INSTANTIATE(VT, MT, FMT)                                                                    \
-    template cmcg_status cluster_cg_launch<VT, MT, FMT>(const SolveArgs<VT, MT>&, int, int, int, int, cudaStream_t, \
-                                                        bool*);
+    template cmcg_status cluster_cg_launch<VT, MT, FMT>(const SolveArgs<VT, MT>&, int, int, int, int, int,   \
+                                                        cudaStream_t, bool*);
 #define CMCG_CLUSTER_FORMATS(VT, MT)           \
     CMCG_CLUSTER_INSTANTIATE(VT, MT, CMCG_CSR) \
     CMCG_CLUSTER_INSTANTIATE(VT, MT, CMCG_ELLPACK)

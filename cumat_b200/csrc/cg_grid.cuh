@@ -271,7 +271,7 @@ __device__ __forceinline__ void seg_rows_vec(int r0, int r1, const void* const (
 constexpr int kCoopMaxInst = 16;
 constexpr int kCoopThreads = 1024;
 constexpr int kCoopMaxSegs = 32;   // segments one CTA may own (cached in shared memory)
-constexpr int kCoopMaxRows = 1 << 19;   // largest system for which the cooperative launch is chosen
+constexpr int kCoopMaxRows = 1 << 15;   // largest system for which the cooperative launch is chosen (larger: graph loop faster)
 
 template <typename VT, typename MT, int FMT>
 cmcg_status coop_cg_occupancy(int* ctas_per_sm);

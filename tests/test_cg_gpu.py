@@ -767,12 +767,12 @@ def test_host_loop_matches_graph_loop(cuda, monkeypatch, kind, cap):
 
 
 def test_cooperative_solve_forced_on_large_system(cuda, monkeypatch):
-    # systems above 2^19 rows take the graph loop unless CUMAT_CG_COOP=2; the
+    # systems above 2^15 rows take the graph loop unless CUMAT_CG_COOP=2; the
     # cooperative launch stages each CTA's window of p (its rows plus the
     # columns they reach) in shared memory and must agree with the graph loop
     m = cm()
     pr = P.poisson2d(760, 1)
-    assert pr.n > (1 << 19)
+    assert pr.n > (1 << 15)
     A = _matrix(pr)
     b = torch.from_numpy(pr.b).to(cuda)
     monkeypatch.setenv("CUMAT_CG_COOP", "0")

@@ -1,6 +1,7 @@
-"""The cluster solve of the grid path: systems of 16,385 .. 262,144 rows (FP32
-vectors; 131,072 with FP64) solved by one thread-block cluster each, p / q / r
-in the cluster's shared memory, scalars summed across the cluster's CTAs.
+"""The cluster solve of the grid path: systems of 16,385 .. 131,072 rows (FP32
+vectors; 65,536 with FP64) solved by one thread-block cluster each, p / q / r /
+x / 1/diag in the cluster's shared memory, scalars summed across the cluster's
+CTAs, the values read in the diagonal layout (stencils) or the sliced layout.
 Compared with the oracle's CG (reference cuMat/src/ConjugateGradient.h:123-206:
 iteration counts within +-2, the same statuses) and with the graph loop of the
 grid path on the same inputs."""
@@ -41,13 +42,16 @@ def _graph_solve(m, monkeypatch, A, b, tol, guess=None, max_iter=-1):
     return x.cpu().numpy(), cg.system_stats()
 
 
-@pytest.mark.parametrize("fmt", ["csr", "ell"])
+@pytest.mark.parametrize("fmt", ["csr", "csr_sliced", "ell"])
 def test_cluster_fp32_poisson_vs_oracle_and_graph(cuda, monkeypatch, fmt):
     # 2D Poisson 200^2 (40,000 rows: clusters of 10 CTAs x 4096 rows), FP32
-    # Jacobi-CG to 1e-6: one cluster launch + the finaliser
+    # Jacobi-CG to 1e-6: one cluster launch + the finaliser; the CSR pattern
+    # is read in the diagonal layout, or (CUMAT_CG_DIA=0) the sliced layout
     m = cm()
+    if fmt == "csr_sliced":
+        monkeypatch.setenv("CUMAT_CG_DIA", "0")
     pr = P.poisson2d(200, 1)
-    A = _csr(m, pr, fmt=fmt)
+    A = _csr(m, pr, fmt="ell" if fmt == "ell" else "csr")
     b = torch.from_numpy(pr.b).to(cuda)
     cg = m.ConjugateGradient(A).setTolerance(1e-6)
     cg.solve(b)
