@@ -715,7 +715,9 @@ def run_ours(args):
                          "dram_frac": round(traffic / (ms / 1e3) / 1e9 / hbm_peak, 4),
                          "dram_peak_gbs": hbm_peak, "dram_peak_source": peak_src,
                          "model_speedup": round(alg / (ms / 1e3) / 1e9 / hbm_peak, 3),
-                         "ncu_l1_pipe_pct_by_tier": {"1024": 54.9, "512": 32.8, "256": 19.6},
+                         # l1tex__data_pipe_lsu_wavefronts pct of peak per CTA tier, from the
+                         # k_mixed_fast ncu capture of the first 512 systems (--profile-small)
+                         "ncu_l1_pipe_pct_by_tier": {"1024": 54.5, "512": 32.7, "256": 19.3},
                          "note": "achieved = L1-pipe model bytes (60 B per row and inner iteration) / time; traffic = "
                                  "DRAM bytes per launch scaled from an ncu capture; model_speedup = HBM streaming "
                                  "model time / measured time"},

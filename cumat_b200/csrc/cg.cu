@@ -1964,11 +1964,21 @@ cmcg_status ensure_state(cmcg_solver s, int32_t n_inst) {
 }
 
 // smem_ok: a shared-memory-resident persistent kernel exists for the solve
-int32_t choose_path(cmcg_solver s, int32_t n_inst, bool smem_ok) {
+// systems above this size are solved faster by a cluster of CTAs than by one
+// CTA, when there are few of them
+constexpr int32_t kClusterMinRows = 4096;
+
+// cluster_ok: the solve has a cluster form (plain solves; refined solves do not)
+int32_t choose_path(cmcg_solver s, int32_t n_inst, bool smem_ok, bool cluster_ok = false) {
     if (s->path != CMCG_PATH_AUTO) return s->path;
     const int sms = s->A->pat->ctx->sm_count;
     // many independent systems of moderate size: one CTA per system
     if (s->max_sys_rows <= 65536 && n_inst >= sms) return CMCG_PATH_PERSISTENT;
+    // a few systems above kClusterMinRows rows: one thread-block cluster each
+    // (the grid path's cluster solve, which falls back to the other grid loops
+    // where it does not apply)
+    if (cluster_ok && s->cluster && s->max_sys_rows > kClusterMinRows && n_inst <= sms / kClusterMaxCtas)
+        return CMCG_PATH_GRID;
     // a few systems that fit in shared memory: one CTA each still beats the
     // grid path's per-iteration launches (2D Poisson 100^2, one system:
     // 9.5 us vs 18.7 us per iteration on the B200)
@@ -2452,12 +2462,11 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     return CMCG_OK;
 }
 
-// One thread-block cluster per instance (cg_cluster.cu), when every system
-// is larger than one CTA solves (kClusterMinRows) yet its p, q and r fit the
-// shared memory of at most kClusterMaxCtas CTAs, and all instances' clusters
-// can be resident at once. *done = false leaves the solve to the cooperative
-// launch or the graph loop.
-constexpr int32_t kClusterMinRows = 16384;
+// One thread-block cluster per instance (cg_cluster.cu), when the largest
+// system has more than kClusterMinRows rows yet its vectors fit the shared
+// memory of at most kClusterMaxCtas CTAs, and all instances' clusters can be
+// resident at once. *done = false leaves the solve to the cooperative launch
+// or the graph loop.
 template <typename VT, typename MT, int FMT>
 cmcg_status run_cluster(cmcg_solver s, SolveArgs<VT, MT>& a, bool* done) {
     *done = false;
@@ -2569,7 +2578,7 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
     CMCG_TRY(get_dinv(s, DT<VT>::id, &dinv));
     CMCG_TRY(ensure_sell_values(s->A));
     const bool smem_ok = (FMT == CMCG_CSR && compact_ok(s)) || (sizeof(VT) == 4 && s->use_smem);
-    const int32_t path = choose_path(s, n_inst, smem_ok);
+    const int32_t path = choose_path(s, n_inst, smem_ok, /*cluster_ok=*/true);
     if (log_on(2))
         log_msg(2, "solve: %d instances of up to %d rows, %s vectors, %s path", n_inst, s->max_sys_rows,
                 sizeof(VT) == 8 ? "FP64" : "FP32", path == CMCG_PATH_GRID ? "grid" : "persistent");

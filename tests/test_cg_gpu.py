@@ -736,6 +736,7 @@ def test_host_loop_matches_graph_loop(cuda, monkeypatch, kind, cap):
     # an iteration cap
     m = cm()
     monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    monkeypatch.setenv("CUMAT_CG_CLUSTER", "0")
     p3 = P.fv3d(24, 1.0, 7)
     pat = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
     A64 = m.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))

@@ -143,3 +143,26 @@ def test_cluster_guess_cap_zero_rhs_identity(cuda, monkeypatch):
     _, it_i, _ = O.cg_csr(pr.n, pr.row_ptr, pr.col, pr.val, pr.b, 1e-6, -1, 0)
     assert cg4.system_stats()["status"][0] == 0 and abs(cg4.iterations() - int(it_i[0])) <= 2
     assert m.Context.current().device_errors() == 0
+
+
+def test_few_small_systems_take_the_cluster(cuda, monkeypatch):
+    # one 100^2 Poisson system (10,000 rows: 10 CTAs x 1024 rows): the
+    # automatic path gives a few systems above 4096 rows to the cluster solve
+    # (one launch + the finaliser) instead of one CTA each; same result as the
+    # one-CTA solver within the FP32 recursion's rounding
+    m = cm()
+    pr = P.poisson2d(100, 4)
+    A = _csr(m, pr)
+    b = torch.from_numpy(pr.b).to(cuda)
+    cg = m.ConjugateGradient(A).setTolerance(1e-6)
+    cg.solve(b)
+    before = m.launch_count()
+    x = cg.solve(b).cpu().numpy()
+    assert m.launch_count() - before == 2
+    st = cg.system_stats()
+    _, it_o, _ = O.cg_csr(pr.n, pr.row_ptr, pr.col, pr.val, pr.b, 1e-6, -1, 1)
+    assert st["status"][0] == 0 and abs(int(st["iterations"][0]) - int(it_o[0])) <= 2
+    monkeypatch.setenv("CUMAT_CG_CLUSTER", "0")
+    cg1 = m.ConjugateGradient(A).setTolerance(1e-6)
+    x1 = cg1.solve(b).cpu().numpy()
+    assert np.linalg.norm(x - x1) / np.linalg.norm(x1) < 1e-4
