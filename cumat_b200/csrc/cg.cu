@@ -898,6 +898,35 @@ __device__ __forceinline__ void p_quad(const VT* __restrict__ p, int c, int lo, 
     }
 }
 
+// p_k of the grid path, formed where it is read: p_k[j] = z_j + beta p_{k-1}[j]
+// with z = M^-1 r (r and beta of iteration k, p_{k-1} the other p buffer), the
+// expression of the former p-update kernel; the product forms it for its own
+// rows (and stores them) and for every entry it gathers, so the iteration needs
+// no p-update launch. Iteration 0 reads beta = 0 and a zeroed p_{-1}.
+template <typename VT>
+struct PNext {
+    const VT* __restrict__ r;
+    const VT* __restrict__ dinv;   // null: identity
+    const VT* __restrict__ pin;    // p_{k-1}
+    VT beta;
+    __device__ __forceinline__ VT form(VT d, VT ri, VT pi) const {
+        const VT z = dinv ? d * ri : ri;
+        return z + beta * pi;
+    }
+    __device__ __forceinline__ VT operator()(int c) const {
+        return form(dinv ? __ldg(dinv + c) : VT(1), __ldg(r + c), __ldg(pin + c));
+    }
+    // entries c .. c + 3, indices clamped into [lo, hi] (see p_quad)
+    __device__ __forceinline__ void quad(int c, int lo, int hi, VT (&o)[4]) const {
+        VT rq[4], pq[4], dq[4] = {VT(1), VT(1), VT(1), VT(1)};
+        p_quad(r, c, lo, hi, rq);
+        p_quad(pin, c, lo, hi, pq);
+        if (dinv) p_quad(dinv, c, lo, hi, dq);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) o[q] = form(dq[q], rq[q], pq[q]);
+    }
+};
+
 // q[i] = sum_d v_d[i] p[i + off_d] for the rows [r0, r1) of one system (global
 // rows sr0 .. send - 1, r0 - sr0 a multiple of 4; v points at the system's
 // first value), diagonals in ascending offset order, the row's CSR order, with
@@ -908,23 +937,24 @@ __device__ __forceinline__ void p_quad(const VT* __restrict__ p, int c, int lo, 
 // rows match too; the values of a diagonal for its four rows are one 16-byte
 // (8-byte for BF16) streaming load. p indices are clamped into the system,
 // where a zero value (or, past the system's end, a row that is not emitted)
-// meets them. The gathers: a thread loads its own four p entries (offset 0)
-// as one quad; offsets -1 and +1 take three of them and one entry from the
-// neighbouring lane (a scalar load at the warp's edges); other offsets load a
-// quad each. The entries are the clamped ones in every case, so the sums do
-// not depend on how they were loaded.
+// meets them. p is p_k formed from r, M^-1 and p_{k-1} (PNext). The gathers:
+// a thread forms its own four p entries (offset 0) from one quad of each
+// input; offsets -1 and +1 take three of them and one entry from the
+// neighbouring lane (formed from scalar loads at the warp's edges); other
+// offsets form a quad each. The entries are the clamped ones in every case,
+// so the sums do not depend on how they were loaded.
 // UNIT: the middle diagonal is offset 0 with every value 1 and is not loaded.
 // emit(global row, value, p[row]).
 template <typename VT, typename MT, int ND, bool UNIT, typename F>
 __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int (&off)[ND], int sr0, int send, int r0,
-                                             int r1, const VT* __restrict__ p, F&& emit) {
+                                             int r1, const PNext<VT>& p, F&& emit) {
     const int lane = threadIdx.x & 31;
     // the loop bound is the same for the whole CTA, so every lane takes part
     // in the shuffles
     for (int base = r0; base < r1; base += 4 * kTile) {
         const int ib = base + 4 * threadIdx.x;
         VT own[4];
-        p_quad(p, ib, sr0, send - 1, own);   // (ib >= sr0: only the upper clamp acts)
+        p.quad(ib, sr0, send - 1, own);   // (ib >= sr0: only the upper clamp acts)
         const VT from_prev = __shfl_up_sync(FULL, own[3], 1);     // p[ib - 1] of lane - 1's quad
         const VT from_next = __shfl_down_sync(FULL, own[0], 1);   // p[ib + 4] of lane + 1's quad
         if (ib >= r1) continue;
@@ -953,13 +983,13 @@ __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int
             } else if (o == -1) {
                 // lane >= 1: lane - 1's quad starts at ib - 4 >= r0, so its last
                 // entry is p[ib - 1] itself
-                pv[0] = lane ? from_prev : __ldg(p + max(ib - 1, sr0));
+                pv[0] = lane ? from_prev : p(max(ib - 1, sr0));
                 pv[1] = own[0]; pv[2] = own[1]; pv[3] = own[2];
             } else if (o == 1) {
                 pv[0] = own[1]; pv[1] = own[2]; pv[2] = own[3];
-                pv[3] = lane != 31 ? from_next : __ldg(p + min(ib + 4, send - 1));
+                pv[3] = lane != 31 ? from_next : p(min(ib + 4, send - 1));
             } else {
-                p_quad(p, ib + o, sr0, send - 1, pv);
+                p.quad(ib + o, sr0, send - 1, pv);
             }
             if (UNIT && d == ND / 2) {
 #pragma unroll
@@ -1057,7 +1087,8 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init(SolveArgs<V
     }
 }
 
-// init B: zero x of zero-rhs systems; p = M^-1 r and r.z of running systems
+// init B: zero x of zero-rhs systems; r.z, beta = 0 and p_{-1} = 0 of running
+// systems (iteration 0's product forms p_0 = M^-1 r)
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
@@ -1078,7 +1109,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<
         for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
             const VT ri = a.r[vo + i];
             const VT zi = dinv ? dinv[i] * ri : ri;
-            a.p[vo + i] = zi;
+            a.p2[vo + i] = VT(0);   // p_{-1}: iteration 0 forms p_0 = z
             acc[0] += ri * zi;
         }
         block_sum<VT, 1>(acc, red);
@@ -1088,6 +1119,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<
             threadIdx.x == 0) {
             const VT rz = tot[0];
             a.st.rz[g.inst] = rz;
+            a.st.beta[g.inst] = 0.0;
             int32_t status = ST_RUNNING;
             if (!finite_(rz)) status = CMCG_SOLVE_NON_FINITE;
             else if (!(rz > VT(0))) status = CMCG_SOLVE_BREAKDOWN;
@@ -1099,33 +1131,44 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<
     }
 }
 
-// iteration kernel 1: q = A p, p.q -> alpha (ND > 0: the values in the
-// pattern's diagonal layout, ND diagonals per system)
+// p_k of iteration k (the loop's count of finished iterations) lives in p for
+// even k and in p2 for odd k
+template <typename VT, typename MT>
+__device__ __forceinline__ VT* grid_pk(const SolveArgs<VT, MT>& a, int k) { return (k & 1) ? a.p2 : a.p; }
+
+// iteration kernel 1: p_k = M^-1 r + beta p_{k-1} (formed inside the product),
+// q = A p_k, p_k.q -> alpha (ND > 0: the values in the pattern's diagonal
+// layout, ND diagonals per system)
 template <typename VT, typename MT, int FMT, int ND = 0>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
     __shared__ VT red[kTile / 32];
     __shared__ bool last_s;
+    const int k = __ldcg(a.loops);
+    VT* const pk = grid_pk(a, k);
+    const VT* const pprev = grid_pk(a, k + 1);
     CMCG_FOR_SEGMENTS(a) {
         const SegInfo g = seg_info(a, b_, seg_);
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
-        const VT* p = a.p + vo;
+        const PNext<VT> pn{a.r + vo, a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr, pprev + vo,
+                           static_cast<VT>(a.st.beta[g.inst])};
+        VT* pout = pk + vo;
         VT* q = a.q + vo;
         VT acc[1] = {VT(0)};
-        const auto emit = [&](int row, VT v) {
-            __stcs(q + row, v);   // read once, by the update kernel
-            acc[0] += p[row] * v;
+        // q is read once, by the update kernel
+        const auto emit3 = [&](int row, VT qv, VT prow) {
+            pout[row] = prow;
+            __stcs(q + row, qv);
+            acc[0] += prow * qv;
         };
         if constexpr (ND > 0) {
             int off[ND];
             const MT* v = dia_system<MT, ND>(a.dia, b_, g.s, off);
-            dia_rows_seg<VT, MT, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, [&](int row, VT qv, VT prow) {
-                __stcs(q + row, qv);
-                acc[0] += prow * qv;
-            });
+            dia_rows_seg<VT, MT, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, pn, emit3);
         } else {
             const auto A = inst_matrix<MT, FMT>(a.m, b_);
-            cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<VT>{p}, emit);
+            cta_rows4_seg<VT>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, pn,
+                              [&](int row, VT qv) { emit3(row, qv, pn(row)); });
         }
         block_sum<VT, 1>(acc, red);
         VT tot[1];
@@ -1147,7 +1190,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_spmv_pq(SolveArg
     }
 }
 
-// iteration kernel 2: x += alpha p, r -= alpha q, |r|^2, r.z -> convergence, beta
+// iteration kernel 2: x += alpha p_k, r -= alpha q, |r|^2, r.z -> convergence, beta
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_update(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
@@ -1160,7 +1203,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_update(SolveArgs
         const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
         VT acc[2] = {VT(0), VT(0)};
         VT* x = a.x + vo;
-        const VT* p = a.p + vo;
+        const VT* p = grid_pk(a, __ldcg(a.loops)) + vo;
         VT* r = a.r + vo;
         const VT* q = a.q + vo;
         const void* const ptrs[5] = {x + g.r0, p + g.r0, r + g.r0, q + g.r0, dinv ? dinv + g.r0 : nullptr};
@@ -1223,37 +1266,6 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_update(SolveArgs
     }
 }
 
-// iteration kernel 3: p = M^-1 r + beta p
-template <typename VT, typename MT, int FMT>
-__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_pupdate(SolveArgs<VT, MT> a) {
-    CMCG_FOR_SEGMENTS(a) {
-        const SegInfo g = seg_info(a, b_, seg_);
-        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
-        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
-        const VT beta = static_cast<VT>(a.st.beta[g.inst]);
-        const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
-        const VT* r = a.r + vo;
-        VT* p = a.p + vo;
-        const void* const ptrs[3] = {r + g.r0, p + g.r0, dinv ? dinv + g.r0 : nullptr};
-        seg_rows_vec<3>(
-            g.r0, g.r1, ptrs,
-            [&](int i) {
-                V4<VT> R, P, D;
-                R.load(r + i);
-                P.load(p + i);
-                if (dinv) D.load(dinv + i);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) P.v[k] = (dinv ? D.v[k] * R.v[k] : R.v[k]) + beta * P.v[k];
-                P.store(p + i);
-            },
-            [&](int i) {
-                const VT ri = r[i];
-                const VT zi = dinv ? dinv[i] * ri : ri;
-                p[i] = zi + beta * p[i];
-            });
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Grid path, mixed precision with reliable updates (large systems)
 //
@@ -1262,9 +1274,9 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_pupdate(SolveArg
 // layout), FP32 increments xh folded into the FP64 solution x with x += S xh,
 // and the recursive residual replaced by S (b - A x) computed in FP64 with the
 // unscaled outer values whenever it dropped by delta (or looks converged).
-// Per iteration the CUDA graph runs: product + p.q, update + |r|^2 (decides
-// whether to replace), fold, FP64 residual (both no-ops unless a replacement is
-// due), p update, loop condition.
+// Per iteration the CUDA graph runs: p update + product + p.q, update + |r|^2
+// (decides whether to replace), fold, FP64 residual (both no-ops unless a
+// replacement is due), loop condition.
 // ---------------------------------------------------------------------------
 
 template <typename MI, typename MO>
@@ -1300,7 +1312,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_init(GMixArgs<MI
             m.x64[vo + i] = 0.0;
             m.xh[vo + i] = 0.0f;
             a.r[vo + i] = rh;
-            a.p[vo + i] = rh;
+            a.p2[vo + i] = 0.0f;   // p_{-1}: iteration 0 forms p_0 = r
             acc[0] += bi * bi;
             acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
         }
@@ -1315,6 +1327,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_init(GMixArgs<MI
             a.st.bb[g.inst] = bb;
             a.st.rr[g.inst] = bb;
             a.st.rz[g.inst] = rz;
+            a.st.beta[g.inst] = 0.0;
             a.st.rmax[g.inst] = rz;
             a.st.goal[g.inst] = static_cast<double>(static_cast<float>(thr / bb) * rz);
             a.st.it[g.inst] = 0;
@@ -1341,7 +1354,8 @@ __device__ __forceinline__ bool gmix_tail_status(int32_t st) {
     return st == ST_RUNNING || st == CMCG_SOLVE_BREAKDOWN || st == CMCG_SOLVE_NON_FINITE;
 }
 
-// product q = (S A S) p and p.q -> alpha (ND > 0: the scaled values in the
+// p_k = r + beta p_{k-1} (formed inside the product), q = (S A S) p_k and
+// p_k.q -> alpha (ND > 0: the scaled values in the
 // pattern's diagonal layout, the unit middle diagonal not loaded where the
 // system's flag says so)
 template <typename MI, typename MO, int ND = 0>
@@ -1349,30 +1363,34 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_spmv(GMixArgs<MI
     const SolveArgs<float, MI>& a = m.g;
     __shared__ float red[kTile / 32];
     __shared__ bool last_s;
+    const int k = __ldcg(a.loops);
+    float* const pk = grid_pk(a, k);
+    const float* const pprev = grid_pk(a, k + 1);
     CMCG_FOR_SEGMENTS(a) {
         const SegInfo g = seg_info(a, b_, seg_);
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
-        const float* p = a.p + vo;
+        // the scaled system needs no preconditioner: p_k = r + beta p_{k-1}
+        const PNext<float> pn{a.r + vo, nullptr, pprev + vo, static_cast<float>(a.st.beta[g.inst])};
+        float* pout = pk + vo;
         float* q = a.q + vo;
         float acc[1] = {0.0f};
-        const auto emit = [&](int row, float v) {
-            __stcs(q + row, v);   // read once, by the update kernel
-            acc[0] += p[row] * v;
+        // q is read once, by the update kernel
+        const auto emit3 = [&](int row, float qv, float prow) {
+            pout[row] = prow;
+            __stcs(q + row, qv);
+            acc[0] += prow * qv;
         };
         if constexpr (ND > 0) {
             int off[ND];
             const MI* v = dia_system<MI, ND>(a.dia, b_, g.s, off);
             const bool unit = a.dia.unit && __ldg(a.dia.unit + (a.dia.mb == 1 ? 0 : b_ * a.n_sys) + g.s);
-            const auto emit3 = [&](int row, float qv, float prow) {
-                __stcs(q + row, qv);
-                acc[0] += prow * qv;
-            };
-            if (unit) dia_rows_seg<float, MI, ND, true>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit3);
-            else dia_rows_seg<float, MI, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, p, emit3);
+            if (unit) dia_rows_seg<float, MI, ND, true>(v, off, g.sr0, g.send, g.r0, g.r1, pn, emit3);
+            else dia_rows_seg<float, MI, ND, false>(v, off, g.sr0, g.send, g.r0, g.r1, pn, emit3);
         } else {
             const auto A = inst_matrix<MI, CMCG_CSR>(a.m, b_);
-            cta_rows4_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, GlobalX<float>{p}, emit);
+            cta_rows4_seg<float>(A, g.s, g.sr0, g.r0 - g.sr0, g.r1 - g.r0, pn,
+                                 [&](int row, float qv) { emit3(row, qv, pn(row)); });
         }
         block_sum<float, 1>(acc, red);
         float tot[1];
@@ -1416,7 +1434,7 @@ __device__ __forceinline__ bool bf16_condition_ok(float ratio, int32_t k) {
     return s * s <= kBf16CondLimit;
 }
 
-// xh += alpha p, r -= alpha q, |r|^2 -> replacement decision or beta
+// xh += alpha p_k, r -= alpha q, |r|^2 -> replacement decision or beta
 template <typename MI, typename MO>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_update(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
@@ -1429,7 +1447,7 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_update(GMixArgs<
         const float alpha = static_cast<float>(a.st.alpha[g.inst]);
         float acc[1] = {0.0f};
         float* xh = m.xh + vo;
-        const float* p = a.p + vo;
+        const float* p = grid_pk(a, __ldcg(a.loops)) + vo;
         float* r = a.r + vo;
         const float* q = a.q + vo;
         const void* const ptrs[4] = {xh + g.r0, p + g.r0, r + g.r0, q + g.r0};
@@ -1574,33 +1592,13 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_residual(GMixArg
     }
 }
 
-// p = r + beta p
-template <typename MI, typename MO>
-__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_pupdate(GMixArgs<MI, MO> m) {
-    const SolveArgs<float, MI>& a = m.g;
-    CMCG_FOR_SEGMENTS(a) {
-        const SegInfo g = seg_info(a, b_, seg_);
-        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
-        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
-        const float beta = static_cast<float>(a.st.beta[g.inst]);
-        const float* r = a.r + vo;
-        float* p = a.p + vo;
-        const void* const ptrs[2] = {r + g.r0, p + g.r0};
-        seg_rows_vec<2>(
-            g.r0, g.r1, ptrs,
-            [&](int i) {
-                V4<float> R, P;
-                R.load(r + i);
-                P.load(p + i);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) P.v[k] = R.v[k] + beta * P.v[k];
-                P.store(p + i);
-            },
-            [&](int i) { p[i] = r[i] + beta * p[i]; });
-    }
-}
 
-// loop condition of the graph's WHILE node (one thread)
+// the host-driven loop's count of finished iterations (the graph's condition
+// kernel keeps it there; the products read its parity)
+__global__ void k_loop_step(int32_t* loops) { ++*loops; }
+
+// loop condition of the graph's WHILE node (one thread); counts the finished
+// iterations
 __global__ void k_grid_cond(const int32_t* active, int32_t* loops, int32_t cap, cudaGraphConditionalHandle h) {
     const int32_t l = ++(*loops);
     const unsigned go = (*reinterpret_cast<const volatile int32_t*>(active) > 0 && l < cap) ? 1u : 0u;
@@ -2405,11 +2403,11 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
                 k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
             }
             k_grid_update<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
-            k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+            k_loop_step<<<1, 1, 0, st>>>(a.loops);
         });
     }
 
-    // graph with a WHILE node over the three iteration kernels; rebuilt when any
+    // graph with a WHILE node over the two iteration kernels; rebuilt when any
     // kernel argument changes
     std::vector<char> key(sizeof(a) + sizeof(int) * 2);
     {
@@ -2447,7 +2445,6 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
             k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
         }
         k_grid_update<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
-        k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
         k_grid_cond<<<1, 1, 0, cs>>>(a.active, a.loops, a.loop_cap, h);
         cudaGraph_t captured = nullptr;
         cudaError_t ce = cudaStreamEndCapture(cs, &captured);
@@ -2456,7 +2453,7 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
         s->gkey = key;
     }
     CMCG_CUDA(cudaGraphLaunch(s->gexec, st));
-    // kernels inside the graph: 4 per executed iteration (counted as launched
+    // kernels inside the graph: 3 per executed iteration (counted as launched
     // by the graph, not by the host)
     count_launch(1);
     return CMCG_OK;
@@ -2599,6 +2596,7 @@ cmcg_status solve_t(cmcg_solver s, const VT* b, int32_t b_b, const VT* guess, VT
         VT* w = static_cast<VT*>(s->vec_ws);
         const size_t nv = p->rows * static_cast<size_t>(ob);
         a.r = w; a.p = w + nv; a.q = w + 2 * nv; a.x = w + 3 * nv;
+        a.p2 = w + 4 * nv;   // (the graph loop's second p buffer, the cooperative launch's p_alt)
         a.b = b; a.b_b = b_b; a.guess = guess; a.g_b = ob;
         bool done = false;
         CMCG_TRY((run_cluster<VT, MT, FMT>(s, a, &done)));
@@ -2912,7 +2910,7 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     if (Ao != s->A) CMCG_TRY(ensure_sell_values(Ao));
     CMCG_TRY(ensure_mix(s));
     const size_t nv = static_cast<size_t>(p->rows) * ob, nb = static_cast<size_t>(p->rows) * b_b;
-    const size_t need = (nv + nb) * sizeof(double) + 4 * nv * sizeof(float) + 512;
+    const size_t need = (nv + nb) * sizeof(double) + 5 * nv * sizeof(float) + 512;
     CMCG_TRY(ensure_buffer(&s->ref_ws, &s->ref_ws_bytes, need));
     double* x64 = static_cast<double*>(s->ref_ws);
     double* b64 = x64 + nv;
@@ -2925,7 +2923,7 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
     m.g.m.sell_vals = static_cast<const MI*>(s->mix_vals);
     m.g.m.sell_vstride = s->mix_stride;
     m.g.b_b = b_b;
-    m.g.r = f; m.g.p = f + nv; m.g.q = f + 2 * nv;
+    m.g.r = f; m.g.p = f + nv; m.g.q = f + 2 * nv; m.g.p2 = f + 4 * nv;   // (f + 3 nv: xh)
     m.g.part1 = reinterpret_cast<float*>(p1 + 2 * items);
     m.g.part2 = m.g.part1 + items;
     m.g.abs_zero_test = 0;
@@ -2969,7 +2967,7 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
             k_gmix_update<MI, MO><<<grid, kTile, 0, st>>>(m);
             k_gmix_fold<MI, MO, false><<<grid, kTile, 0, st>>>(m);
             k_gmix_residual<MI, MO, false><<<grid, kTile, 0, st>>>(m);
-            k_gmix_pupdate<MI, MO><<<grid, kTile, 0, st>>>(m);
+            k_loop_step<<<1, 1, 0, st>>>(m.g.loops);
         }));
     } else {
         std::vector<char> key(sizeof(m) + sizeof(int) * 2);
@@ -3006,7 +3004,6 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
             k_gmix_update<MI, MO><<<grid, kTile, 0, cs>>>(m);
             k_gmix_fold<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
             k_gmix_residual<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
-            k_gmix_pupdate<MI, MO><<<grid, kTile, 0, cs>>>(m);
             k_grid_cond<<<1, 1, 0, cs>>>(m.g.active, m.g.loops, m.g.loop_cap, h);
             cudaGraph_t captured = nullptr;
             cudaError_t ce = cudaStreamEndCapture(cs, &captured);

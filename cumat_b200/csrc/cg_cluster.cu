@@ -16,6 +16,9 @@
 // early-outs, statuses and iteration count are those of the one-CTA solver
 // (reference cuMat/src/ConjugateGradient.h:123-206).
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include <cooperative_groups.h>
 
@@ -278,8 +281,8 @@ cmcg_status cluster_cg_launch(const SolveArgs<VT, MT>& a, int n_inst, int ctas, 
     const auto kern = nd == 5 ? k_cluster_cg<VT, MT, FMT, 5> : nd == 7 ? k_cluster_cg<VT, MT, FMT, 7>
                                                                         : k_cluster_cg<VT, MT, FMT, 0>;
     const size_t smem = kClusterVectors * sizeof(VT) * (size_t(1) << rows_log2);
-    CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int device = 0;
+    CMCG_CUDA(cudaGetDevice(&device));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(n_inst) * static_cast<unsigned>(ctas));
     cfg.blockDim = dim3(kClusterThreads);
@@ -292,10 +295,28 @@ cmcg_status cluster_cg_launch(const SolveArgs<VT, MT>& a, int n_inst, int ctas, 
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    int resident = 0;
-    if (cudaOccupancyMaxActiveClusters(&resident, kern, &cfg) != cudaSuccess) {
-        (void)cudaGetLastError();   // (a cluster shape the device cannot place: leave the solve to the others)
-        return CMCG_OK;
+    // (the shared-memory attribute belongs to the kernel, not to the shape:
+    // set on every launch)
+    CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    CMCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    // the resident-cluster count of a (device, kernel, shape) is looked up once
+    // per process (the occupancy query costs more than a small solve)
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, int, size_t>, int> resident_of;
+    const auto key = std::make_tuple(device, reinterpret_cast<const void*>(kern), ctas, smem);
+    int resident = -1;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = resident_of.find(key);
+        if (it != resident_of.end()) resident = it->second;
+    }
+    if (resident < 0) {
+        if (cudaOccupancyMaxActiveClusters(&resident, kern, &cfg) != cudaSuccess) {
+            (void)cudaGetLastError();   // (a cluster shape the device cannot place: leave the solve to the others)
+            resident = 0;
+        }
+        std::lock_guard<std::mutex> lock(mu);
+        resident_of[key] = resident;
     }
     if (resident < min_resident) return CMCG_OK;
     const ClusterArgs c{ctas, rows_log2};

@@ -143,6 +143,7 @@ struct SolveArgs {
     VT* x;
     VT* r;
     VT* p;
+    VT* p2;        // graph loop: p_k is in p for even k, in p2 for odd k
     VT* q;
     double tol;
     int64_t max_iter;              // < 0: 2 * rows of the system
