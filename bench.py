@@ -470,10 +470,12 @@ def cg_config2(cm, torch, dev, stream, hbm_peak):
 def cg_poisson10000(cm, torch, dev, stream, hbm_peak):
     """The grid path's iteration on the 10000^2 Poisson matrix (10^8 rows, FP32,
     Jacobi; every vector 400 MB, far above L2): the per-iteration time is the
-    difference of two solves capped at 40 and 10 iterations, over 30. The
-    diagonal-layout iteration streams 68 B per row in two kernels: p update +
-    product + p.q (5 values, r, 1/diag, p_{k-1} read, p_k and q written: 40 B),
-    x / r update + |r|^2 + r.z (x, p_k, r, q, 1/diag read, x, r written: 28 B)."""
+    difference of two solves capped at 40 and 10 iterations, over 30. At this
+    size (vectors far above L2) the product reads p as stored and a separate
+    kernel updates it; the diagonal-layout iteration streams 72 B per row:
+    product + p.q (5 values, p, q: 28 B), x / r update + |r|^2 + r.z (x, p, r,
+    q, 1/diag read, x, r written: 28 B), p update (r, p, 1/diag read, p
+    written: 16 B)."""
     from cumat_b200 import problems as P
     pr = P.poisson2d(10000, 1)
     A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
@@ -487,7 +489,7 @@ def cg_poisson10000(cm, torch, dev, stream, hbm_peak):
         its = cg.iterations()
         del cg
     us = (t[40] - t[10]) * 1e3 / 30
-    byt = 68.0 * A.rows
+    byt = 72.0 * A.rows
     out = {"rows": A.rows, "us_per_iter": round(us, 2), "gbs_model": round(byt / us / 1e3, 1),
            "frac_model": round(byt / us / 1e3 / hbm_peak, 3), "iterations_checked": int(its)}
     del A, b, x

@@ -927,6 +927,15 @@ struct PNext {
     }
 };
 
+// p_k read as stored (the separate p-update kernel formed it): the product's
+// source when the vectors do not stay in L2 (see fuse_p_update)
+template <typename VT>
+struct PDirect {
+    const VT* __restrict__ p;
+    __device__ __forceinline__ VT operator()(int c) const { return __ldg(p + c); }
+    __device__ __forceinline__ void quad(int c, int lo, int hi, VT (&o)[4]) const { p_quad(p, c, lo, hi, o); }
+};
+
 // q[i] = sum_d v_d[i] p[i + off_d] for the rows [r0, r1) of one system (global
 // rows sr0 .. send - 1, r0 - sr0 a multiple of 4; v points at the system's
 // first value), diagonals in ascending offset order, the row's CSR order, with
@@ -937,7 +946,8 @@ struct PNext {
 // rows match too; the values of a diagonal for its four rows are one 16-byte
 // (8-byte for BF16) streaming load. p indices are clamped into the system,
 // where a zero value (or, past the system's end, a row that is not emitted)
-// meets them. p is p_k formed from r, M^-1 and p_{k-1} (PNext). The gathers:
+// meets them. p is p_k: formed from r, M^-1 and p_{k-1} (PNext) or read as
+// stored (PDirect). The gathers:
 // a thread forms its own four p entries (offset 0) from one quad of each
 // input; offsets -1 and +1 take three of them and one entry from the
 // neighbouring lane (formed from scalar loads at the warp's edges); other
@@ -945,9 +955,9 @@ struct PNext {
 // so the sums do not depend on how they were loaded.
 // UNIT: the middle diagonal is offset 0 with every value 1 and is not loaded.
 // emit(global row, value, p[row]).
-template <typename VT, typename MT, int ND, bool UNIT, typename F>
+template <typename VT, typename MT, int ND, bool UNIT, typename PS, typename F>
 __device__ __forceinline__ void dia_rows_seg(const MT* __restrict__ v, const int (&off)[ND], int sr0, int send, int r0,
-                                             int r1, const PNext<VT>& p, F&& emit) {
+                                             int r1, const PS& p, F&& emit) {
     const int lane = threadIdx.x & 31;
     // the loop bound is the same for the whole CTA, so every lane takes part
     // in the shuffles
@@ -1087,8 +1097,8 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init(SolveArgs<V
     }
 }
 
-// init B: zero x of zero-rhs systems; r.z, beta = 0 and p_{-1} = 0 of running
-// systems (iteration 0's product forms p_0 = M^-1 r)
+// init B: zero x of zero-rhs systems; r.z, beta = 0 and p_{-1} = 0 (or, when
+// the product reads p as stored, p_0 = M^-1 r) of running systems
 template <typename VT, typename MT, int FMT>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<VT, MT> a) {
     __shared__ VT red[2 * (kTile / 32)];
@@ -1109,7 +1119,8 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_init2(SolveArgs<
         for (int i = g.r0 + threadIdx.x; i < g.r1; i += kTile) {
             const VT ri = a.r[vo + i];
             const VT zi = dinv ? dinv[i] * ri : ri;
-            a.p2[vo + i] = VT(0);   // p_{-1}: iteration 0 forms p_0 = z
+            if (a.p2 != a.p) a.p2[vo + i] = VT(0);   // p_{-1}: iteration 0's product forms p_0 = z
+            else a.p[vo + i] = zi;                    // p_0 (the product reads p as stored)
             acc[0] += ri * zi;
         }
         block_sum<VT, 1>(acc, red);
@@ -1139,7 +1150,7 @@ __device__ __forceinline__ VT* grid_pk(const SolveArgs<VT, MT>& a, int k) { retu
 // iteration kernel 1: p_k = M^-1 r + beta p_{k-1} (formed inside the product),
 // q = A p_k, p_k.q -> alpha (ND > 0: the values in the pattern's diagonal
 // layout, ND diagonals per system)
-template <typename VT, typename MT, int FMT, int ND = 0>
+template <typename VT, typename MT, int FMT, int ND, bool FUSED>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_spmv_pq(SolveArgs<VT, MT> a) {
     __shared__ VT red[kTile / 32];
     __shared__ bool last_s;
@@ -1150,14 +1161,19 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_spmv_pq(SolveArg
         const SegInfo g = seg_info(a, b_, seg_);
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
-        const PNext<VT> pn{a.r + vo, a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr, pprev + vo,
-                           static_cast<VT>(a.st.beta[g.inst])};
+        using PS = std::conditional_t<FUSED, PNext<VT>, PDirect<VT>>;
+        PS pn;
+        if constexpr (FUSED)
+            pn = PS{a.r + vo, a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr, pprev + vo,
+                    static_cast<VT>(a.st.beta[g.inst])};
+        else
+            pn = PS{pk + vo};
         VT* pout = pk + vo;
         VT* q = a.q + vo;
         VT acc[1] = {VT(0)};
         // q is read once, by the update kernel
         const auto emit3 = [&](int row, VT qv, VT prow) {
-            pout[row] = prow;
+            if constexpr (FUSED) pout[row] = prow;
             __stcs(q + row, qv);
             acc[0] += prow * qv;
         };
@@ -1266,6 +1282,37 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_update(SolveArgs
     }
 }
 
+// iteration kernel 3 where the product does not form p (p2 == p): p = M^-1 r + beta p
+template <typename VT, typename MT, int FMT>
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_pupdate(SolveArgs<VT, MT> a) {
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const VT beta = static_cast<VT>(a.st.beta[g.inst]);
+        const VT* dinv = a.dinv ? a.dinv + (a.dinv_b == 1 ? 0 : vo) : nullptr;
+        const VT* r = a.r + vo;
+        VT* p = a.p + vo;
+        const void* const ptrs[3] = {r + g.r0, p + g.r0, dinv ? dinv + g.r0 : nullptr};
+        seg_rows_vec<3>(
+            g.r0, g.r1, ptrs,
+            [&](int i) {
+                V4<VT> R, P, D;
+                R.load(r + i);
+                P.load(p + i);
+                if (dinv) D.load(dinv + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) P.v[k] = (dinv ? D.v[k] * R.v[k] : R.v[k]) + beta * P.v[k];
+                P.store(p + i);
+            },
+            [&](int i) {
+                const VT ri = r[i];
+                const VT zi = dinv ? dinv[i] * ri : ri;
+                p[i] = zi + beta * p[i];
+            });
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Grid path, mixed precision with reliable updates (large systems)
 //
@@ -1312,7 +1359,8 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_init(GMixArgs<MI
             m.x64[vo + i] = 0.0;
             m.xh[vo + i] = 0.0f;
             a.r[vo + i] = rh;
-            a.p2[vo + i] = 0.0f;   // p_{-1}: iteration 0 forms p_0 = r
+            if (a.p2 != a.p) a.p2[vo + i] = 0.0f;   // p_{-1}: iteration 0's product forms p_0 = r
+            else a.p[vo + i] = rh;                   // p_0 (the product reads p as stored)
             acc[0] += bi * bi;
             acc[1] += static_cast<double>(rh) * static_cast<double>(rh);
         }
@@ -1358,7 +1406,7 @@ __device__ __forceinline__ bool gmix_tail_status(int32_t st) {
 // p_k.q -> alpha (ND > 0: the scaled values in the
 // pattern's diagonal layout, the unit middle diagonal not loaded where the
 // system's flag says so)
-template <typename MI, typename MO, int ND = 0>
+template <typename MI, typename MO, int ND, bool FUSED>
 __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_spmv(GMixArgs<MI, MO> m) {
     const SolveArgs<float, MI>& a = m.g;
     __shared__ float red[kTile / 32];
@@ -1371,13 +1419,16 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_spmv(GMixArgs<MI
         if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
         const int64_t vo = static_cast<int64_t>(b_) * a.rows;
         // the scaled system needs no preconditioner: p_k = r + beta p_{k-1}
-        const PNext<float> pn{a.r + vo, nullptr, pprev + vo, static_cast<float>(a.st.beta[g.inst])};
+        using PS = std::conditional_t<FUSED, PNext<float>, PDirect<float>>;
+        PS pn;
+        if constexpr (FUSED) pn = PS{a.r + vo, nullptr, pprev + vo, static_cast<float>(a.st.beta[g.inst])};
+        else pn = PS{pk + vo};
         float* pout = pk + vo;
         float* q = a.q + vo;
         float acc[1] = {0.0f};
         // q is read once, by the update kernel
         const auto emit3 = [&](int row, float qv, float prow) {
-            pout[row] = prow;
+            if constexpr (FUSED) pout[row] = prow;
             __stcs(q + row, qv);
             acc[0] += prow * qv;
         };
@@ -1593,6 +1644,31 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_residual(GMixArg
 }
 
 
+// p = r + beta p, where the product does not form p (p2 == p)
+template <typename MI, typename MO>
+__global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_pupdate(GMixArgs<MI, MO> m) {
+    const SolveArgs<float, MI>& a = m.g;
+    CMCG_FOR_SEGMENTS(a) {
+        const SegInfo g = seg_info(a, b_, seg_);
+        if (ld_status(a.st.status + g.inst) != ST_RUNNING) continue;
+        const int64_t vo = static_cast<int64_t>(b_) * a.rows;
+        const float beta = static_cast<float>(a.st.beta[g.inst]);
+        const float* r = a.r + vo;
+        float* p = a.p + vo;
+        const void* const ptrs[2] = {r + g.r0, p + g.r0};
+        seg_rows_vec<2>(
+            g.r0, g.r1, ptrs,
+            [&](int i) {
+                V4<float> R, P;
+                R.load(r + i);
+                P.load(p + i);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) P.v[k] = R.v[k] + beta * P.v[k];
+                P.store(p + i);
+            },
+            [&](int i) { p[i] = r[i] + beta * p[i]; });
+    }
+}
 // the host-driven loop's count of finished iterations (the graph's condition
 // kernel keeps it there; the products read its parity)
 __global__ void k_loop_step(int32_t* loops) { ++*loops; }
@@ -1703,6 +1779,9 @@ struct cmcg_solver_s {
     int coop = 1;
     // cluster solve of the grid path where it applies (CUMAT_CG_CLUSTER=0 disables)
     bool cluster = true;
+    // grid path: the product forms p_k (-1: by the batch's vector bytes against
+    // L2, see fuse_p_update; 0 / 1: CUMAT_CG_FUSE)
+    int fuse_p = -1;
     // grid path iteration loop: true = one CUDA graph with a device-side WHILE
     // node; false = the same kernels launched from the host, polling the count
     // of running instances (CUMAT_CG_GRAPH=0; kernel profilers do not replay
@@ -2352,6 +2431,23 @@ cmcg_status run_persistent(cmcg_solver s, SolveArgs<VT, MT>& a) {
     return CMCG_OK;
 }
 
+// Whether the grid path's product forms p_k itself (one launch less per
+// iteration) or reads it from a separate p-update kernel. Forming it re-reads
+// r, M^-1 and p_{k-1} at every gathered offset, which costs nothing while
+// those vectors of the whole batch (vec_bytes) stay in L2, and triples their
+// DRAM traffic when they do not: measured on the B200, 2D Poisson 1024^2 26.0
+// against 27.2 us per iteration formed, 10000^2 1436 against 1199 us. The
+// split is half the L2.
+bool fuse_p_update(cmcg_solver s, double vec_bytes) {
+    if (s->fuse_p >= 0) return s->fuse_p != 0;
+    int l2 = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->A->pat->ctx->device) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return vec_bytes <= 0.5 * l2;
+}
+
 template <typename VT, typename MT, int FMT>
 cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
     cmcg_ctx ctx = s->A->pat->ctx;
@@ -2387,27 +2483,41 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
         }
     }
 
+    const bool fused = fuse_p_update(s, 3.0 * sizeof(VT) * static_cast<double>(a.rows) * a.ob);
+    if (!fused) a.p2 = a.p;   // (one p buffer: the kernels read p_k as stored)
     CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), st));
     k_grid_init<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
     k_grid_init2<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
     count_launch(2);
     CMCG_CHECK_LAUNCH();
 
-    if (!s->graph_loop) {
-        return host_loop(st, a.active, a.loop_cap, 3, [&] {
+    // one iteration's kernels on stream t: p update + product + p.q (or the
+    // product alone and a separate p update), then the x / r update
+    const auto iteration = [&](cudaStream_t t) {
+        const auto product = [&](auto fuse) {
+            constexpr bool F = decltype(fuse)::value;
             if constexpr (FMT == CMCG_CSR) {
-                if (nd == 5) k_grid_spmv_pq<VT, MT, FMT, 5><<<grid, kTile, 0, st>>>(a);
-                else if (nd == 7) k_grid_spmv_pq<VT, MT, FMT, 7><<<grid, kTile, 0, st>>>(a);
-                else k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+                if (nd == 5) k_grid_spmv_pq<VT, MT, FMT, 5, F><<<grid, kTile, 0, t>>>(a);
+                else if (nd == 7) k_grid_spmv_pq<VT, MT, FMT, 7, F><<<grid, kTile, 0, t>>>(a);
+                else k_grid_spmv_pq<VT, MT, FMT, 0, F><<<grid, kTile, 0, t>>>(a);
             } else {
-                k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+                k_grid_spmv_pq<VT, MT, FMT, 0, F><<<grid, kTile, 0, t>>>(a);
             }
-            k_grid_update<VT, MT, FMT><<<grid, kTile, 0, st>>>(a);
+        };
+        if (fused) product(std::true_type{});
+        else product(std::false_type{});
+        k_grid_update<VT, MT, FMT><<<grid, kTile, 0, t>>>(a);
+        if (!fused) k_grid_pupdate<VT, MT, FMT><<<grid, kTile, 0, t>>>(a);
+    };
+    const int per_iter = fused ? 2 : 3;
+    if (!s->graph_loop) {
+        return host_loop(st, a.active, a.loop_cap, per_iter + 1, [&] {
+            iteration(st);
             k_loop_step<<<1, 1, 0, st>>>(a.loops);
         });
     }
 
-    // graph with a WHILE node over the two iteration kernels; rebuilt when any
+    // graph with a WHILE node over the iteration kernels; rebuilt when any
     // kernel argument changes
     std::vector<char> key(sizeof(a) + sizeof(int) * 2);
     {
@@ -2437,14 +2547,7 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
         if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
         cudaStream_t cs = ctx->capture_stream;
         CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        if constexpr (FMT == CMCG_CSR) {
-            if (nd == 5) k_grid_spmv_pq<VT, MT, FMT, 5><<<grid, kTile, 0, cs>>>(a);
-            else if (nd == 7) k_grid_spmv_pq<VT, MT, FMT, 7><<<grid, kTile, 0, cs>>>(a);
-            else k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
-        } else {
-            k_grid_spmv_pq<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
-        }
-        k_grid_update<VT, MT, FMT><<<grid, kTile, 0, cs>>>(a);
+        iteration(cs);
         k_grid_cond<<<1, 1, 0, cs>>>(a.active, a.loops, a.loop_cap, h);
         cudaGraph_t captured = nullptr;
         cudaError_t ce = cudaStreamEndCapture(cs, &captured);
@@ -2453,8 +2556,8 @@ cmcg_status run_grid(cmcg_solver s, SolveArgs<VT, MT>& a) {
         s->gkey = key;
     }
     CMCG_CUDA(cudaGraphLaunch(s->gexec, st));
-    // kernels inside the graph: 3 per executed iteration (counted as launched
-    // by the graph, not by the host)
+    // kernels inside the graph: per_iter + 1 per executed iteration (counted as
+    // launched by the graph, not by the host)
     count_launch(1);
     return CMCG_OK;
 }
@@ -2954,19 +3057,32 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
         }
     }
 
+    // the product forms p_k when r and p of the batch stay in L2 (fuse_p_update)
+    const bool fused = fuse_p_update(s, 2.0 * sizeof(float) * static_cast<double>(nv));
+    if (!fused) m.g.p2 = m.g.p;   // (one p buffer: the kernels read p_k as stored)
     CMCG_CUDA(cudaMemcpyAsync(b64, b, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CMCG_CUDA(cudaMemsetAsync(s->counters, 0, 3 * sizeof(int32_t), st));
     k_gmix_init<MI, MO><<<grid, kTile, 0, st>>>(m);
     count_launch();
     CMCG_CHECK_LAUNCH();
+    // one iteration's kernels on stream t
+    const auto iteration = [&](cudaStream_t t) {
+        const auto product = [&](auto fuse) {
+            constexpr bool F = decltype(fuse)::value;
+            if (nd == 5) k_gmix_spmv<MI, MO, 5, F><<<grid, kTile, 0, t>>>(m);
+            else if (nd == 7) k_gmix_spmv<MI, MO, 7, F><<<grid, kTile, 0, t>>>(m);
+            else k_gmix_spmv<MI, MO, 0, F><<<grid, kTile, 0, t>>>(m);
+        };
+        if (fused) product(std::true_type{});
+        else product(std::false_type{});
+        k_gmix_update<MI, MO><<<grid, kTile, 0, t>>>(m);
+        k_gmix_fold<MI, MO, false><<<grid, kTile, 0, t>>>(m);
+        k_gmix_residual<MI, MO, false><<<grid, kTile, 0, t>>>(m);
+        if (!fused) k_gmix_pupdate<MI, MO><<<grid, kTile, 0, t>>>(m);
+    };
     if (!s->graph_loop) {
-        CMCG_TRY(host_loop(st, m.g.active, m.g.loop_cap, 5, [&] {
-            if (nd == 5) k_gmix_spmv<MI, MO, 5><<<grid, kTile, 0, st>>>(m);
-            else if (nd == 7) k_gmix_spmv<MI, MO, 7><<<grid, kTile, 0, st>>>(m);
-            else k_gmix_spmv<MI, MO><<<grid, kTile, 0, st>>>(m);
-            k_gmix_update<MI, MO><<<grid, kTile, 0, st>>>(m);
-            k_gmix_fold<MI, MO, false><<<grid, kTile, 0, st>>>(m);
-            k_gmix_residual<MI, MO, false><<<grid, kTile, 0, st>>>(m);
+        CMCG_TRY(host_loop(st, m.g.active, m.g.loop_cap, fused ? 5 : 6, [&] {
+            iteration(st);
             k_loop_step<<<1, 1, 0, st>>>(m.g.loops);
         }));
     } else {
@@ -2998,12 +3114,7 @@ cmcg_status refined_grid_mixed(cmcg_solver s, cmcg_matrix Ao, const double* b, i
             if (!ctx->capture_stream) CMCG_CUDA(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
             cudaStream_t cs = ctx->capture_stream;
             CMCG_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-            if (nd == 5) k_gmix_spmv<MI, MO, 5><<<grid, kTile, 0, cs>>>(m);
-            else if (nd == 7) k_gmix_spmv<MI, MO, 7><<<grid, kTile, 0, cs>>>(m);
-            else k_gmix_spmv<MI, MO><<<grid, kTile, 0, cs>>>(m);
-            k_gmix_update<MI, MO><<<grid, kTile, 0, cs>>>(m);
-            k_gmix_fold<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
-            k_gmix_residual<MI, MO, false><<<grid, kTile, 0, cs>>>(m);
+            iteration(cs);
             k_grid_cond<<<1, 1, 0, cs>>>(m.g.active, m.g.loops, m.g.loop_cap, h);
             cudaGraph_t captured = nullptr;
             cudaError_t ce = cudaStreamEndCapture(cs, &captured);
@@ -3053,6 +3164,7 @@ cmcg_status cmcg_cg_create(cmcg_matrix A, int32_t precond, cmcg_solver* out) {
     if (const char* e = std::getenv("CUMAT_CG_SMALL")) s->mix_small = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_COOP")) s->coop = std::max(0, std::min(2, std::atoi(e)));
     if (const char* e = std::getenv("CUMAT_CG_CLUSTER")) s->cluster = std::atoi(e) != 0;
+    if (const char* e = std::getenv("CUMAT_CG_FUSE")) s->fuse_p = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_GRAPH")) s->graph_loop = std::atoi(e) != 0;
     if (const char* e = std::getenv("CUMAT_CG_BF16_FALLBACK")) s->bf16_fallback = std::atoi(e) != 0;
     cmcg_status st = build_plan(s);

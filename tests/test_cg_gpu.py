@@ -767,6 +767,44 @@ def test_host_loop_matches_graph_loop(cuda, monkeypatch, kind, cap):
         assert s1["status"][0] == m._native.SOLVE_MAX_ITER and int(s1["iterations"][0]) == cap
 
 
+@pytest.mark.parametrize("kind", ["fp64", "mixed_f32"])
+def test_grid_p_update_fused_or_separate(cuda, monkeypatch, kind):
+    # the grid path's product forms p_k itself where the batch's vectors stay
+    # in L2 and reads it from a separate p-update kernel otherwise
+    # (CUMAT_CG_FUSE forces either); both evaluate M^-1 r + beta p_{k-1} with
+    # the same expression, so iterations, statuses and solutions agree bit for
+    # bit, with one kernel launch per iteration less when fused
+    m = cm()
+    monkeypatch.setenv("CUMAT_CG_COOP", "0")
+    monkeypatch.setenv("CUMAT_CG_CLUSTER", "0")
+    p3 = P.fv3d(24, 1.0, 9)
+    pat = m.SparsityPattern.csr(p3.n, p3.n, p3.row_ptr, p3.col)
+    A64 = m.SparseMatrix(pat, dtype=torch.float64).setData(p3.val.astype(np.float64))
+    A32 = m.SparseMatrix(pat, dtype=torch.float32).setData(p3.val)
+    b64 = torch.from_numpy(p3.b.astype(np.float64)).to(cuda)
+
+    def run(fuse):
+        monkeypatch.setenv("CUMAT_CG_FUSE", fuse)
+        monkeypatch.setenv("CUMAT_CG_GRAPH", "0")   # (host loop: launches counted per kernel)
+        if kind == "fp64":
+            cg = m.ConjugateGradient(A64).setTolerance(1e-10).set_path(2)
+            before = m.launch_count()
+            x = cg.solve(b64)
+        else:
+            cg = m.ConjugateGradient(A32).setTolerance(1e-4).set_path(2)
+            before = m.launch_count()
+            x = cg.solve_refined(b64, outer=A32, outer_tol=1e-10, max_outer=60)
+        x = x.cpu().numpy()
+        return x, cg.system_stats(), m.launch_count() - before
+
+    x1, s1, l1 = run("1")
+    x0, s0, l0 = run("0")
+    assert np.array_equal(s1["iterations"], s0["iterations"]) and np.array_equal(s1["status"], s0["status"])
+    assert s1["status"][0] == 0
+    assert np.array_equal(x1, x0)
+    assert l0 - l1 >= int(s1["iterations"][0])   # one p-update launch per iteration saved
+
+
 def test_cooperative_solve_forced_on_large_system(cuda, monkeypatch):
     # systems above 2^15 rows take the graph loop unless CUMAT_CG_COOP=2; the
     # cooperative launch stages each CTA's window of p (its rows plus the
