@@ -909,9 +909,11 @@ struct PNext {
     const VT* __restrict__ dinv;   // null: identity
     const VT* __restrict__ pin;    // p_{k-1}
     VT beta;
+    // (one explicit fused multiply-add, as in the separate p-update kernels,
+    // so that both forms round alike)
     __device__ __forceinline__ VT form(VT d, VT ri, VT pi) const {
         const VT z = dinv ? d * ri : ri;
-        return z + beta * pi;
+        return fma(beta, pi, z);
     }
     __device__ __forceinline__ VT operator()(int c) const {
         return form(dinv ? __ldg(dinv + c) : VT(1), __ldg(r + c), __ldg(pin + c));
@@ -1302,13 +1304,13 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_grid_pupdate(SolveArg
                 P.load(p + i);
                 if (dinv) D.load(dinv + i);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) P.v[k] = (dinv ? D.v[k] * R.v[k] : R.v[k]) + beta * P.v[k];
+                for (int k = 0; k < 4; ++k) P.v[k] = fma(beta, P.v[k], dinv ? D.v[k] * R.v[k] : R.v[k]);
                 P.store(p + i);
             },
             [&](int i) {
                 const VT ri = r[i];
                 const VT zi = dinv ? dinv[i] * ri : ri;
-                p[i] = zi + beta * p[i];
+                p[i] = fma(beta, p[i], zi);
             });
     }
 }
@@ -1663,10 +1665,10 @@ __global__ void __launch_bounds__(kTile, kGridCtasPerSm) k_gmix_pupdate(GMixArgs
                 R.load(r + i);
                 P.load(p + i);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) P.v[k] = R.v[k] + beta * P.v[k];
+                for (int k = 0; k < 4; ++k) P.v[k] = fmaf(beta, P.v[k], R.v[k]);
                 P.store(p + i);
             },
-            [&](int i) { p[i] = r[i] + beta * p[i]; });
+            [&](int i) { p[i] = fmaf(beta, p[i], r[i]); });
     }
 }
 // the host-driven loop's count of finished iterations (the graph's condition
