@@ -467,6 +467,121 @@ def cg_config2(cm, torch, dev, stream, hbm_peak):
     return out
 
 
+# benchmarks/batched_reductions_22.json (RTX 2070, ms per call): 2^22 FP32
+# values, N of them reduced per output along one axis, the other two axes
+# sqrt(2^22 / N) and the rest (benchmarks/batched_reduction/main.cpp:89-153).
+# Per N: the reference's default sum (its "Baseline" column) and the fastest
+# of its Thread / Warp / Block / Device kernels.
+REF_REDUCE_MS = {
+    "Row": {2: (33.7065, 0.071104), 16: (4.46387, 0.105552), 128: (0.525456, 0.0472), 1024: (0.165888, 0.045168),
+            8192: (0.173024, 0.04704), 65536: (0.216528, 0.221456), 1048576: (2.53859, 0.073376)},
+    "Column": {2: (33.7774, 0.077824), 16: (4.3645, 0.054336), 128: (0.475952, 0.045056), 1024: (0.17608, 0.077648),
+               8192: (0.195568, 0.058), 65536: (0.213344, 0.314016), 1048576: (2.52806, 0.106976)},
+    "Batch": {2: (34.2191, 0.070992), 16: (4.37658, 0.054528), 128: (0.47696, 0.04416), 1024: (0.180176, 0.076672),
+              8192: (0.188512, 0.146992), 65536: (0.222464, 0.537232), 1048576: (2.52939, 0.182544)},
+}
+_REDUCE_AXIS = {"Row": ("rows",), "Column": ("cols",), "Batch": ("batches",)}
+
+
+def _reduce_shape(axis, n, total):
+    """(rows, cols, batches) of the reference's benchmark: N along the reduced
+    axis, the others sqrt(total / N) and the rest."""
+    o1 = int(np.sqrt(total / n))
+    o2 = total // (n * o1)
+    return {"Row": (n, o1, o2), "Column": (o1, n, o2), "Batch": (o1, o2, n)}[axis]
+
+
+def _block_poisson(g, B, seed):
+    """3D-vector 2D Poisson in block CSR: on a g x g grid, diagonal blocks
+    5 I + C (C symmetric, entries in [-0.1, 0.1]), off-diagonal blocks -I:
+    symmetric positive definite (the Laplacian plus a block diagonal with
+    eigenvalues above 0.6)."""
+    from cumat_b200 import problems as P
+    pr = P.poisson2d(g, 0)
+    rows = np.repeat(np.arange(pr.n), np.diff(pr.row_ptr))
+    blocks = np.broadcast_to(-np.eye(B, dtype=np.float32), (pr.nnz, B, B)).copy()
+    diag = rows == pr.col
+    C = np.random.default_rng(seed).uniform(-0.1, 0.1, (int(diag.sum()), B, B)).astype(np.float32)
+    blocks[diag] = 5 * np.eye(B, dtype=np.float32) + (C + C.transpose(0, 2, 1)) / 2
+    return pr.n, pr.row_ptr, pr.col, blocks
+
+
+def next_rows(cm, torch, dev, stream, hbm_peak):
+    """The rows beside the CG path, measured (ms per call through the public
+    API, CUDA events after warm-up and the first call's kernel choice):
+
+    reduce        the reference's batched-reduction benchmark (2^22 FP32
+                  values along each axis, against its RTX 2070 times)
+    reduce_hbm    2^28 FP32 values (1 GiB, beyond L2) reduced along each axis
+                  with N = 1024 and fully: GB/s of the input read
+    transposed    4096^2 Poisson (FP32, 84 M entries, beyond L2): A x (CSR),
+                  A^T x (transposed product) and A x on the same arrays
+                  declared CSC, bytes as for the CSR product
+    blocked_cg    Jacobi-CG on a 3 x 3-block Poisson matrix (BSR, 512^2
+                  blocks, 786,432 rows) to 1e-6: us per iteration
+    """
+    def ev_ms(fn, reps, warm=3):
+        return _ev_time(torch, stream, fn, reps, warm)
+
+    out = {"reduce": [], "reduce_hbm": []}
+    gen = torch.Generator(device=dev).manual_seed(5)
+    for axis, table in REF_REDUCE_MS.items():
+        for n, (ref_def, ref_best) in table.items():
+            R, Cc, B = _reduce_shape(axis, n, 1 << 22)
+            x = torch.rand((B, Cc, R), device=dev, generator=gen)
+            ax = _REDUCE_AXIS[axis]
+            t = ev_ms(lambda: cm.reduce(x, "sum", ax), 100)
+            out["reduce"].append({"axis": axis, "n": n, "shape_rcb": [R, Cc, B], "ms": round(t, 5),
+                                  "ref_default_ms": ref_def, "ref_best_ms": ref_best,
+                                  "speedup_vs_default": round(ref_def / t, 1), "speedup_vs_best": round(ref_best / t, 1)})
+            del x
+    total = 1 << 28
+    x = torch.rand(total, device=dev, generator=gen)
+    for axis in ("Row", "Column", "Batch", "All"):
+        if axis == "All":
+            shape, ax = (1 << 10, 1 << 9, 1 << 9), ("rows", "cols", "batches")
+        else:
+            shape, ax = _reduce_shape(axis, 1024, total), _REDUCE_AXIS[axis]
+        R, Cc, B = shape
+        xv = x.view(B, Cc, R)
+        o = cm.reduce(xv, "sum", ax)
+        t = ev_ms(lambda: cm.reduce(xv, "sum", ax), 20)
+        byt = (total + o.numel()) * 4
+        out["reduce_hbm"].append({"axis": axis, "shape_rcb": [R, Cc, B], "ms": round(t, 4),
+                                  "gbs": round(byt / t / 1e6, 1), "frac": round(byt / t / 1e6 / hbm_peak, 3)})
+    del x
+    torch.cuda.empty_cache()
+
+    from cumat_b200 import problems as P
+    pr = P.poisson2d(4096, 1)
+    A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    Ac = cm.SparseMatrix(cm.SparsityPattern.csc(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+    xv = torch.from_numpy(pr.b).to(dev)
+    y = torch.empty_like(xv)
+    byt = pr.nnz * 8 + (pr.n + 1) * 4 + 2 * pr.n * 4
+    tr = {"rows": pr.n, "nnz": pr.nnz, "alg_bytes": byt}
+    for name, fn in (("csr", lambda: A.product(xv, out=y)), ("transposed", lambda: A.transposed_product(xv, out=y)),
+                     ("csc", lambda: Ac.product(xv, out=y))):
+        t = ev_ms(fn, 20)
+        tr[name] = {"ms": round(t, 4), "gbs": round(byt / t / 1e6, 1), "frac": round(byt / t / 1e6 / hbm_peak, 3)}
+    out["transposed"] = tr
+    del A, Ac, xv, y, pr
+    torch.cuda.empty_cache()
+
+    nb, brp, bci, blocks = _block_poisson(512, 3, 3)
+    Ab = cm.SparseMatrix(cm.SparsityPattern.bsr(nb, nb, 3, brp, bci)).setData(blocks.reshape(-1))
+    n = nb * 3
+    b = torch.from_numpy(np.random.default_rng(4).uniform(-1, 1, n).astype(np.float32)).to(dev)
+    xs = torch.empty_like(b)
+    cg = cm.ConjugateGradient(Ab).setTolerance(1e-6)
+    cg.solve(b, out=xs)
+    t = ev_ms(lambda: cg.solve(b, out=xs), 3, warm=1)
+    its = cg.iterations()
+    out["blocked_cg"] = {"block": 3, "block_rows": nb, "rows": n, "nnz": int(bci.size) * 9, "iterations": its,
+                         "error": cg.error(), "ms": round(t, 3), "us_per_iter": round(t * 1e3 / max(1, its), 2)}
+    return out
+
+
 def cg_poisson10000(cm, torch, dev, stream, hbm_peak):
     """The grid path's iteration on the 10000^2 Poisson matrix (10^8 rows, FP32,
     Jacobi; every vector 400 MB, far above L2): the per-iteration time is the
@@ -695,6 +810,8 @@ def run_ours(args):
         extra["cg_poisson1024"] = cg_config2(cm, torch, dev, stream, hbm_peak)
         extra["cg_poisson10000"] = cg_poisson10000(cm, torch, dev, stream, hbm_peak)
         extra["precision_c4"] = precision_c4(cm, torch, dev, stream)
+    if rank == 0 and world == 1 and not args.no_next:
+        extra["next_rows"] = next_rows(cm, torch, dev, stream, hbm_peak)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(bt, args.cpu_budget)
@@ -757,6 +874,12 @@ def run_ours(args):
                       c4_ratio_f32=c4["ratio_f32"], c4_ratio_bf16=c4["ratio_bf16"],
                       c4_true_res=[c4["mixed_f32"]["true_rel_residual"], c4["mixed_bf16"]["true_rel_residual"],
                                    c4["fp64"]["true_rel_residual"]])
+        if "next_rows" in extra:
+            nr = extra["next_rows"]
+            hl.update(reduce_hbm_frac={r["axis"]: r["frac"] for r in nr["reduce_hbm"]},
+                      reduce_speedup_vs_best_min=min(r["speedup_vs_best"] for r in nr["reduce"]),
+                      transposed_frac=nr["transposed"]["transposed"]["frac"], csc_frac=nr["transposed"]["csc"]["frac"],
+                      blocked_cg_us_per_iter=nr["blocked_cg"]["us_per_iter"])
         line["headline"] = hl
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -892,6 +1015,10 @@ def run_profile_case(case: str):
                 sampled outer product on n = 64 Mi entries (k_dot, k_lincomb,
                 k_sddmm_csr on the 8192^2 Poisson pattern)
     spmv_big    CSR and ELLPACK products on the 8192^2 Poisson matrix (3 each)
+    reduce      sums of 2^28 FP32 values along rows, columns, batches (1024
+                each) and over all axes, kernel choice included (k_red_*)
+    transposed  three transposed products on the 4096^2 Poisson matrix
+                (k_spmv_t, after the one-time value gather)
     cg10000     three grid-path Jacobi-CG iterations on the 10000^2 Poisson
                 matrix (FP32, diagonal layout: the fused product + p.q kernel;
                 about 10 GB on the device: launch lists only)
@@ -971,6 +1098,22 @@ def run_profile_case(case: str):
         u = torch.rand(pr.n, device=dev, generator=g)
         cm.sddmm(A, u, u)
         out.update(n=n, sddmm_rows=pr.n, sddmm_nnz=pr.nnz)
+    elif case == "reduce":
+        # 2^28 FP32 values (1 GiB) summed along rows, columns and batches (N =
+        # 1024 each) and fully; the first call of each shape times its candidates
+        x = torch.rand(1 << 28, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+        for axis in ("Row", "Column", "Batch"):
+            R, Cc, B = _reduce_shape(axis, 1024, 1 << 28)
+            cm.reduce(x.view(B, Cc, R), "sum", _REDUCE_AXIS[axis])
+        cm.reduce(x.view(1 << 9, 1 << 9, 1 << 10), "sum", ("rows", "cols", "batches"))
+        out.update(n=1 << 28)
+    elif case == "transposed":
+        pr = P.poisson2d(4096, 1)
+        A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
+        x = torch.from_numpy(pr.b).to(dev)
+        for _ in range(3):
+            A.transposed_product(x)
+        out.update(rows=pr.n, nnz=pr.nnz)
     elif case == "spmv_big":
         pr = P.poisson2d(8192, 1)
         A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
@@ -997,6 +1140,8 @@ def main():
     ap.add_argument("--no-spmv", action="store_true", help="skip the SpMV GB/s sub-benchmark")
     ap.add_argument("--no-suite", action="store_true",
                     help="skip the reference's own benchmark shapes (SpMV grids 10..10000, CG grids 10..1000)")
+    ap.add_argument("--no-next", action="store_true",
+                    help="skip the reductions, transposed / CSC products and blocked CG")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the 1024^2 Poisson Jacobi-CG and the 256^3 precision comparison")
     ap.add_argument("--cpu-budget", type=float, default=15.0)

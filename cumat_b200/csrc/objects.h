@@ -142,6 +142,11 @@ struct cmcg_matrix_s {
     int64_t sell_stride = 0;
     int64_t sell_version = -1;
     int64_t sell_plan_id = -1;
+    // values in the entry order of the pattern's transpose ([batch][t_stride]),
+    // regathered when `version` changes (the transposed product)
+    void* d_t_vals = nullptr;
+    int64_t t_stride = 0;
+    int64_t t_version = -1;
     // handle + every solver created on it; freed when the last one is released
     int refs = 1;
 };

@@ -13,8 +13,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "common.cuh"
 #include "objects.h"
@@ -79,15 +81,114 @@ cmcg_status cuda_fail(cudaError_t e, const char* what, const char* file, int lin
 
 void count_launch(int n) { g_launches += n; }
 
+// ---- device memory ----------------------------------------------------------------
+//
+// A process-wide cache of freed device blocks, in place of the reference's
+// caching device allocator behind Context::mallocDevice / freeDevice
+// (cuMat/src/Context.h:271-320): building and releasing solvers, matrices
+// and work buffers per call (as the reference's CG benchmark does) then costs
+// no driver allocation. Sizes are rounded to classes (powers of two from
+// 512 B to 1 MiB, multiples of 2 MiB above); a freed block joins the cache
+// only after a device synchronisation (cudaFree synchronises the device as
+// well), so no kernel still in flight can read it once it is handed out
+// again. Cached bytes per process are capped by CUMAT_CACHE_MB (default
+// 1024; 0 turns the cache off); a block above a quarter of the cap goes back
+// to the driver, and an allocation that fails empties the cache and retries.
+namespace {
+struct MemBlock {
+    int device;
+    size_t bytes;
+};
+std::mutex g_mem_mu;
+// (never destroyed: no CUDA call may run from a static destructor)
+std::unordered_map<void*, MemBlock>& live_blocks() {
+    static auto* m = new std::unordered_map<void*, MemBlock>();
+    return *m;
+}
+std::multimap<std::pair<int, size_t>, void*>& free_blocks() {
+    static auto* m = new std::multimap<std::pair<int, size_t>, void*>();
+    return *m;
+}
+size_t g_cached_bytes = 0;
+
+size_t cache_cap() {
+    static const size_t cap = [] {
+        const char* e = std::getenv("CUMAT_CACHE_MB");
+        return static_cast<size_t>(e ? std::max(0, std::atoi(e)) : 1024) << 20;
+    }();
+    return cap;
+}
+
+size_t size_class(size_t b) {
+    if (b > (size_t(1) << 20)) return (b + (size_t(2) << 20) - 1) / (size_t(2) << 20) * (size_t(2) << 20);
+    size_t c = 512;
+    while (c < b) c <<= 1;
+    return c;
+}
+
+// returns every cached block to the driver (lock held)
+void trim_cache_locked() {
+    for (auto& kv : free_blocks()) cudaFree(kv.second);
+    free_blocks().clear();
+    g_cached_bytes = 0;
+}
+}  // namespace
+
 cmcg_status dev_alloc(void** p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) return CMCG_OK;
-    CMCG_CUDA(cudaMalloc(p, bytes));
+    int dev = 0;
+    CMCG_CUDA(cudaGetDevice(&dev));
+    const size_t cls = size_class(bytes);
+    std::lock_guard<std::mutex> lk(g_mem_mu);
+    auto it = free_blocks().find({dev, cls});
+    if (it != free_blocks().end()) {
+        *p = it->second;
+        free_blocks().erase(it);
+        g_cached_bytes -= cls;
+        live_blocks()[*p] = MemBlock{dev, cls};
+        return CMCG_OK;
+    }
+    cudaError_t e = cudaMalloc(p, cls);
+    if (e == cudaErrorMemoryAllocation && !free_blocks().empty()) {
+        cudaGetLastError();
+        trim_cache_locked();
+        e = cudaMalloc(p, cls);
+    }
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    live_blocks()[*p] = MemBlock{dev, cls};
     return CMCG_OK;
 }
 
 void dev_free(void* p) {
-    if (p) cudaFree(p);
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_mem_mu);
+    auto it = live_blocks().find(p);
+    if (it == live_blocks().end()) {   // (not from dev_alloc)
+        cudaFree(p);
+        return;
+    }
+    const MemBlock b = it->second;
+    live_blocks().erase(it);
+    int cur = -1;
+    if (b.bytes > cache_cap() / 4 || cudaGetDevice(&cur) != cudaSuccess || cur != b.device ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+        cudaFree(p);
+        return;
+    }
+    free_blocks().emplace(std::make_pair(b.device, b.bytes), p);
+    g_cached_bytes += b.bytes;
+    // over the cap: return the largest cached blocks first
+    while (g_cached_bytes > cache_cap() && !free_blocks().empty()) {
+        auto big = std::max_element(free_blocks().begin(), free_blocks().end(),
+                                    [](const auto& x, const auto& y) { return x.first.second < y.first.second; });
+        cudaFree(big->second);
+        g_cached_bytes -= big->first.second;
+        free_blocks().erase(big);
+    }
 }
 
 cmcg_status ensure_buffer(void** p, size_t* cur, size_t need) {
@@ -140,6 +241,7 @@ void matrix_release(cmcg_matrix m) {
     cudaStreamSynchronize(m->pat->ctx->stream);
     dev_free(m->d_vals);
     dev_free(m->d_sell_vals);
+    dev_free(m->d_t_vals);
     cmcg_pattern p = m->pat;
     delete m;
     pattern_release(p);

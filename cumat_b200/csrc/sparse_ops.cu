@@ -18,8 +18,10 @@
 // map and downloads scatter back, so products, the CG kernels (persistent,
 // grid, mixed precision, adjoint) and reductions need no format of their own.
 // The transposed product walks the pattern's transpose (built once per
-// pattern, counting sort by column) thread per column, reading the values
-// through the transpose's entry map: no atomics, a fixed summation order.
+// pattern, counting sort by column) thread per column, over a copy of the
+// values in the transpose's entry order (gathered once per value upload, so
+// the product streams them like a CSR product): no atomics, a fixed
+// summation order.
 
 #include <algorithm>
 #include <string>
@@ -51,22 +53,38 @@ __device__ __forceinline__ void put(VT* y, VT v) {
 }
 
 // y[b][c] (mode)= sum over the entries (r, c) of A of a_rc x[b][r]: thread per
-// column c of A, entries in ascending row order
+// column c of A over the transpose's entries (row index trow[k], value tv[k]
+// in the transpose's order), entries in ascending row order; kTUnroll entries
+// of the column are loaded before the first gather
+constexpr int kTUnroll = 8;
+
 template <typename MT, typename VT, int MODE>
 __global__ void __launch_bounds__(256) k_spmv_t(const int32_t* __restrict__ trp, const int32_t* __restrict__ trow,
-                                                const int32_t* __restrict__ tperm, const MT* __restrict__ vals,
-                                                int64_t vstride, int32_t mb, const VT* __restrict__ x, int32_t rows,
-                                                int32_t xb, VT* __restrict__ y, int32_t cols, int32_t ob) {
+                                                const MT* __restrict__ tvals, int64_t tstride, int32_t mb,
+                                                const VT* __restrict__ x, int32_t rows, int32_t xb, VT* __restrict__ y,
+                                                int32_t cols, int32_t ob) {
     const int64_t items = static_cast<int64_t>(cols) * ob;
     for (int64_t it = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; it < items;
          it += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int b = static_cast<int>(it / cols);
         const int c = static_cast<int>(it - static_cast<int64_t>(b) * cols);
-        const MT* v = vals + (mb == 1 ? 0 : b * vstride);
+        const MT* tv = tvals + (mb == 1 ? 0 : b * tstride);
         const VT* xv = x + (xb == 1 ? 0 : static_cast<int64_t>(b) * rows);
         VT acc = VT(0);
         const int e = __ldg(trp + c + 1);
-        for (int k = __ldg(trp + c); k < e; ++k) acc += mval<VT>(v[__ldg(tperm + k)]) * __ldg(xv + __ldg(trow + k));
+        for (int k = __ldg(trp + c); k < e; k += kTUnroll) {
+            int r[kTUnroll];
+            MT w[kTUnroll];
+#pragma unroll
+            for (int u = 0; u < kTUnroll; ++u) {
+                const bool in = k + u < e;
+                r[u] = in ? __ldg(trow + k + u) : -1;
+                w[u] = in ? tv[k + u] : MT{};
+            }
+#pragma unroll
+            for (int u = 0; u < kTUnroll; ++u)
+                if (r[u] >= 0) acc = fma(mval<VT>(w[u]), __ldg(xv + r[u]), acc);
+        }
         put<MODE>(y + it, acc);
     }
 }
@@ -169,17 +187,53 @@ cmcg_status ensure_transpose(cmcg_pattern p) {
     return CMCG_OK;
 }
 
+// A's values in the transpose's entry order (gathered through d_t_perm once
+// per value upload)
+cmcg_status ensure_t_values(cmcg_matrix A) {
+    if (A->d_t_vals && A->t_version == A->version) return CMCG_OK;
+    cmcg_pattern p = A->pat;
+    cmcg_ctx ctx = p->ctx;
+    const int64_t stride = csr_padded_nnz(p->nnz);
+    if (!A->d_t_vals) {
+        CMCG_TRY(dev_alloc(&A->d_t_vals, static_cast<size_t>(stride) * A->batches * dtype_size(A->dtype)));
+        A->t_stride = stride;
+    }
+    if (p->nnz > 0) {
+        const int grid = grid_for(ctx, p->nnz * A->batches);
+        switch (dtype_size(A->dtype)) {
+            case 2:
+                k_permute<uint16_t><<<grid, 256, 0, ctx->stream>>>(static_cast<const uint16_t*>(A->d_vals), A->stride,
+                                                                   static_cast<uint16_t*>(A->d_t_vals), stride,
+                                                                   p->d_t_perm, p->nnz, A->batches, 1);
+                break;
+            case 4:
+                k_permute<uint32_t><<<grid, 256, 0, ctx->stream>>>(static_cast<const uint32_t*>(A->d_vals), A->stride,
+                                                                   static_cast<uint32_t*>(A->d_t_vals), stride,
+                                                                   p->d_t_perm, p->nnz, A->batches, 1);
+                break;
+            default:
+                k_permute<uint64_t><<<grid, 256, 0, ctx->stream>>>(static_cast<const uint64_t*>(A->d_vals), A->stride,
+                                                                   static_cast<uint64_t*>(A->d_t_vals), stride,
+                                                                   p->d_t_perm, p->nnz, A->batches, 1);
+        }
+        count_launch();
+        CMCG_CHECK_LAUNCH();
+    }
+    A->t_version = A->version;
+    return CMCG_OK;
+}
+
 template <typename MT, typename VT>
 cmcg_status launch_spmv_t(cmcg_matrix A, const void* x, int32_t xb, void* y, int32_t mode) {
     cmcg_pattern p = A->pat;
     cmcg_ctx ctx = p->ctx;
+    CMCG_TRY(ensure_t_values(A));
     const int32_t ob = std::max(A->batches, xb);
     const int grid = grid_for(ctx, static_cast<int64_t>(p->cols) * ob);
-#define CMCG_SPMV_T(M)                                                                                          \
-    k_spmv_t<MT, VT, M><<<grid, 256, 0, ctx->stream>>>(p->d_t_row_ptr, p->d_t_col, p->d_t_perm,                 \
-                                                       static_cast<const MT*>(A->d_vals), A->stride, A->batches, \
-                                                       static_cast<const VT*>(x), p->rows, xb, static_cast<VT*>(y), \
-                                                       p->cols, ob)
+#define CMCG_SPMV_T(M)                                                                                              \
+    k_spmv_t<MT, VT, M><<<grid, 256, 0, ctx->stream>>>(p->d_t_row_ptr, p->d_t_col, static_cast<const MT*>(A->d_t_vals), \
+                                                       A->t_stride, A->batches, static_cast<const VT*>(x), p->rows, xb, \
+                                                       static_cast<VT*>(y), p->cols, ob)
     if (mode == CMCG_ASSIGN) CMCG_SPMV_T(CMCG_ASSIGN);
     else if (mode == CMCG_ADD) CMCG_SPMV_T(CMCG_ADD);
     else CMCG_SPMV_T(CMCG_SUB);

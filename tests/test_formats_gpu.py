@@ -115,6 +115,25 @@ def test_transposed_product_vs_oracle(cuda, dt):
     assert np.allclose(out.cpu().numpy(), y + 1, rtol=1e-6, atol=1e-6)
 
 
+def test_transposed_product_follows_new_values(cuda):
+    # the transposed product reads a copy of the values in the transpose's
+    # order; a value upload after the first product must reach the next one
+    m = cm()
+    Acsr = _rand_csr(300, 500, 0.05, 12)
+    p = m.SparsityPattern.csr(300, 500, Acsr.indptr, Acsr.indices)
+    A = m.SparseMatrix(p).setData(Acsr.data.astype(np.float32))
+    x = torch.from_numpy(np.random.default_rng(13).uniform(-1, 1, 300).astype(np.float32)).to(cuda)
+    y1 = A.transposed_product(x).cpu().numpy()
+    A.setData((-3.0 * Acsr.data).astype(np.float32))
+    y2 = A.transposed_product(x).cpu().numpy()
+    assert np.allclose(y2, -3.0 * y1, rtol=1e-5, atol=1e-5)
+    Atb = sp.csr_matrix(((-3.0 * Acsr.data).astype(np.float32), Acsr.indices, Acsr.indptr), shape=(300, 500)).T.tocsr()
+    Atb.sort_indices()
+    ref = O.spmv_csr(500, 300, Atb.indptr, Atb.indices, Atb.data, x.cpu().numpy())[0]
+    scale = np.abs(Atb).astype(np.float64) @ np.abs(x.cpu().numpy().astype(np.float64))
+    assert np.all(np.abs(y2 - ref) <= 1e-6 * np.maximum(scale, 1e-30))
+
+
 def _bsr_expand(block_rows, B, brp, bci, blocks):
     """The equivalent scalar CSR (rows of a block row in order, entries block by block)."""
     rp, col, val = [0], [], []

@@ -58,11 +58,12 @@ def _numpy_reduce(a, op, axes):
     return f(a, axis=ax, keepdims=True) if ax else a
 
 
-SHAPES = [(1000, 3, 7), (5, 900, 4), (300, 200, 2), (100000, 2, 3), (7, 5, 3000), (1 << 20, 1, 1)]
+SHAPES = [(1000, 3, 7), (5, 900, 4), (300, 200, 2), (100000, 2, 3), (7, 5, 3000), (1 << 20, 1, 1), (130, 1000, 3),
+          (2, 3, 5000)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
-@pytest.mark.parametrize("kernel", [None, "thread", "warp", "block", "split"])
+@pytest.mark.parametrize("kernel", [None, "thread", "warp", "block", "split", "tile"])
 def test_all_axis_sets_vs_numpy(cuda, monkeypatch, shape, kernel):
     # every axis set (the tuned kernel, then each kernel forced where it
     # applies), sum / min / max in FP64 and FP32
@@ -105,3 +106,31 @@ def test_prod_and_log_callback(cuda):
     finally:
         m.set_log_callback(None)
     assert any(level == 0 and "NULL" in msg for level, msg in msgs), msgs
+
+
+@pytest.mark.parametrize("kernel", ["warp", "tile", "block", "split"])
+@pytest.mark.parametrize("dt", [torch.float32, torch.float64])
+def test_unaligned_input_takes_scalar_loads(cuda, monkeypatch, kernel, dt):
+    # an input that starts 4 or 8 bytes past a 16-byte boundary (a slice of a
+    # larger buffer): the warp and tile kernels step back to scalar loads,
+    # block and split read each contiguous run with scalar loads up to the
+    # first 16-byte boundary; same sums as numpy
+    m = cm()
+    monkeypatch.setenv("CUMAT_REDUCE_KERNEL", kernel)
+    B, Cc, R = 3, 64, 256
+    rng = np.random.default_rng(11)
+    a = rng.uniform(-1.0, 1.0, (B, Cc, R))
+    base = torch.zeros(B * Cc * R + 1, dtype=dt, device=cuda)
+    base[1:] = torch.from_numpy(a.reshape(-1)).to(device=cuda, dtype=dt)
+    x = base[1:].view(B, Cc, R)
+    assert x.data_ptr() % 16 != 0
+    a_in = a.astype(np.float32).astype(np.float64) if dt == torch.float32 else a
+    tol = 2e-5 if dt == torch.float32 else 1e-13
+    for axes in (("rows",), ("cols",), ("batches",), ("cols", "batches"), ("rows", "batches"), ("rows", "cols"),
+                 ("rows", "cols", "batches")):
+        got = m.reduce(x, "sum", axes).cpu().numpy().astype(np.float64)
+        ref = _numpy_reduce(a_in, "sum", axes)
+        scale = _numpy_reduce(np.abs(a), "sum", axes)
+        assert np.all(np.abs(got - ref) <= tol * scale), (kernel, axes)
+        for op in ("min", "max"):
+            assert np.array_equal(m.reduce(x, op, axes).cpu().numpy().astype(np.float64), _numpy_reduce(a_in, op, axes))
