@@ -1024,6 +1024,8 @@ def run_profile_case(case: str):
                 about 10 GB on the device: launch lists only)
     cg4096      the same on the 4096^2 Poisson matrix (16.8 M rows, 1.2 GB
                 streamed per iteration), for full captures
+    cg1024      50 grid-path Jacobi-CG iterations on the 1024^2 Poisson matrix
+                (the 2456-iteration solve's shape; data L2-resident)
     cluster200  the 200^2 Poisson matrix (40,000 rows), FP32 Jacobi-CG capped at
                 50 iterations: the cluster solve (k_cluster_cg, one launch)
     c4          the 256^3 precision system: 12 plain FP64 Jacobi-CG iterations
@@ -1066,12 +1068,13 @@ def run_profile_case(case: str):
         b = torch.from_numpy(pr.b).to(dev)
         cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(50).solve(b)
         out.update(rows=pr.n, nnz=pr.nnz)
-    elif case in ("cg10000", "cg4096"):
-        pr = P.poisson2d(10000 if case == "cg10000" else 4096, 1)
+    elif case in ("cg10000", "cg4096", "cg1024"):
+        pr = P.poisson2d({"cg10000": 10000, "cg4096": 4096, "cg1024": 1024}[case], 1)
         A = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
         b = torch.from_numpy(pr.b).to(dev)
-        cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(3).set_path(2).solve(b)
-        out.update(rows=pr.n, nnz=pr.nnz)
+        its = 50 if case == "cg1024" else 3
+        cm.ConjugateGradient(A).setTolerance(1e-12).setMaxIterations(its).set_path(2).solve(b)
+        out.update(rows=pr.n, nnz=pr.nnz, iterations=its)
     elif case == "plain_dia":
         bt = P.fv2d_batch(N_SYS, SIDE_LO, SIDE_HI, SIGMA, SEED)
         k = int(bt.row_off[512])

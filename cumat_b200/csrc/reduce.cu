@@ -18,14 +18,15 @@
 //   block    one CTA per output, threads over (k2, k1), shuffles + one shared
 //            combine
 //   split    outputs' reductions cut into S chunks over S CTAs (few outputs,
-//            long reductions), partials in context scratch, then one thread per
-//            output adds its S partials in order
+//            long reductions), partials in context scratch, then one warp per
+//            output adds its S partials (lanes over the partials in order,
+//            then the shuffle tree)
 //   tile     reductions along an outer axis (K1 == 1, the kept innermost axis
 //            O1 contiguous): a CTA covers 32 V consecutive outputs of one o2
 //            (16-byte loads, V = 16 / sizeof(T), where O1 and the address
 //            allow) and a chunk of k2 split over its 8 warps; the warps'
 //            partials are added in warp order, and with S chunks per output
-//            the chunks' partials are added in chunk order as for split
+//            the chunks' partials are combined as for split
 // The warp kernel reads the contiguous reduced run with 16-byte loads where
 // K1 and the address allow; block and split do so wherever the reduced range
 // of an output is one contiguous run (K2 == 1).
@@ -319,13 +320,20 @@ __global__ void __launch_bounds__(256) k_red_split(const T* __restrict__ in, T* 
     }
 }
 
+// the S partials of each output added by one warp: lane l takes partials
+// l, l + 32, ... in order, then the lanes are combined by the shuffle tree
+// (a fixed order for a given S)
 template <typename T, int OP>
-__global__ void k_red_split_combine(const T* __restrict__ part, T* __restrict__ out, int64_t n, int32_t S) {
-    for (int64_t o = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; o < n;
-         o += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+__global__ void __launch_bounds__(256) k_red_split_combine(const T* __restrict__ part, T* __restrict__ out, int64_t n,
+                                                           int32_t S) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t o = w0; o < n; o += nw) {   // uniform per warp
         T acc = RedOp<T, OP>::id();
-        for (int s = 0; s < S; ++s) acc = RedOp<T, OP>::f(acc, part[o * S + s]);
-        out[o] = acc;
+        for (int s = lane; s < S; s += 32) acc = RedOp<T, OP>::f(acc, part[o * S + s]);
+        acc = warp_red<T, OP>(acc);
+        if (lane == 0) out[o] = acc;
     }
 }
 
@@ -381,7 +389,7 @@ cmcg_status launch_kern(cmcg_ctx ctx, int kern, const View& v, const T* in, T* o
         if (vec) k_red_tile<T, OP, kVec<T>><<<grid, 256, 0, st>>>(in, dst, v, S, tiles_o1);
         else k_red_tile<T, OP, 1><<<grid, 256, 0, st>>>(in, dst, v, S, tiles_o1);
         if (S > 1) {
-            const int g2 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 4)));
+            const int g2 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, sms * 16)));
             k_red_split_combine<T, OP><<<g2, 256, 0, st>>>(dst, out, n, S);
             count_launch();
         }
@@ -398,7 +406,7 @@ cmcg_status launch_kern(cmcg_ctx ctx, int kern, const View& v, const T* in, T* o
         T* part = static_cast<T*>(ctx->red_partial);
         const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(n * S, sms * 8)));
         k_red_split<T, OP><<<grid, 256, 0, st>>>(in, part, v, S);
-        const int g2 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 4)));
+        const int g2 = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, sms * 16)));
         k_red_split_combine<T, OP><<<g2, 256, 0, st>>>(part, out, n, S);
         count_launch();
     }
