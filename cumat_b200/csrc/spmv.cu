@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -100,9 +101,14 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_ell(const int32_t* __rest
 // the loads taken out of the dependency chain: a thread loads up to
 // kCsrUnroll column indices and values of its row (predicated on the row end)
 // before the first gather, so each thread keeps 2 * kCsrUnroll independent
-// loads and then kCsrUnroll gathers in flight. The scattered 4-byte loads of
-// neighbouring rows fall into the same cache lines, which L1 merges. Sums are
-// in entry order with fused multiply-adds, like the reference.
+// loads and then kCsrUnroll gathers in flight (variant 0). Variant 9 works on
+// R = 2 rows per thread at once (items it and it + stride of the flattened
+// (batch, row) index), with twice the loads in flight per thread at half the
+// resident threads, (batch, row) advanced by a step computed once per thread,
+// and a grid sized so that every grid-stride pass is equally full. The
+// scattered 4-byte loads of neighbouring rows fall into the same cache lines,
+// which L1 merges. Each row is summed in entry order with fused multiply-adds,
+// like the reference, so both give the same bits.
 
 constexpr int kCsrUnroll = 8;
 
@@ -134,6 +140,80 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_csr_rows(const int32_t* _
                 if (c[u] >= 0) acc = fma(mval<VT>(w[u]), __ldg(xv + c[u]), acc);
         }
         assign_out<MODE>(y + it, acc);
+    }
+}
+
+template <typename MT, typename VT, int MODE, int R>
+__global__ void __launch_bounds__(kSpmvThreads, 4) k_spmv_csr_rows2(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                                const MT* __restrict__ vals, int64_t vstride, int32_t mb,
+                                                                const VT* __restrict__ x, int32_t cols, int32_t xb,
+                                                                VT* __restrict__ y, int32_t rows, int32_t ob) {
+    const int64_t items = static_cast<int64_t>(rows) * ob;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kSpmvThreads;
+    int64_t it = static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x;
+    if (it >= items) return;
+    const int64_t db = stride / rows, dr = stride - db * rows;
+    int64_t b0 = it / rows, r0 = it - b0 * rows;
+    const auto advance = [&](int64_t& b, int64_t& r) {
+        r += dr;
+        b += db;
+        if (r >= rows) {
+            r -= rows;
+            ++b;
+        }
+    };
+    for (; it < items; it += R * stride) {
+        // the thread's rows of this pass: items it + j * stride
+        int64_t bb[R], rr[R];
+        bool has[R];
+        int k[R], e[R];
+        VT acc[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            if (j == 0) {
+                bb[0] = b0;
+                rr[0] = r0;
+            } else {
+                bb[j] = bb[j - 1];
+                rr[j] = rr[j - 1];
+                advance(bb[j], rr[j]);
+            }
+            has[j] = it + j * stride < items;
+            k[j] = has[j] ? __ldg(rp + rr[j]) : 0;
+            e[j] = has[j] ? __ldg(rp + rr[j] + 1) : 0;
+            acc[j] = VT(0);
+        }
+        bool more = true;
+        while (more) {
+            int c[R][kCsrUnroll];
+            MT w[R][kCsrUnroll];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const MT* v = vals + (mb == 1 ? 0 : bb[j] * vstride);
+#pragma unroll
+                for (int u = 0; u < kCsrUnroll; ++u) {
+                    const bool in = k[j] + u < e[j];
+                    c[j][u] = in ? __ldg(ci + k[j] + u) : -1;
+                    w[j][u] = in ? v[k[j] + u] : MT{};
+                }
+            }
+            more = false;
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const VT* xv = x + (xb == 1 ? 0 : bb[j] * cols);
+#pragma unroll
+                for (int u = 0; u < kCsrUnroll; ++u)
+                    if (c[j][u] >= 0) acc[j] = fma(mval<VT>(w[j][u]), __ldg(xv + c[j][u]), acc[j]);
+                k[j] += kCsrUnroll;
+                more = more || k[j] < e[j];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+            if (has[j]) assign_out<MODE>(y + it + j * stride, acc[j]);
+        b0 = bb[R - 1];
+        r0 = rr[R - 1];
+        advance(b0, r0);
     }
 }
 
@@ -558,9 +638,33 @@ cmcg_status launch_csr_tma(cmcg_matrix A, const VT* xv, int32_t xb, VT* yv, int3
 // wave of resident CTAs (grid-stride loop over the row quads)
 template <typename K>
 int resident_grid(K kern, int needed, int sm_count) {
+    // resident CTAs per SM, queried once per kernel (a host call per product
+    // would show in small products)
+    static std::mutex mu;
+    static std::map<const void*, int> occ_of;
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSpmvThreads, 0) != cudaSuccess || occ < 1) occ = 1;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = occ_of.find(reinterpret_cast<const void*>(kern));
+        if (it != occ_of.end()) occ = it->second;
+    }
+    if (occ == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSpmvThreads, 0) != cudaSuccess || occ < 1) occ = 1;
+        std::lock_guard<std::mutex> lk(mu);
+        occ_of[reinterpret_cast<const void*>(kern)] = occ;
+    }
     return std::max(1, std::min(needed, sm_count * occ));
+}
+
+// CTAs for `units` CTA-passes of grid-stride work: all of them when they fit
+// at once, else as few passes as the resident grid needs with every pass
+// equally full (no last pass that leaves most of the GPU idle)
+template <typename K>
+int balanced_grid(K kern, int64_t units, int sm_count) {
+    const int cap = resident_grid(kern, INT32_MAX, sm_count);
+    if (units <= cap) return static_cast<int>(std::max<int64_t>(1, units));
+    const int64_t passes = (units + cap - 1) / cap;
+    return static_cast<int>((units + passes - 1) / passes);
 }
 
 template <typename MT, typename VT, int MODE>
@@ -653,16 +757,29 @@ cmcg_status launch_spmv_variant(cmcg_matrix A, const void* x, int32_t xb, void* 
         CMCG_CHECK_LAUNCH();
         return CMCG_OK;
     }
-    if (p->format == CMCG_CSR && variant == 0) {
-        const int64_t threads = static_cast<int64_t>(p->rows) * ob;
-        const int needed = static_cast<int>(std::min<int64_t>((threads + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
-#define CMCG_LAUNCH_CSR_ROWS(M)                                                                                  \
+    if (p->format == CMCG_CSR && (variant == 0 || variant == 9)) {
+        const int64_t items = static_cast<int64_t>(p->rows) * ob;
+        const int rpt = variant == 9 ? 2 : 1;   // rows in flight per thread
+        const int64_t units = (items + static_cast<int64_t>(kSpmvThreads) * rpt - 1) / (static_cast<int64_t>(kSpmvThreads) * rpt);
+#define CMCG_LAUNCH_CSR_ROW1(M)                                                                                  \
     k_spmv_csr_rows<MT, VT, M><<<resident_grid(k_spmv_csr_rows<MT, VT, M>, needed, ctx->sm_count), kSpmvThreads, 0, \
                                  ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride, A->batches, xv, p->cols, xb, \
                                                 yv, p->rows, ob)
-        if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR_ROWS(CMCG_ASSIGN);
-        else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR_ROWS(CMCG_ADD);
-        else CMCG_LAUNCH_CSR_ROWS(CMCG_SUB);
+#define CMCG_LAUNCH_CSR_ROWS(M, R)                                                                                     \
+    k_spmv_csr_rows2<MT, VT, M, R><<<balanced_grid(k_spmv_csr_rows2<MT, VT, M, R>, units, ctx->sm_count), kSpmvThreads, \
+                                     0, ctx->stream>>>(p->d_row_ptr, p->d_col, vals, A->stride, A->batches, xv, p->cols, \
+                                                      xb, yv, p->rows, ob)
+        if (variant == 0) {
+            const int needed = static_cast<int>(std::min<int64_t>((items + kSpmvThreads - 1) / kSpmvThreads, max_blocks));
+            if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR_ROW1(CMCG_ASSIGN);
+            else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR_ROW1(CMCG_ADD);
+            else CMCG_LAUNCH_CSR_ROW1(CMCG_SUB);
+        } else {
+            if (mode == CMCG_ASSIGN) CMCG_LAUNCH_CSR_ROWS(CMCG_ASSIGN, 2);
+            else if (mode == CMCG_ADD) CMCG_LAUNCH_CSR_ROWS(CMCG_ADD, 2);
+            else CMCG_LAUNCH_CSR_ROWS(CMCG_SUB, 2);
+        }
+#undef CMCG_LAUNCH_CSR_ROW1
 #undef CMCG_LAUNCH_CSR_ROWS
         count_launch();
         CMCG_CHECK_LAUNCH();
@@ -964,7 +1081,7 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     }
     const std::string key = tune_key(p, DT<MT>::id, DT<VT>::id);
     const int cached = tune_lookup(key);
-    if (cached == 0 || cached == 1 || cached == 2 || ((cached == 7 || cached == 8) && p->format == CMCG_CSR)) {
+    if (cached == 0 || cached == 1 || cached == 2 || ((cached == 7 || cached == 8 || cached == 9) && p->format == CMCG_CSR)) {
         choice = static_cast<int8_t>(cached);
         return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, cached);
     }
@@ -972,11 +1089,12 @@ cmcg_status launch_spmv(cmcg_matrix A, const void* x, int32_t xb, void* y, int32
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (mode != CMCG_ASSIGN || cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
         return launch_spmv_variant<MT, VT>(A, x, xb, y, mode, 0);
-    // CSR: thread per row, warp-staged entries, four rows per thread with
-    // 16-byte chunks, bulk-staged tiles (the last candidate's output stays in
-    // y); ELLPACK: four rows per thread, thread per row
-    int cands[4] = {0, 8, 7, 2};
-    int nc = 4;
+    // CSR: thread per row (one or two rows in flight), warp-staged entries,
+    // four rows per thread with 16-byte chunks, bulk-staged tiles (the last
+    // candidate's output stays in y); ELLPACK: four rows per thread, thread
+    // per row
+    int cands[5] = {0, 9, 8, 7, 2};
+    int nc = 5;
     if (p->format != CMCG_CSR) {
         cands[1] = 1;
         nc = 2;

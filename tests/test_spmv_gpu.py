@@ -295,7 +295,7 @@ def test_tuning_cache_records_the_choice(cuda, monkeypatch, tmp_path):
     y0 = (A * x).cpu().numpy()
     lines = cache.read_text().split("\n")
     key = f"|csr|0|0|{pr.n}|{pr.nnz}|0 "
-    assert any(key in (l + " ") and l.split()[-1] in ("0", "2", "7", "8") for l in lines if l), lines
+    assert any(key in (l + " ") and l.split()[-1] in ("0", "2", "7", "8", "9") for l in lines if l), lines
     B = cm.SparseMatrix(cm.SparsityPattern.csr(pr.n, pr.n, pr.row_ptr, pr.col)).setData(pr.val)
     before = cm.launch_count()
     y1 = (B * x).cpu().numpy()
@@ -304,11 +304,12 @@ def test_tuning_cache_records_the_choice(cuda, monkeypatch, tmp_path):
 
 
 @pytest.mark.parametrize("dt", [torch.float32, torch.float64, torch.bfloat16])
-@pytest.mark.parametrize("variant,max_len", [("7", 12), ("8", 12), ("8", 700)])
+@pytest.mark.parametrize("variant,max_len", [("7", 12), ("8", 12), ("8", 700), ("9", 12), ("9", 700)])
 def test_row_order_kernels_equal_thread_per_row(cuda, monkeypatch, dt, variant, max_len):
-    # the 16-byte-chunk kernel (variant 7) and the warp-staged kernel (variant
-    # 8) add every row in entry order with fused multiply-adds, so they equal
-    # thread per row (variant 0) bit for bit: random rows of 0..max_len
+    # the 16-byte-chunk kernel (variant 7), the warp-staged kernel (variant 8)
+    # and thread per row with two rows in flight (variant 9) add every row in
+    # entry order with fused multiply-adds, so they equal thread per row
+    # (variant 0) bit for bit: random rows of 0..max_len
     # entries (empty rows, a row count that is not a multiple of 4 or 32, and
     # with max_len 700 rows that span several staging rounds of 256 entries),
     # two batches of values and vectors, all assignment modes
