@@ -911,29 +911,52 @@ cmcg_status launch_dot(cmcg_ctx ctx, int64_t n, const void* x, int32_t xb, const
 // ---- sampled outer product on the pattern -----------------------------------------
 
 // Sampled outer product on a CSR pattern, out_k = alpha * u[row(k)] * v[col(k)]
-// for every stored entry k: thread per row, as the row-unrolled product, with
-// kCsrUnroll column indices loaded before the first gather and reused for all
-// value batches; each product is (alpha * u) * v, the reference's order.
+// for every stored entry k: thread per row, two rows per thread in flight (r
+// and r + stride), with kCsrUnroll column indices of each loaded before the
+// first gather and reused for all value batches; each product is
+// (alpha * u) * v, the reference's order.
 template <typename VT>
 __global__ void __launch_bounds__(kSpmvThreads) k_sddmm_csr(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                                             int32_t rows, int32_t cols, int64_t vstride, VT alpha,
                                                             const VT* __restrict__ u, int32_t ub,
                                                             const VT* __restrict__ v, int32_t vb,
                                                             VT* __restrict__ out, int32_t ob) {
-    for (int r = blockIdx.x * kSpmvThreads + threadIdx.x; r < rows; r += gridDim.x * kSpmvThreads) {
-        const int e = __ldg(rp + r + 1);
-        for (int k = __ldg(rp + r); k < e; k += kCsrUnroll) {
-            int c[kCsrUnroll];
+    // two rows per thread in flight: r and r + stride
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kSpmvThreads;
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * kSpmvThreads + threadIdx.x; r < rows; r += 2 * stride) {
+        const int64_t rr[2] = {r, r + stride};
+        const bool has1 = r + stride < rows;
+        int k[2], e[2];
+        k[0] = __ldg(rp + r);
+        e[0] = __ldg(rp + r + 1);
+        k[1] = has1 ? __ldg(rp + rr[1]) : 0;
+        e[1] = has1 ? __ldg(rp + rr[1] + 1) : 0;
+        while (k[0] < e[0] || k[1] < e[1]) {
+            int c[2][kCsrUnroll];
 #pragma unroll
-            for (int q = 0; q < kCsrUnroll; ++q) c[q] = k + q < e ? __ldg(ci + k + q) : -1;
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int q = 0; q < kCsrUnroll; ++q) c[j][q] = k[j] + q < e[j] ? __ldg(ci + k[j] + q) : -1;
             for (int b = 0; b < ob; ++b) {
-                const VT au = alpha * __ldg(u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows) + r);
+                const VT* uu = u + (ub == 1 ? 0 : static_cast<int64_t>(b) * rows);
                 const VT* vv = v + (vb == 1 ? 0 : static_cast<int64_t>(b) * cols);
-                VT* o = out + static_cast<int64_t>(b) * vstride + k;
+                VT g[2][kCsrUnroll];
 #pragma unroll
-                for (int q = 0; q < kCsrUnroll; ++q)
-                    if (c[q] >= 0) o[q] = au * __ldg(vv + c[q]);
+                for (int j = 0; j < 2; ++j)
+#pragma unroll
+                    for (int q = 0; q < kCsrUnroll; ++q) g[j][q] = c[j][q] >= 0 ? __ldg(vv + c[j][q]) : VT(0);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    if (k[j] >= e[j]) continue;
+                    const VT au = alpha * __ldg(uu + rr[j]);
+                    VT* o = out + static_cast<int64_t>(b) * vstride + k[j];
+#pragma unroll
+                    for (int q = 0; q < kCsrUnroll; ++q)
+                        if (c[j][q] >= 0) o[q] = au * g[j][q];
+                }
             }
+            k[0] += kCsrUnroll;
+            k[1] += kCsrUnroll;
         }
     }
 }
@@ -964,8 +987,9 @@ cmcg_status launch_sddmm(cmcg_matrix M, double alpha, const void* u, int32_t ub,
     cmcg_pattern p = M->pat;
     cmcg_ctx ctx = p->ctx;
     if (p->format == CMCG_CSR) {
-        const int64_t need = (static_cast<int64_t>(p->rows) + kSpmvThreads - 1) / kSpmvThreads;
-        const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, ctx->sm_count * 8)));
+        // two rows per thread; 64 registers leave 4 CTAs per SM
+        const int64_t need = (static_cast<int64_t>(p->rows) + 2 * kSpmvThreads - 1) / (2 * kSpmvThreads);
+        const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(need, ctx->sm_count * 4)));
         k_sddmm_csr<VT><<<blocks, kSpmvThreads, 0, ctx->stream>>>(p->d_row_ptr, p->d_col, p->rows, p->cols, p->nnz,
                                                          static_cast<VT>(alpha), static_cast<const VT*>(u), ub,
                                                          static_cast<const VT*>(v), vb, static_cast<VT*>(out), ob);
